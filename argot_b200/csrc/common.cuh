@@ -1,0 +1,84 @@
+// common.cuh -- shared definitions of libargot_b200 (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/argot_b200.h"
+
+namespace argot {
+
+// Physical constants and flags exactly as the reference spells them
+// (constants.h, prim_chem/chemistry.h:25,286-314, calc_optical_depth.c:15).
+constexpr double kTiny = 1.0e-31;
+constexpr double kHeliumFact = 0.0811258278;
+constexpr double kPi = 3.1415926535897932384626433;
+constexpr double kHPlanck = 6.626e-27;
+constexpr double kNuL = 3.28e15;
+constexpr double kThrHI = 1.0, kThrHeI = 1.8125, kThrHeII = 4.0;
+constexpr int kNu = 256;
+
+// Rays are generated and consumed per block of 32 target cells.
+constexpr int kBlkX = 2, kBlkY = 4, kBlkZ = 4;
+
+// Thread-local status of the last API call (argot_b200_last_error).
+void set_status(int code);
+int status_from_cuda(cudaError_t e);
+
+#define ARGOT_CUDA_TRY(expr)                                   \
+  do {                                                         \
+    cudaError_t _e = (expr);                                   \
+    if (_e != cudaSuccess) return argot::status_from_cuda(_e); \
+  } while (0)
+
+// Geometry as the kernels see it (by value in kernel parameters).
+struct GridDev {
+  int nx, ny, nz;
+  int ix0, iy0, iz0;
+  float xmin, ymin, zmin, xmax, ymax, zmax;
+  float xminl, yminl, zminl;
+  float dx, dy, dz;
+  double lunit, denstonh;
+  int nbx, nby, nbz;  // blocks per axis
+};
+
+GridDev make_grid(const argot_b200_grid &g);
+bool grid_valid(const argot_b200_grid *g);
+
+// Tables in constant memory (filled once per device by ensure_tables()).
+struct RateTables {
+  float nu_f[kNu];        // (float) nu, as the reference compares it
+  float cs[3][kNu];       // sigma_s(nu) [cm^2]
+  float cs_l2e[3][kNu];   // sigma_s(nu) * log2(e)
+  float hw[3][kNu];       // sigma_s(nu) * max((float)nu - nu_s, 0)
+};
+// Uploads the tables to the constant bank of the translation unit that owns
+// the rate kernels (photoion.cu), once per device.
+int ensure_tables(int device);
+
+// Host copies of the tables (computed with the reference's formulas).
+void host_tables(double *nu, float *cs3);
+
+// Emitters and tree on the device.
+struct DevNode {
+  float cx, cy, cz, len;   // centre (float, as stored by the reference), side
+  int n;                   // number of sources below
+  int skip;                // preorder index after this subtree
+  int has_child;           // children follow at index+1 in preorder
+  int src_first;           // first entry of the leaf's source list
+};
+
+}  // namespace argot
+
+// Opaque handle bodies (C ABI types).
+struct argot_b200_dev_tree {
+  int device;
+  int n_nodes, n_src, n_emit;
+  float theta_sq;          // SQR(theta) in float, as the reference's walk
+  argot::DevNode *nodes;   // n_nodes (preorder)
+  int *src_list;           // n_src: source index per leaf slot
+  float4 *emit_pos;        // n_emit (x, y, z, 0)
+  double *emit_spec64;     // n_emit x 256
+  float *emit_specn;       // n_emit x 256: spectrum / total
+  double *emit_total;      // n_emit
+};

@@ -1,0 +1,494 @@
+// march.cu -- field packing, light-ray generation (tree walk), the segment
+// march (calc_optical_depth) and the stitching of segment columns
+// (accum_optical_depth) on sm_100a.
+#include <cub/device/device_scan.cuh>
+
+#include "march.cuh"
+#include "ref_layout.h"
+
+namespace argot {
+
+// ------------------------------------------------------------------ packing
+// cells[c] = {n_HI, n_HeI, n_HeII, 0} with the reference's per-crossing
+// products (calc_optical_depth.c:150-155): n_HI = dens*fHI in float,
+// n_He = (float)(dens * HELIUM_FACT) in double, n_HeI = n_He*fHeI in float.
+// raw[c] = {dens, fHI, fHeI, fHeII} for the rate stage, which forms its own
+// products in double (calc_photoion_rate.c:211-218).
+__global__ void k_pack_fields(uint64_t n, const float *__restrict__ dens, const float *__restrict__ fHI,
+                              const float *__restrict__ fHeI, const float *__restrict__ fHeII,
+                              float4 *__restrict__ cells, float4 *__restrict__ raw) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const float d = dens[i], a = fHI[i], b = fHeI[i], c = fHeII[i];
+    const float nhe = __double2float_rn(__dmul_rn((double)d, kHeliumFact));
+    cells[i] = make_float4(__fmul_rn(d, a), __fmul_rn(nhe, b), __fmul_rn(nhe, c), 0.f);
+    if (raw) raw[i] = make_float4(d, a, b, c);
+  }
+}
+
+__global__ void k_pack_mesh(uint64_t n, const fluid_mesh *__restrict__ mesh, float4 *__restrict__ cells,
+                            float4 *__restrict__ raw) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const float d = mesh[i].dens, a = mesh[i].chem.fHI, b = mesh[i].chem.fHeI, c = mesh[i].chem.fHeII;
+    const float nhe = __double2float_rn(__dmul_rn((double)d, kHeliumFact));
+    cells[i] = make_float4(__fmul_rn(d, a), __fmul_rn(nhe, b), __fmul_rn(nhe, c), 0.f);
+    if (raw) raw[i] = make_float4(d, a, b, c);
+  }
+}
+
+static int grid_blocks_for(uint64_t n, int threads) {
+  uint64_t b = (n + threads - 1) / threads;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const uint64_t cap = (uint64_t)sms * 16;
+  return (int)(b < cap ? (b ? b : 1) : cap);
+}
+
+// --------------------------------------------------------------- tree walk
+// One warp per block of 32 target cells.  The warp walks the preorder node
+// array once for all its lanes; a lane that accepts node v (r^2 theta^2 >
+// side^2, all in float as setup_light_ray_tree.c:341-354) records v's
+// subtree end and stays idle until the walk leaves that subtree.  A node is
+// opened when any lane needs it: internal nodes descend into their children
+// (octant order), leaves (<= 1 source) emit one ray per source.  Each lane
+// therefore sees the nodes in the reference's depth-first order and emits
+// its rays in the reference's order.
+template <bool kEmit>
+__global__ void __launch_bounds__(256) k_walk(GridDev g, const DevNode *__restrict__ nodes, int n_nodes,
+                                              const int *__restrict__ src_list, float theta_sq,
+                                              uint64_t b0, uint64_t b1, uint64_t *__restrict__ blk_count,
+                                              uint32_t *__restrict__ cell_count,
+                                              const uint64_t *__restrict__ blk_off, uint64_t base,
+                                              uint32_t *__restrict__ rays) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  for (uint64_t b = b0 + warp; b < b1; b += nwarp) {
+    int ix, iy, iz;
+    const bool valid = block_cell(g, b, lane, &ix, &iy, &iz);
+    const float px = cell_centre(g.xmin, g.ix0 + ix, g.dx);
+    const float py = cell_centre(g.ymin, g.iy0 + iy, g.dy);
+    const float pz = cell_centre(g.zmin, g.iz0 + iz, g.dz);
+    int blocked_until = 0;
+    uint32_t mine = 0;
+    uint64_t off = kEmit ? blk_off[b] - base : 0;
+    int cur = 0;
+    while (cur < n_nodes) {
+      const DevNode nd = nodes[cur];
+      const bool act = valid && cur >= blocked_until;
+      const float ddx = __fsub_rn(px, nd.cx), ddy = __fsub_rn(py, nd.cy), ddz = __fsub_rn(pz, nd.cz);
+      const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)), __fmul_rn(ddz, ddz));
+      const bool acc = act && (__fmul_rn(r2, theta_sq) > __fmul_rn(nd.len, nd.len));
+      const bool opn = act && !acc;
+      const unsigned macc = __ballot_sync(0xffffffffu, acc);
+      const unsigned mopn = __ballot_sync(0xffffffffu, opn);
+      if (macc) {
+        if (kEmit) {
+          if (acc) rays[off + __popc(macc & lt)] = ((uint32_t)cur << 5) | (uint32_t)lane;
+          off += __popc(macc);
+        } else {
+          mine += acc;
+        }
+      }
+      int next = nd.skip;
+      if (mopn) {
+        if (nd.n > 1) {
+          if (nd.has_child) {
+            if (acc) blocked_until = nd.skip;
+            next = cur + 1;
+          }
+        } else {
+          for (int j = 0; j < nd.n; j++) {
+            const uint32_t e = (uint32_t)(n_nodes + src_list[nd.src_first + j]);
+            if (kEmit) {
+              if (opn) rays[off + __popc(mopn & lt)] = (e << 5) | (uint32_t)lane;
+              off += __popc(mopn);
+            } else {
+              mine += opn;
+            }
+          }
+        }
+      }
+      cur = next;
+    }
+    if (!kEmit) {
+      if (cell_count && valid) cell_count[cell_index(g, ix, iy, iz)] = mine;
+      uint32_t tot = mine;
+      for (int o = 16; o; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+      if (lane == 0) blk_count[b] = tot;
+    }
+  }
+}
+
+// -------------------------------------------------------------- ray march
+// One warp per target block; the warp takes the block's rays 32 at a time.
+// Consecutive rays of a block come from the same emitter and end in
+// neighbouring cells, so the 32 lanes march nearly parallel paths of nearly
+// equal length and their gathers hit the same cache lines.
+template <int kPrec>
+__global__ void __launch_bounds__(256) k_march_rays(GridDev g, const float4 *__restrict__ cells,
+                                                    const float4 *__restrict__ emit_pos, uint64_t b0,
+                                                    uint64_t b1, const uint64_t *__restrict__ blk_off,
+                                                    uint64_t base, const uint32_t *__restrict__ rays,
+                                                    uint64_t nray, float *__restrict__ tau,
+                                                    unsigned long long *__restrict__ crossings,
+                                                    int *__restrict__ err) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long steps_total = 0;
+  bool bad = false;
+  for (uint64_t b = b0 + warp; b < b1; b += nwarp) {
+    const uint64_t r0 = blk_off[b] - base, r1 = blk_off[b + 1] - base;
+    int bix, biy, biz;
+    block_cell(g, b, 0, &bix, &biy, &biz);
+    for (uint64_t r = r0 + lane; r < r1; r += 32) {
+      const uint32_t w = __ldg(rays + r);
+      const uint32_t e = w >> 5;
+      const int l = (int)(w & 31u);
+      const int gx = g.ix0 + bix + (l >> 4), gy = g.iy0 + biy + ((l >> 2) & 3), gz = g.iz0 + biz + (l & 3);
+      const float xe = cell_centre(g.xmin, gx, g.dx);
+      const float ye = cell_centre(g.ymin, gy, g.dy);
+      const float ze = cell_centre(g.zmin, gz, g.dz);
+      const float4 ep = __ldg(emit_pos + e);
+      float xs, ys, zs;
+      ray_start(g, ep.x, ep.y, ep.z, xe, ye, ze, &xs, &ys, &zs);
+      int steps = 0;
+      const Tau3 t = (kPrec == ARGOT_B200_PRECISION_REFERENCE)
+                         ? march_reference(g, cells, xs, ys, zs, xe, ye, ze, &steps, &bad)
+                         : march_kahan(g, cells, xs, ys, zs, xe, ye, ze, &steps, &bad);
+      tau[r] = t.hi;
+      tau[nray + r] = t.hei;
+      tau[2 * nray + r] = t.heii;
+      steps_total += (unsigned long long)steps;
+    }
+  }
+  if (crossings) {
+    for (int o = 16; o; o >>= 1) steps_total += __shfl_xor_sync(0xffffffffu, steps_total, o);
+    if (lane == 0 && steps_total) atomicAdd(crossings, steps_total);
+  }
+  if (bad) atomicExch(err, 1);
+}
+
+// -------------------------------------------------------- explicit segments
+template <int kPrec>
+__global__ void k_march_segments(GridDev g, const float4 *__restrict__ cells, uint64_t nseg,
+                                 const float *__restrict__ pos6, float *__restrict__ tau3,
+                                 int *__restrict__ err) {
+  bool bad = false;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nseg;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const float *p = pos6 + 6 * i;
+    int steps;
+    const Tau3 t = (kPrec == ARGOT_B200_PRECISION_REFERENCE)
+                       ? march_reference(g, cells, p[0], p[1], p[2], p[3], p[4], p[5], &steps, &bad)
+                       : march_kahan(g, cells, p[0], p[1], p[2], p[3], p[4], p[5], &steps, &bad);
+    tau3[3 * i + 0] = t.hi;
+    tau3[3 * i + 1] = t.hei;
+    tau3[3 * i + 2] = t.heii;
+  }
+  if (bad) atomicExch(err, 1);
+}
+
+// the reference's struct ray_segment array, in place (drop-in path)
+template <int kPrec>
+__global__ void k_march_aos(GridDev g, const float4 *__restrict__ cells, uint64_t nseg,
+                            ray_segment *__restrict__ seg, int *__restrict__ err) {
+  bool bad = false;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nseg;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    ray_segment &s = seg[i];
+    int steps;
+    const Tau3 t = (kPrec == ARGOT_B200_PRECISION_REFERENCE)
+                       ? march_reference(g, cells, s.xpos_start, s.ypos_start, s.zpos_start, s.xpos_end,
+                                         s.ypos_end, s.zpos_end, &steps, &bad)
+                       : march_kahan(g, cells, s.xpos_start, s.ypos_start, s.zpos_start, s.xpos_end,
+                                     s.ypos_end, s.zpos_end, &steps, &bad);
+    s.optical_depth_HI = t.hi;
+    s.optical_depth_HeI = t.hei;
+    s.optical_depth_HeII = t.heii;
+  }
+  if (bad) atomicExch(err, 1);
+}
+
+int launch_march_aos(const GridDev &g, const float4 *cells, uint64_t nseg, void *seg_dev, int prec,
+                     int *err_dev, cudaStream_t st) {
+  if (!nseg) return 0;
+  const int threads = 128;
+  const int blocks = grid_blocks_for(nseg, threads);
+  if (prec == ARGOT_B200_PRECISION_REFERENCE)
+    k_march_aos<ARGOT_B200_PRECISION_REFERENCE><<<blocks, threads, 0, st>>>(g, cells, nseg, (ray_segment *)seg_dev, err_dev);
+  else
+    k_march_aos<ARGOT_B200_PRECISION_KAHAN><<<blocks, threads, 0, st>>>(g, cells, nseg, (ray_segment *)seg_dev, err_dev);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int launch_pack_mesh(uint64_t n, const void *mesh, float4 *cells, float4 *raw, cudaStream_t st) {
+  if (!n) return 0;
+  k_pack_mesh<<<grid_blocks_for(n, 256), 256, 0, st>>>(n, (const fluid_mesh *)mesh, cells, raw);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+// ---------------------------------------------------------------- stitching
+// Segments sorted by ray index: one thread per ray boundary run.  Each run
+// of equal ray_indx is summed with Kahan compensation and written to its
+// ray; rays without segments are zeroed first.
+__global__ void k_zero3(uint64_t n, float *__restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < 3 * n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = 0.f;
+}
+
+__global__ void k_stitch(uint64_t nseg, const uint64_t *__restrict__ ray_indx,
+                         const float *__restrict__ seg_tau3, uint64_t nray, float *__restrict__ ray_tau3) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nseg;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t r = ray_indx[i];
+    if (i > 0 && ray_indx[i - 1] == r) continue;  // not the head of a run
+    if (r >= nray) continue;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
+    for (uint64_t j = i; j < nseg && ray_indx[j] == r; j++) {
+      kahan_add(s0, c0, seg_tau3[3 * j + 0]);
+      kahan_add(s1, c1, seg_tau3[3 * j + 1]);
+      kahan_add(s2, c2, seg_tau3[3 * j + 2]);
+    }
+    ray_tau3[3 * r + 0] = s0;
+    ray_tau3[3 * r + 1] = s1;
+    ray_tau3[3 * r + 2] = s2;
+  }
+}
+
+// per-device scratch: an error flag and a counter
+struct DevScratch {
+  int *err = nullptr;
+};
+static DevScratch g_scratch[64];
+
+int *err_flag(int dev) {
+  if (dev < 0 || dev >= 64) return nullptr;
+  if (!g_scratch[dev].err) {
+    if (cudaMalloc(&g_scratch[dev].err, sizeof(int)) != cudaSuccess) return nullptr;
+    cudaMemset(g_scratch[dev].err, 0, sizeof(int));
+  }
+  return g_scratch[dev].err;
+}
+
+// Reads and clears the device error flag (synchronises the stream).
+int check_err_flag(int *flag, cudaStream_t st) {
+  int h = 0;
+  ARGOT_CUDA_TRY(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+  ARGOT_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h) {
+    cudaMemsetAsync(flag, 0, sizeof(int), st);
+    set_status(ARGOT_B200_EDEVICE);
+    return ARGOT_B200_EDEVICE;
+  }
+  return 0;
+}
+
+}  // namespace argot
+
+using namespace argot;
+
+extern "C" {
+
+int argot_b200_pack_fields(const argot_b200_grid *gp, const float *dens, const float *fHI,
+                           const float *fHeI, const float *fHeII, void *packed_dev, void *stream) {
+  if (!grid_valid(gp) || !dens || !fHI || !fHeI || !fHeII || !packed_dev) {
+    set_status(ARGOT_B200_EINVAL);
+    return ARGOT_B200_EINVAL;
+  }
+  const uint64_t n = (uint64_t)gp->nx * gp->ny * gp->nz;
+  float4 *cells = (float4 *)packed_dev;
+  k_pack_fields<<<grid_blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(n, dens, fHI, fHeI, fHeII,
+                                                                          cells, cells + n);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  set_status(0);
+  return 0;
+}
+
+int argot_b200_pack_fluid_mesh(const argot_b200_grid *gp, const void *mesh_dev, void *packed_dev,
+                               void *stream) {
+  if (!grid_valid(gp) || !mesh_dev || !packed_dev) {
+    set_status(ARGOT_B200_EINVAL);
+    return ARGOT_B200_EINVAL;
+  }
+  const uint64_t n = (uint64_t)gp->nx * gp->ny * gp->nz;
+  float4 *cells = (float4 *)packed_dev;
+  int rc = launch_pack_mesh(n, mesh_dev, cells, cells + n, (cudaStream_t)stream);
+  set_status(rc);
+  return rc;
+}
+
+int argot_b200_num_blocks(const argot_b200_grid *gp, uint64_t *nblocks) {
+  if (!grid_valid(gp) || !nblocks) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
+  GridDev g = make_grid(*gp);
+  *nblocks = (uint64_t)g.nbx * g.nby * g.nbz;
+  set_status(0);
+  return 0;
+}
+
+int argot_b200_count_rays(const argot_b200_grid *gp, const argot_b200_dev_tree *t, uint64_t b0,
+                          uint64_t b1, uint64_t *blk_count, uint32_t *cell_count, void *stream) {
+  uint64_t nb = 0;
+  if (!grid_valid(gp) || !t || !blk_count || argot_b200_num_blocks(gp, &nb) || b0 > b1 || b1 > nb) {
+    set_status(ARGOT_B200_EINVAL);
+    return ARGOT_B200_EINVAL;
+  }
+  if (b0 == b1) { set_status(0); return 0; }
+  GridDev g = make_grid(*gp);
+  const int threads = 256;
+  const int blocks = grid_blocks_for((b1 - b0) * 32, threads);
+  k_walk<false><<<blocks, threads, 0, (cudaStream_t)stream>>>(g, t->nodes, t->n_nodes, t->src_list,
+                                                              t->theta_sq, b0, b1, blk_count, cell_count,
+                                                              nullptr, 0, nullptr);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  set_status(0);
+  return 0;
+}
+
+int argot_b200_scan_blocks(const uint64_t *blk_count, uint64_t nb, uint64_t base, uint64_t *blk_off,
+                           uint64_t *total, void *stream) {
+  if (!blk_count || !blk_off) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
+  cudaStream_t st = (cudaStream_t)stream;
+  // blk_off[0] = base; blk_off[i+1] = base + sum(count[0..i])
+  ARGOT_CUDA_TRY(cudaMemcpyAsync(blk_off, &base, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+  if (nb) {
+    size_t tmp_bytes = 0;
+    ARGOT_CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, blk_count, blk_off + 1, (int64_t)nb, st));
+    void *tmp = nullptr;
+    ARGOT_CUDA_TRY(cudaMallocAsync(&tmp, tmp_bytes, st));
+    cudaError_t e = cub::DeviceScan::InclusiveSum(tmp, tmp_bytes, blk_count, blk_off + 1, (int64_t)nb, st);
+    cudaFreeAsync(tmp, st);
+    ARGOT_CUDA_TRY(e);
+    if (base) {
+      // shift by base (rare: group offsets are usually rebased by the caller)
+      uint64_t *h = (uint64_t *)malloc(sizeof(uint64_t) * (nb + 1));
+      if (!h) { set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
+      ARGOT_CUDA_TRY(cudaMemcpyAsync(h, blk_off, sizeof(uint64_t) * (nb + 1), cudaMemcpyDeviceToHost, st));
+      ARGOT_CUDA_TRY(cudaStreamSynchronize(st));
+      for (uint64_t i = 1; i <= nb; i++) h[i] += base;
+      cudaError_t e2 = cudaMemcpyAsync(blk_off, h, sizeof(uint64_t) * (nb + 1), cudaMemcpyHostToDevice, st);
+      if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(st);
+      free(h);
+      ARGOT_CUDA_TRY(e2);
+    }
+  }
+  if (total) {
+    ARGOT_CUDA_TRY(cudaMemcpyAsync(total, blk_off + nb, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    ARGOT_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  set_status(0);
+  return 0;
+}
+
+int argot_b200_emit_rays(const argot_b200_grid *gp, const argot_b200_dev_tree *t, uint64_t b0,
+                         uint64_t b1, const uint64_t *blk_off, uint64_t base, uint32_t *rays,
+                         void *stream) {
+  uint64_t nb = 0;
+  if (!grid_valid(gp) || !t || !blk_off || !rays || argot_b200_num_blocks(gp, &nb) || b0 > b1 || b1 > nb) {
+    set_status(ARGOT_B200_EINVAL);
+    return ARGOT_B200_EINVAL;
+  }
+  if (b0 == b1) { set_status(0); return 0; }
+  GridDev g = make_grid(*gp);
+  const int threads = 256;
+  const int blocks = grid_blocks_for((b1 - b0) * 32, threads);
+  k_walk<true><<<blocks, threads, 0, (cudaStream_t)stream>>>(g, t->nodes, t->n_nodes, t->src_list,
+                                                             t->theta_sq, b0, b1, nullptr, nullptr, blk_off,
+                                                             base, rays);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  set_status(0);
+  return 0;
+}
+
+int argot_b200_march_rays(const argot_b200_grid *gp, const void *packed, const argot_b200_dev_tree *t,
+                          uint64_t b0, uint64_t b1, const uint64_t *blk_off, uint64_t base,
+                          const uint32_t *rays, uint64_t nray, float *tau, int prec,
+                          unsigned long long *crossings, void *stream) {
+  uint64_t nb = 0;
+  if (!grid_valid(gp) || !packed || !t || !blk_off || (nray && (!rays || !tau)) ||
+      argot_b200_num_blocks(gp, &nb) || b0 > b1 || b1 > nb ||
+      (prec != ARGOT_B200_PRECISION_REFERENCE && prec != ARGOT_B200_PRECISION_KAHAN)) {
+    set_status(ARGOT_B200_EINVAL);
+    return ARGOT_B200_EINVAL;
+  }
+  if (b0 == b1) { set_status(0); return 0; }
+  int dev = 0;
+  ARGOT_CUDA_TRY(cudaGetDevice(&dev));
+  int *err = err_flag(dev);
+  if (!err) { set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
+  GridDev g = make_grid(*gp);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int threads = 256;
+  const int blocks = grid_blocks_for((b1 - b0) * 32, threads);
+  if (prec == ARGOT_B200_PRECISION_REFERENCE)
+    k_march_rays<ARGOT_B200_PRECISION_REFERENCE><<<blocks, threads, 0, st>>>(
+        g, (const float4 *)packed, t->emit_pos, b0, b1, blk_off, base, rays, nray, tau, crossings, err);
+  else
+    k_march_rays<ARGOT_B200_PRECISION_KAHAN><<<blocks, threads, 0, st>>>(
+        g, (const float4 *)packed, t->emit_pos, b0, b1, blk_off, base, rays, nray, tau, crossings, err);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  set_status(0);
+  return 0;
+}
+
+int argot_b200_march_segments(const argot_b200_grid *gp, const void *packed, uint64_t nseg,
+                              const float *pos6, float *tau3, int prec, void *stream) {
+  if (!grid_valid(gp) || !packed || (nseg && (!pos6 || !tau3)) ||
+      (prec != ARGOT_B200_PRECISION_REFERENCE && prec != ARGOT_B200_PRECISION_KAHAN)) {
+    set_status(ARGOT_B200_EINVAL);
+    return ARGOT_B200_EINVAL;
+  }
+  if (!nseg) { set_status(0); return 0; }
+  int dev = 0;
+  ARGOT_CUDA_TRY(cudaGetDevice(&dev));
+  int *err = err_flag(dev);
+  if (!err) { set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
+  GridDev g = make_grid(*gp);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int threads = 128;
+  const int blocks = grid_blocks_for(nseg, threads);
+  if (prec == ARGOT_B200_PRECISION_REFERENCE)
+    k_march_segments<ARGOT_B200_PRECISION_REFERENCE><<<blocks, threads, 0, st>>>(g, (const float4 *)packed,
+                                                                                 nseg, pos6, tau3, err);
+  else
+    k_march_segments<ARGOT_B200_PRECISION_KAHAN><<<blocks, threads, 0, st>>>(g, (const float4 *)packed,
+                                                                             nseg, pos6, tau3, err);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  int rc = check_err_flag(err, st);
+  set_status(rc);
+  return rc;
+}
+
+int argot_b200_stitch(uint64_t nseg, const uint64_t *ray_indx, const float *seg_tau3, uint64_t nray,
+                      float *ray_tau3, void *stream) {
+  if ((nseg && (!ray_indx || !seg_tau3)) || (nray && !ray_tau3)) {
+    set_status(ARGOT_B200_EINVAL);
+    return ARGOT_B200_EINVAL;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  if (nray) k_zero3<<<grid_blocks_for(3 * nray, 256), 256, 0, st>>>(nray, ray_tau3);
+  if (nseg) k_stitch<<<grid_blocks_for(nseg, 256), 256, 0, st>>>(nseg, ray_indx, seg_tau3, nray, ray_tau3);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  set_status(0);
+  return 0;
+}
+
+// Reads and clears the march error flag of the current device; returns
+// ARGOT_B200_EDEVICE if any march since the last check hit its step cap.
+int argot_b200_check_device_error(void *stream) {
+  int dev = 0;
+  ARGOT_CUDA_TRY(cudaGetDevice(&dev));
+  int *err = err_flag(dev);
+  if (!err) { set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
+  int rc = check_err_flag(err, (cudaStream_t)stream);
+  set_status(rc);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,260 @@
+// photoion.cu -- per-cell photo-ionisation and heating rates from the rays
+// of each target block (calc_photoion_rate on the device-resident layout).
+#include "photoion.cuh"
+#include "ref_layout.h"
+
+#include <mutex>
+
+namespace argot {
+
+int grid_blocks_for_rates(uint64_t n, int threads);
+
+int ensure_tables(int device) {
+  static std::mutex mu;
+  static bool done[64] = {false};
+  std::lock_guard<std::mutex> lock(mu);
+  if (device < 0 || device >= 64) return ARGOT_B200_EINVAL;
+  if (done[device]) return 0;
+  double nu[kNu];
+  float cs3[3 * kNu];
+  host_tables(nu, cs3);
+  RateTables t;
+  const double thr[3] = {kThrHI, kThrHeI, kThrHeII};
+  const double l2e = 1.4426950408889634074;
+  for (int i = 0; i < kNu; i++) {
+    const float nf = (float)nu[i];
+    t.nu_f[i] = nf;
+    for (int s = 0; s < 3; s++) {
+      const float c = cs3[3 * i + s];
+      t.cs[s][i] = c;
+      t.cs_l2e[s][i] = (float)((double)c * l2e);
+      const double w = ((double)nf > thr[s]) ? ((double)nf - thr[s]) : 0.0;
+      t.hw[s][i] = (float)((double)c * w);
+    }
+  }
+  ARGOT_CUDA_TRY(cudaMemcpyToSymbol(c_tab, &t, sizeof(t)));
+  done[device] = true;
+  return 0;
+}
+
+constexpr int kRateWarps = 4;  // warps per CTA in the block-rate kernel
+
+// One warp per target block.  Lanes compute the rates of 32 rays at a time
+// into shared memory; then lane j, which owns cell j of the block, adds the
+// contributions of the rays that end in its cell in ray order.  No atomics:
+// the result does not depend on scheduling.  EXACT_F64 adds to the existing
+// float value with the reference's float += double rounding per ray
+// (calc_photoion_rate.c:403-425); the other modes sum in double and store.
+template <int kMode>
+__global__ void __launch_bounds__(32 * kRateWarps)
+    k_rate_blocks(GridDev g, const float4 *__restrict__ raw, const float4 *__restrict__ emit_pos,
+                  const double *__restrict__ spec64, const float *__restrict__ specn,
+                  const double *__restrict__ total, uint64_t b0, uint64_t b1,
+                  const uint64_t *__restrict__ blk_off, uint64_t base, const uint32_t *__restrict__ rays,
+                  uint64_t nray, const float *__restrict__ tau, float *__restrict__ rates6) {
+  __shared__ double buf[kRateWarps][32][7];
+  __shared__ int tl[kRateWarps][32];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
+  for (uint64_t b = b0 + warp; b < b1; b += nwarp) {
+    int ix, iy, iz;
+    const bool own_valid = block_cell(g, b, lane, &ix, &iy, &iz);
+    const uint64_t own = own_valid ? cell_index(g, ix, iy, iz) : 0;
+    float accf[6];
+    double accd[6];
+#pragma unroll
+    for (int s = 0; s < 6; s++) {
+      accf[s] = (kMode == ARGOT_B200_RATE_EXACT_F64 && own_valid) ? rates6[s * ncell + own] : 0.f;
+      accd[s] = 0.0;
+    }
+    int bix, biy, biz;
+    block_cell(g, b, 0, &bix, &biy, &biz);
+    const uint64_t r0 = blk_off[b] - base, r1 = blk_off[b + 1] - base;
+    for (uint64_t rc = r0; rc < r1; rc += 32) {
+      const uint64_t r = rc + lane;
+      int t = -1;
+      if (r < r1) {
+        const uint32_t w = __ldg(rays + r);
+        const uint32_t e = w >> 5;
+        t = (int)(w & 31u);
+        const int lx = bix + (t >> 4), ly = biy + ((t >> 2) & 3), lz = biz + (t & 3);
+        const float4 ep = __ldg(emit_pos + e);
+        const RayGeom geo = ray_geometry(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z);
+        const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
+        const RayCols cols = ray_columns(g, __ldg(tau + r), __ldg(tau + nray + r), __ldg(tau + 2 * nray + r), rw, geo);
+        double out[6];
+        if (kMode == ARGOT_B200_RATE_EXACT_F64)
+          rate_bins_f64(cols, spec64 + (size_t)e * kNu, out);
+        else
+          rate_bins_f32(cols, specn + (size_t)e * kNu, __ldg(total + e), out);
+#pragma unroll
+        for (int s = 0; s < 6; s++) buf[wib][lane][s] = out[s];
+      }
+      tl[wib][lane] = t;
+      __syncwarp();
+      const int nk = (int)min((uint64_t)32, r1 - rc);
+      for (int k = 0; k < nk; k++) {
+        if (tl[wib][k] == lane) {
+#pragma unroll
+          for (int s = 0; s < 6; s++) {
+            if (kMode == ARGOT_B200_RATE_EXACT_F64)
+              accf[s] = __double2float_rn(__dadd_rn((double)accf[s], buf[wib][k][s]));
+            else
+              accd[s] += buf[wib][k][s];
+          }
+        }
+      }
+      __syncwarp();
+    }
+    if (own_valid) {
+#pragma unroll
+      for (int s = 0; s < 6; s++)
+        rates6[s * ncell + own] = (kMode == ARGOT_B200_RATE_EXACT_F64) ? accf[s] : (float)accd[s];
+    }
+  }
+}
+
+// ------------------------------------------------------------- drop-in rays
+// Per-ray rates of the reference's light_ray_IO array (one thread per ray).
+__global__ void k_rate_rayio(GridDev g, const float4 *__restrict__ raw, const light_ray_IO *__restrict__ rays,
+                             uint64_t nray, int rank_x, int rank_y, int rank_z, double *__restrict__ per6) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nray;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const light_ray_IO &r = rays[i];
+    const int lx = r.ix_target - rank_x * g.nx, ly = r.iy_target - rank_y * g.ny, lz = r.iz_target - rank_z * g.nz;
+    double out[6] = {0, 0, 0, 0, 0, 0};
+    if ((unsigned)lx < (unsigned)g.nx && (unsigned)ly < (unsigned)g.ny && (unsigned)lz < (unsigned)g.nz) {
+      const RayGeom geo = ray_geometry(g, r.ix_target, r.iy_target, r.iz_target, r.src.xpos, r.src.ypos, r.src.zpos);
+      const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
+      const RayCols cols = ray_columns(g, r.optical_depth_HI, r.optical_depth_HeI, r.optical_depth_HeII, rw, geo);
+      rate_bins_f64(cols, r.src.photon_rate, out);
+    }
+#pragma unroll
+    for (int s = 0; s < 6; s++) per6[6 * i + s] = out[s];
+  }
+}
+
+// Adds per-ray rates into mesh[].prev_chem in ray order.  One thread per run
+// of consecutive rays with the same target (the reference emits the rays of
+// a cell consecutively); each field is updated with a compare-and-swap so
+// that a cell appearing in several runs still receives every contribution.
+__device__ __forceinline__ void add_run(float *field, const double *per6, int s, uint64_t i0, uint64_t i1) {
+  unsigned int *addr = (unsigned int *)field;
+  unsigned int old = *((volatile unsigned int *)addr);
+  for (int attempt = 0; attempt < 1 << 20; attempt++) {
+    float v = __uint_as_float(old);
+    for (uint64_t i = i0; i < i1; i++) v = __double2float_rn(__dadd_rn((double)v, per6[6 * i + s]));
+    const unsigned int prev = atomicCAS(addr, old, __float_as_uint(v));
+    if (prev == old) return;
+    old = prev;
+  }
+}
+
+__global__ void k_accum_runs(GridDev g, const light_ray_IO *__restrict__ rays, uint64_t nray, int rank_x,
+                             int rank_y, int rank_z, const double *__restrict__ per6, fluid_mesh *__restrict__ mesh) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nray;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const int tx = rays[i].ix_target, ty = rays[i].iy_target, tz = rays[i].iz_target;
+    if (i > 0 && rays[i - 1].ix_target == tx && rays[i - 1].iy_target == ty && rays[i - 1].iz_target == tz)
+      continue;
+    uint64_t j = i + 1;
+    while (j < nray && rays[j].ix_target == tx && rays[j].iy_target == ty && rays[j].iz_target == tz) j++;
+    const int lx = tx - rank_x * g.nx, ly = ty - rank_y * g.ny, lz = tz - rank_z * g.nz;
+    if ((unsigned)lx >= (unsigned)g.nx || (unsigned)ly >= (unsigned)g.ny || (unsigned)lz >= (unsigned)g.nz) continue;
+    prim_chem &pc = mesh[cell_index(g, lx, ly, lz)].prev_chem;
+    add_run(&pc.GammaHI, per6, 0, i, j);
+    add_run(&pc.GammaHeI, per6, 1, i, j);
+    add_run(&pc.GammaHeII, per6, 2, i, j);
+    add_run(&pc.HeatHI, per6, 3, i, j);
+    add_run(&pc.HeatHeI, per6, 4, i, j);
+    add_run(&pc.HeatHeII, per6, 5, i, j);
+  }
+}
+
+__global__ void k_zero_rates(uint64_t n, fluid_mesh *__restrict__ mesh) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    prim_chem &pc = mesh[i].prev_chem;
+    pc.GammaHI = 0.f; pc.HeatHI = 0.f;
+    pc.GammaHeI = 0.f; pc.GammaHeII = 0.f;
+    pc.HeatHeI = 0.f; pc.HeatHeII = 0.f;
+  }
+}
+
+int launch_rate_rayio(const GridDev &g, const float4 *raw, const void *rays_io, uint64_t nray, int rx, int ry,
+                      int rz, double *per6, cudaStream_t st) {
+  if (!nray) return 0;
+  k_rate_rayio<<<grid_blocks_for_rates(nray, 128), 128, 0, st>>>(g, raw, (const light_ray_IO *)rays_io, nray, rx,
+                                                                  ry, rz, per6);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int launch_accum_runs(const GridDev &g, const void *rays_io, uint64_t nray, int rx, int ry, int rz,
+                      const double *per6, void *mesh, cudaStream_t st) {
+  if (!nray) return 0;
+  k_accum_runs<<<grid_blocks_for_rates(nray, 128), 128, 0, st>>>(g, (const light_ray_IO *)rays_io, nray, rx, ry,
+                                                                  rz, per6, (fluid_mesh *)mesh);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int launch_zero_rates(uint64_t n, void *mesh, cudaStream_t st) {
+  if (!n) return 0;
+  k_zero_rates<<<grid_blocks_for_rates(n, 256), 256, 0, st>>>(n, (fluid_mesh *)mesh);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int grid_blocks_for_rates(uint64_t n, int threads) {
+  uint64_t b = (n + threads - 1) / threads;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const uint64_t cap = (uint64_t)sms * 16;
+  return (int)(b < cap ? (b ? b : 1) : cap);
+}
+
+}  // namespace argot
+
+using namespace argot;
+
+extern "C" int argot_b200_photoion_rays(const argot_b200_grid *gp, const void *packed,
+                                        const argot_b200_dev_tree *t, uint64_t b0, uint64_t b1,
+                                        const uint64_t *blk_off, uint64_t base, const uint32_t *rays,
+                                        uint64_t nray, const float *tau, int mode, float *rates6,
+                                        void *stream) {
+  uint64_t nb = 0;
+  if (!grid_valid(gp) || !packed || !t || !blk_off || !rates6 || (nray && (!rays || !tau)) ||
+      argot_b200_num_blocks(gp, &nb) || b0 > b1 || b1 > nb) {
+    set_status(ARGOT_B200_EINVAL);
+    return ARGOT_B200_EINVAL;
+  }
+  if (mode != ARGOT_B200_RATE_EXACT_F64 && mode != ARGOT_B200_RATE_EXACT_F32) {
+    set_status(ARGOT_B200_ENOTSUP);
+    return ARGOT_B200_ENOTSUP;
+  }
+  if (b0 == b1) { set_status(0); return 0; }
+  int dev = 0;
+  ARGOT_CUDA_TRY(cudaGetDevice(&dev));
+  int rc = ensure_tables(dev);
+  if (rc) return rc;
+  GridDev g = make_grid(*gp);
+  const uint64_t ncell = (uint64_t)gp->nx * gp->ny * gp->nz;
+  const float4 *raw = (const float4 *)packed + ncell;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int threads = 32 * kRateWarps;
+  const int blocks = grid_blocks_for_rates((b1 - b0) * 32, threads);
+  if (mode == ARGOT_B200_RATE_EXACT_F64)
+    k_rate_blocks<ARGOT_B200_RATE_EXACT_F64><<<blocks, threads, 0, st>>>(
+        g, raw, t->emit_pos, t->emit_spec64, t->emit_specn, t->emit_total, b0, b1, blk_off, base, rays, nray, tau,
+        rates6);
+  else
+    k_rate_blocks<ARGOT_B200_RATE_EXACT_F32><<<blocks, threads, 0, st>>>(
+        g, raw, t->emit_pos, t->emit_spec64, t->emit_specn, t->emit_total, b0, b1, blk_off, base, rays, nray, tau,
+        rates6);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  set_status(0);
+  return 0;
+}

@@ -1,0 +1,164 @@
+// photoion.cuh -- per-ray photo-ionisation / heating rates
+// (calc_photoion_rate, photon-conserving branch, H + He, not cosmological).
+#pragma once
+#include "march.cuh"
+
+namespace argot {
+
+constexpr double kHNuL = kHPlanck * kNuL;  // hplanck*nuL, double
+
+// Frequency tables of the rate kernels (filled by ensure_tables).
+__constant__ RateTables c_tab;
+
+// Geometry shared by both precisions (calc_photoion_rate.c:176-246, FP32
+// where the reference uses float): target centre, distance, and the cell
+// chord `delta` along the ray (delta_length, :52-90).
+struct RayGeom {
+  float dist, delta;
+};
+
+__device__ __forceinline__ RayGeom ray_geometry(const GridDev &g, int gix, int giy, int giz, float sx,
+                                                float sy, float sz) {
+  // x = delta_x*((float)ix + 0.5) + xmin, in double, stored as float
+  const float x = __double2float_rn(__dadd_rn(__dmul_rn((double)g.dx, __dadd_rn((double)__int2float_rn(gix), 0.5)), (double)g.xmin));
+  const float y = __double2float_rn(__dadd_rn(__dmul_rn((double)g.dy, __dadd_rn((double)__int2float_rn(giy), 0.5)), (double)g.ymin));
+  const float z = __double2float_rn(__dadd_rn(__dmul_rn((double)g.dz, __dadd_rn((double)__int2float_rn(giz), 0.5)), (double)g.zmin));
+  const float dx = __fsub_rn(x, sx), dy = __fsub_rn(y, sy), dz = __fsub_rn(z, sz);
+  const float sxy = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+  const float s3 = __fadd_rn(sxy, __fmul_rn(dz, dz));
+  const float dl = __double2float_rn(__dsqrt_rn(__dadd_rn((double)s3, kTiny)));
+  const float dxy = __double2float_rn(__dsqrt_rn(__dadd_rn((double)sxy, kTiny)));
+  const float ct = __fdiv_rn(dz, dl), st = __fdiv_rn(dxy, dl);
+  const float cp = __fdiv_rn(dx, dxy), sp = __fdiv_rn(dy, dxy);
+  const float xo = cosine_guard(__fmul_rn(cp, st));
+  const float yo = cosine_guard(__fmul_rn(sp, st));
+  const float zo = cosine_guard(ct);
+  const float rx = fabsf(__fdiv_rn(g.dx, xo)), ry = fabsf(__fdiv_rn(g.dy, yo)), rz = fabsf(__fdiv_rn(g.dz, zo));
+  RayGeom r;
+  r.delta = fminf(rx, fminf(ry, rz));
+  r.dist = __double2float_rn(__dsqrt_rn((double)s3));
+  return r;
+}
+
+// Per-species quantities of the target cell for one ray (double):
+// the column to the cell's entry face N_s [cm^-2], the cell's own column
+// dN_s, and 1/(n_s V_shell + TINY).
+struct RayCols {
+  double N[3], dN[3], rN[3];
+};
+
+__device__ __forceinline__ RayCols ray_columns(const GridDev &g, float t_hi, float t_hei, float t_heii,
+                                               float4 raw, RayGeom geo) {
+  RayCols c;
+  const double cd = __dmul_rn(g.lunit, g.denstonh);
+  const double nH = __dmul_rn((double)raw.x, g.denstonh);
+  const double nHe = __dmul_rn(nH, kHeliumFact);
+  const double n[3] = {__dmul_rn(nH, (double)raw.y), __dmul_rn(nHe, (double)raw.z), __dmul_rn(nHe, (double)raw.w)};
+  const float tt[3] = {t_hi, t_hei, t_heii};
+  const double a = __dadd_rn((double)geo.dist, __dmul_rn(0.5, (double)geo.delta));
+  const double b = __dsub_rn((double)geo.dist, __dmul_rn(0.5, (double)geo.delta));
+  const double l3 = __dmul_rn(__dmul_rn(g.lunit, g.lunit), g.lunit);
+  const double vsh = __dmul_rn(__dmul_rn(4.0 * kPi / 3.0, __dsub_rn(__dmul_rn(__dmul_rn(a, a), a), __dmul_rn(__dmul_rn(b, b), b))), l3);
+#pragma unroll
+  for (int s = 0; s < 3; s++) {
+    c.dN[s] = __dmul_rn(__dmul_rn(n[s], (double)geo.delta), g.lunit);
+    c.N[s] = __dsub_rn(__dmul_rn((double)tt[s], cd), __dmul_rn(0.5, c.dN[s]));
+    c.rN[s] = __ddiv_rn(1.0, __dadd_rn(__dmul_rn(n[s], vsh), kTiny));
+  }
+  return c;
+}
+
+// The reference's 256-bin loop in FP64 with its operation order
+// (calc_photoion_rate.c:285-387); out[0..2] Gamma, out[3..5] Heat*h*nu_L.
+static __device__ __noinline__ void rate_bins_f64(const RayCols &c, const double *__restrict__ spec, double out[6]) {
+  double G0 = 0, G1 = 0, G2 = 0, H0 = 0, H1 = 0, H2 = 0;
+  for (int k = 0; k < kNu; k++) {
+    const float v = c_tab.nu_f[k];
+    const double s0 = (double)c_tab.cs[0][k], s1 = (double)c_tab.cs[1][k], s2 = (double)c_tab.cs[2][k];
+    double tau = __dmul_rn(c.N[0], s0);
+    double d0 = __dmul_rn(c.dN[0], s0);
+    double dtot = d0;
+    tau = __dadd_rn(tau, __dmul_rn(c.N[1], s1));
+    tau = __dadd_rn(tau, __dmul_rn(c.N[2], s2));
+    double d1 = __dmul_rn(c.dN[1], s1);
+    double d2 = __dmul_rn(c.dN[2], s2);
+    dtot = __dadd_rn(dtot, __dadd_rn(d1, d2));
+    const double pabs = __dmul_rn(__dmul_rn(__ldg(spec + k), exp(-tau)), __dsub_rn(1.0, exp(-dtot)));
+    const double den = __dadd_rn(dtot, kTiny);
+    d0 = __ddiv_rn(d0, den);
+    G0 = __dadd_rn(G0, __dmul_rn(__dmul_rn(d0, pabs), c.rN[0]));
+    if ((double)v > kThrHI) H0 = __dadd_rn(H0, __dmul_rn(__dmul_rn(__dmul_rn(d0, pabs), __dsub_rn((double)v, kThrHI)), c.rN[0]));
+    d1 = __ddiv_rn(d1, den);
+    d2 = __ddiv_rn(d2, den);
+    G1 = __dadd_rn(G1, __dmul_rn(__dmul_rn(d1, pabs), c.rN[1]));
+    G2 = __dadd_rn(G2, __dmul_rn(__dmul_rn(d2, pabs), c.rN[2]));
+    if ((double)v > kThrHeI) H1 = __dadd_rn(H1, __dmul_rn(__dmul_rn(__dmul_rn(d1, pabs), __dsub_rn((double)v, kThrHeI)), c.rN[1]));
+    if ((double)v > kThrHeII) H2 = __dadd_rn(H2, __dmul_rn(__dmul_rn(__dmul_rn(d2, pabs), __dsub_rn((double)v, kThrHeII)), c.rN[2]));
+  }
+  out[0] = G0; out[1] = G1; out[2] = G2;
+  out[3] = __dmul_rn(H0, kHNuL);
+  out[4] = __dmul_rn(H1, kHNuL);
+  out[5] = __dmul_rn(H2, kHNuL);
+}
+
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// (1 - e^-x)/x.  Below x = 0.1 the difference 1 - e^-x cancels, so the
+// value is taken in FP64 from its Taylor series (error < x^6/5040 < 2e-10);
+// above, FP32 with the hardware exponential is accurate to ~3e-6.
+__device__ __forceinline__ float phi_pc(float x, float e_minus_x) {
+  if (x < 0.1f) {
+    const double d = (double)x;
+    double p = fma(d, -1.0 / 720.0, 1.0 / 120.0);
+    p = fma(d, p, -1.0 / 24.0);
+    p = fma(d, p, 1.0 / 6.0);
+    p = fma(d, p, -0.5);
+    p = fma(d, p, 1.0);
+    return (float)p;
+  }
+  return (1.0f - e_minus_x) / x;
+}
+
+// FP32 rates: the same integral with the spectrum normalised by its total
+// (FP32 cannot hold photon rates of 1e50 or rates of 1e-58) and the FP64
+// per-ray prefactor total * dN_s * rN_s applied once.  Sums run in FP32 over
+// 32 bins and are carried in FP64 across blocks of bins.
+static __device__ __noinline__ void rate_bins_f32(const RayCols &c, const float *__restrict__ specn, double total,
+                                           double out[6]) {
+  const float N0 = (float)c.N[0], N1 = (float)c.N[1], N2 = (float)c.N[2];
+  const float D0 = (float)c.dN[0], D1 = (float)c.dN[1], D2 = (float)c.dN[2];
+  const float ln2 = 0.69314718055994531f;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int k0 = 0; k0 < kNu; k0 += 32) {
+    float g0 = 0.f, g1 = 0.f, g2 = 0.f, h0 = 0.f, h1 = 0.f, h2 = 0.f;
+#pragma unroll 8
+    for (int k = k0; k < k0 + 32; k++) {
+      const float a0 = c_tab.cs_l2e[0][k], a1 = c_tab.cs_l2e[1][k], a2 = c_tab.cs_l2e[2][k];
+      const float tl2 = fmaf(N0, a0, fmaf(N1, a1, N2 * a2));
+      const float dl2 = fmaf(D0, a0, fmaf(D1, a1, D2 * a2));
+      const float e = ex2_approx(-tl2);
+      const float ed = ex2_approx(-dl2);
+      const float w = __ldg(specn + k) * e * phi_pc(dl2 * ln2, ed);
+      g0 = fmaf(c_tab.cs[0][k], w, g0);
+      g1 = fmaf(c_tab.cs[1][k], w, g1);
+      g2 = fmaf(c_tab.cs[2][k], w, g2);
+      h0 = fmaf(c_tab.hw[0][k], w, h0);
+      h1 = fmaf(c_tab.hw[1][k], w, h1);
+      h2 = fmaf(c_tab.hw[2][k], w, h2);
+    }
+    acc[0] += g0; acc[1] += g1; acc[2] += g2;
+    acc[3] += h0; acc[4] += h1; acc[5] += h2;
+  }
+#pragma unroll
+  for (int s = 0; s < 3; s++) {
+    const double p = total * c.dN[s] * c.rN[s];
+    out[s] = p * acc[s];
+    out[3 + s] = p * acc[3 + s] * kHNuL;
+  }
+}
+
+}  // namespace argot

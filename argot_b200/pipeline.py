@@ -1,0 +1,217 @@
+"""Host-side driver of the device-resident path (Python over the C ABI).
+
+``Problem`` owns the device buffers of one mesh + source set (allocated
+through PyTorch, which is only the allocator and stream provider here) and
+runs the hot path through libargot_b200:
+
+    pack fields -> oct-tree (host) -> device walk: count, scan, emit rays
+    -> march (columns per ray) -> per-cell rates
+
+The rays of one target block are contiguous; ``groups`` bounds the ray
+buffer by processing contiguous ranges of target blocks, the device analogue
+of the reference's memory-bounded target groups
+(step_radiation_tree.c:235-308).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .workload import Workload, photon_rates
+
+
+def _p(t) -> int:
+    return 0 if t is None else t.data_ptr()
+
+
+def photon_counts(typ: int, param: float):
+    lib = L.load()
+    counts = np.zeros(256, np.float64)
+    norm = C.c_double()
+    lib.argot_b200_photon_counts(int(typ), float(param), counts.ctypes.data, C.byref(norm))
+    return counts, norm.value
+
+
+def tables():
+    lib = L.load()
+    nu = np.zeros(256, np.float64)
+    cs = np.zeros((256, 3), np.float32)
+    lib.argot_b200_tables(nu.ctypes.data, cs.ctypes.data)
+    return nu, cs
+
+
+def unit_box_grid(edge: int, lunit: float, denstonh: float) -> L.Grid:
+    d = float(np.float32(1.0) / np.float32(edge))
+    return L.Grid(edge, edge, edge, 0, 0, 0, 0.0, 0.0, 0.0, 1.0, 1.0, 1.0, 0.0, 0.0, 0.0,
+                  d, d, d, lunit, denstonh)
+
+
+@dataclass
+class RayGroup:
+    b0: int
+    b1: int
+    base: int
+    nray: int
+
+
+class Problem:
+    def __init__(self, wl: Workload, device: str | torch.device = "cuda:0",
+                 max_group_rays: int | None = None, host_fields=None):
+        """host_fields: optional pinned host tensors (dens, fHI, fHeI, fHeII)
+        copied asynchronously instead of the workload's numpy arrays."""
+        self.lib = L.load()
+        self.wl = wl
+        self.device = torch.device(device)
+        self.grid = unit_box_grid(wl.edge, wl.lunit, wl.denstonh)
+        self.ncell = wl.edge ** 3
+        self.spectra = photon_rates(photon_counts, wl.src_type, wl.src_param, wl.src_rate)
+        with torch.cuda.device(self.device):
+            self.stream = torch.cuda.current_stream(self.device)
+            if host_fields is not None:
+                self.fields = [t.to(self.device, non_blocking=True) for t in host_fields]
+            else:
+                self.fields = [torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
+                               for a in wl.fields()]
+            self.packed = torch.empty(8 * self.ncell, dtype=torch.float32, device=self.device)
+            self._tree = C.c_void_p()
+            self._dtree = C.c_void_p()
+            self._build_tree()
+            self.pack()
+            self._count_rays()
+        self.max_group_rays = max_group_rays
+        self.groups = self._make_groups(max_group_rays)
+
+    # ------------------------------------------------------------- setup
+    @property
+    def sp(self):
+        return C.c_void_p(self.stream.cuda_stream)
+
+    def pack(self):
+        d, a, b, c = (_p(t) for t in self.fields)
+        L.check(self.lib.argot_b200_pack_fields(C.byref(self.grid), d, a, b, c, _p(self.packed),
+                                                self.sp), "pack_fields")
+
+    def _build_tree(self):
+        pos = np.ascontiguousarray(self.wl.src_pos, np.float32)
+        spec = np.ascontiguousarray(self.spectra, np.float64)
+        L.check(self.lib.argot_b200_tree_build(C.byref(self.grid), len(pos), pos.ctypes.data,
+                                               spec.ctypes.data, float(self.wl.theta),
+                                               C.byref(self._tree)), "tree_build")
+        L.check(self.lib.argot_b200_dev_tree_upload(self._tree, C.byref(self._dtree), self.sp),
+                "dev_tree_upload")
+        self.n_nodes = self.lib.argot_b200_tree_num_nodes(self._tree)
+        self.n_emit = self.lib.argot_b200_tree_num_emitters(self._tree)
+
+    def emitters(self):
+        pos4 = np.zeros((self.n_emit, 4), np.float32)
+        spec = np.zeros((self.n_emit, 256), np.float64)
+        L.check(self.lib.argot_b200_tree_emitters(self._tree, pos4.ctypes.data, spec.ctypes.data),
+                "tree_emitters")
+        return pos4, spec
+
+    def _count_rays(self):
+        nb = C.c_uint64()
+        L.check(self.lib.argot_b200_num_blocks(C.byref(self.grid), C.byref(nb)), "num_blocks")
+        self.nblocks = nb.value
+        self.blk_count = torch.zeros(self.nblocks, dtype=torch.int64, device=self.device)
+        self.cell_count = torch.zeros(self.ncell, dtype=torch.int32, device=self.device)
+        L.check(self.lib.argot_b200_count_rays(C.byref(self.grid), self._dtree, 0, self.nblocks,
+                                               _p(self.blk_count), _p(self.cell_count), self.sp),
+                "count_rays")
+        self.blk_off = torch.zeros(self.nblocks + 1, dtype=torch.int64, device=self.device)
+        tot = C.c_uint64()
+        L.check(self.lib.argot_b200_scan_blocks(_p(self.blk_count), self.nblocks, 0,
+                                                _p(self.blk_off), C.byref(tot), self.sp),
+                "scan_blocks")
+        self.nray = tot.value
+        self.blk_off_host = self.blk_off.cpu().numpy()
+
+    def _make_groups(self, max_rays):
+        if not max_rays or self.nray <= max_rays:
+            return [RayGroup(0, self.nblocks, 0, self.nray)]
+        groups, b0 = [], 0
+        off = self.blk_off_host
+        while b0 < self.nblocks:
+            b1 = int(np.searchsorted(off, off[b0] + max_rays, side="right")) - 1
+            b1 = max(b1, b0 + 1)
+            b1 = min(b1, self.nblocks)
+            groups.append(RayGroup(b0, b1, int(off[b0]), int(off[b1] - off[b0])))
+            b0 = b1
+        return groups
+
+    def alloc_group_buffers(self, group: RayGroup | None = None):
+        n = max(g.nray for g in self.groups) if group is None else group.nray
+        rays = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
+        tau = torch.empty(3 * max(n, 1), dtype=torch.float32, device=self.device)
+        return rays, tau
+
+    def emit(self, group: RayGroup, rays):
+        L.check(self.lib.argot_b200_emit_rays(C.byref(self.grid), self._dtree, group.b0, group.b1,
+                                              _p(self.blk_off), group.base, _p(rays), self.sp),
+                "emit_rays")
+
+    def march(self, group: RayGroup, rays, tau, precision=L.PRECISION_KAHAN, crossings=None):
+        L.check(self.lib.argot_b200_march_rays(C.byref(self.grid), _p(self.packed), self._dtree,
+                                               group.b0, group.b1, _p(self.blk_off), group.base,
+                                               _p(rays), group.nray, _p(tau), int(precision),
+                                               _p(crossings), self.sp), "march_rays")
+
+    def rates(self, group: RayGroup, rays, tau, rates6, mode=L.RATE_EXACT_F32):
+        L.check(self.lib.argot_b200_photoion_rays(C.byref(self.grid), _p(self.packed), self._dtree,
+                                                  group.b0, group.b1, _p(self.blk_off), group.base,
+                                                  _p(rays), group.nray, _p(tau), int(mode),
+                                                  _p(rates6), self.sp), "photoion_rays")
+
+    def check_device_error(self):
+        L.check(self.lib.argot_b200_check_device_error(self.sp), "device error flag")
+
+    # ------------------------------------------------------------- whole pass
+    def run(self, precision=L.PRECISION_KAHAN, mode=L.RATE_EXACT_F32, rates6=None,
+            buffers=None, crossings=None, keep_rays=False):
+        """march + rates over every group; returns rates6 (6, ncell)."""
+        if rates6 is None:
+            rates6 = torch.zeros(6 * self.ncell, dtype=torch.float32, device=self.device)
+        rays, tau = buffers if buffers is not None else self.alloc_group_buffers()
+        for g in self.groups:
+            if len(self.groups) > 1 or not keep_rays:
+                self.emit(g, rays)
+            self.march(g, rays, tau, precision, crossings)
+            self.rates(g, rays, tau, rates6, mode)
+        return rates6
+
+    def close(self):
+        if self._dtree:
+            self.lib.argot_b200_dev_tree_free(self._dtree)
+            self._dtree = C.c_void_p()
+        if self._tree:
+            self.lib.argot_b200_tree_free(self._tree)
+            self._tree = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------- helpers
+    def ray_table(self, rays: torch.Tensor, group: RayGroup):
+        """Host view of a group's rays: (emitter, target cell (ix,iy,iz), block)."""
+        w = rays[:group.nray].cpu().numpy().view(np.uint32)
+        emit = (w >> 5).astype(np.int64)
+        lane = (w & 31).astype(np.int64)
+        off = self.blk_off_host
+        blk = np.repeat(np.arange(group.b0, group.b1), np.diff(off[group.b0:group.b1 + 1]))
+        e = self.wl.edge
+        nbz = (e + 3) // 4
+        nby = (e + 3) // 4
+        bx = blk // (nby * nbz)
+        by = (blk - bx * nby * nbz) // nbz
+        bz = blk - bx * nby * nbz - by * nbz
+        ix = bx * 2 + (lane >> 4)
+        iy = by * 4 + ((lane >> 2) & 3)
+        iz = bz * 4 + (lane & 3)
+        return emit, np.stack([ix, iy, iz], 1).astype(np.int32), blk

@@ -1,0 +1,415 @@
+"""Benchmark of the ARGOT point-source RT hot path on B200.
+
+One step = one pass of the hot path over one synthetic workload with its
+inputs resident in HBM: the march of every light ray (calc_optical_depth,
+FP32 with Kahan columns), the stitching of columns into rays, and the
+per-cell photo-ionisation / heating rates (calc_photoion_rate; FP32 exact
+quadrature by default).  Rays are generated on the device by the tree walk
+before timing (the producer step of the path).
+
+Default workload: 256^3 lognormal mesh (sigma_ln 1.2), 4096 clustered
+sources, theta 0.5 -- the largest single-GPU configuration, on which the
+target throughput is quoted.  Inputs (13 GB of rays + a 268 MB field) are
+larger than the 126 MB L2, so no flush is needed between steps.
+
+metric: ray-cell crossings/s of the whole step; the JSON line also carries
+Gamma-cells/s, the per-kernel split, a roofline object for the march (HBM
+bound) and the reference's CPU path timed on a bounded sample.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W]
+                       [--impl ours|reference] [--config largest|plain|...]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+CONFIGS = ("largest", "plain", "precision", "learned", "tiny")
+METRIC = "ray-cell crossings/s (march+stitch+rates, 1 B200)"
+UNIT = "crossings/s"
+
+
+def make_workload(name: str, rank: int = 0):
+    from argot_b200 import workload as W
+    seed_shift = 1000 * rank
+    if name == "largest":
+        return W.largest(seed=5 + seed_shift)
+    if name == "plain":
+        return W.plain(seed=1 + seed_shift)
+    if name == "precision":
+        return W.precision(seed=2 + seed_shift)
+    if name == "learned":
+        return W.learned(seed=4 + seed_shift)
+    if name == "tiny":
+        return W.tiny(32, 16, seed=7 + seed_shift)
+    raise ValueError(name)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+# ------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clocks and throttle
+    reasons); reading settings only."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ distributed
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def init_dist(ws, backend):
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(ws, x: float, device=None) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allsum(ws, x: float, device=None) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_sample(wl, target_seconds: float = 15.0, max_cells: int = 4096, threads: int | None = None,
+               seed: int = 0):
+    """ARGOT's own C (the reference build for this mesh edge) on a bounded,
+    seeded sample of target cells: one contiguous group of target cells,
+    the reference's own grouping unit.  Returns crossings/s over the hot
+    path (calc_optical_depth + accum_optical_depth + calc_photoion_rate)."""
+    from oracle.oracle import Oracle, RefLib, unit_box_grid
+    threads = threads or os.cpu_count() or 1
+    R = RefLib(wl.edge)
+    R.init(wl.lunit, wl.denstonh, wl.theta, threads)
+    R.set_mesh(*wl.fields())
+    R.set_sources(wl.src_type, wl.src_param, wl.src_pos, wl.src_rate)
+    rng = np.random.default_rng(seed)
+    ncell = wl.edge ** 3
+    # size the group by a short probe, then run it
+    ncells = 64
+    im0 = int(rng.integers(0, ncell - max_cells))
+    R.zero_rates()
+    t0 = time.time()
+    probe = R.run_range(im0, im0 + ncells, True, want=("seg",))
+    dt = max(time.time() - t0, 1e-3)
+    ncells = int(min(max_cells, max(64, ncells * target_seconds / dt)))
+    R.zero_rates()
+    out = R.run_range(im0, im0 + ncells, True, want=("seg",))
+    times = out["times"]
+    o = Oracle()
+    cross = float(o.count_crossings(unit_box_grid(wl.edge, wl.lunit, wl.denstonh), out["seg"]).sum())
+    hot = float(times[1] + times[2] + times[3])
+    return {"value": cross / hot, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": (f"{ncells} consecutive target cells from index {im0} of {wl.name} "
+                       f"({out['nray']} rays, {cross:.3e} crossings); hot-path wall "
+                       f"{hot:.2f} s (march {times[1]:.2f}, accum {times[2]:.3f}, "
+                       f"rates {times[3]:.2f})"),
+            "march_crossings_per_s": cross / times[1] if times[1] > 0 else None,
+            "gamma_cells_per_s": ncells / times[3] if times[3] > 0 else None,
+            "_probe_rays": probe["nray"]}
+
+
+# ------------------------------------------------------------ our arm
+def run_ours(args):
+    import torch
+    from argot_b200 import _lib as L
+    from argot_b200.pipeline import Problem
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    init_dist(ws, "nccl")
+    dev = torch.device("cuda", local)
+    wl = make_workload(args.config, rank)
+    prec = L.PRECISION_KAHAN if args.precision == "kahan" else L.PRECISION_REFERENCE
+    mode = {"f32": L.RATE_EXACT_F32, "f64": L.RATE_EXACT_F64}[args.rate]
+
+    free, _ = torch.cuda.mem_get_info(dev)
+    pb = Problem(wl, dev, max_group_rays=None)
+    need = pb.nray * 16 + (1 << 30)
+    if need > free * 0.9:
+        pb.groups = pb._make_groups(int(free * 0.8 / 16))
+    stream = pb.stream
+    rays, tau = pb.alloc_group_buffers()
+    rates6 = torch.zeros(6 * pb.ncell, dtype=torch.float32, device=dev)
+    single = len(pb.groups) == 1
+    if single:
+        pb.emit(pb.groups[0], rays)
+    crossings = torch.zeros(1, dtype=torch.int64, device=dev)
+
+    def step(count=None):
+        for g in pb.groups:
+            if not single:
+                pb.emit(g, rays)
+            pb.march(g, rays, tau, prec, count)
+            pb.rates(g, rays, tau, rates6, mode)
+
+    # warm-up (the first one also counts the crossings)
+    for w in range(args.warmup):
+        step(crossings if w == 0 else None)
+    torch.cuda.synchronize()
+    pb.check_device_error()
+    n_cross = int(crossings.item())
+
+    # per-kernel split (one extra pass, events around each kernel)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(stream)
+    for g in pb.groups:
+        if not single:
+            pb.emit(g, rays)
+        pb.march(g, rays, tau, prec)
+    ev[1].record(stream)
+    for g in pb.groups:
+        pb.rates(g, rays, tau, rates6, mode)
+    ev[2].record(stream)
+    torch.cuda.synchronize()
+    t_march = ev[0].elapsed_time(ev[1]) / 1e3
+    t_rates = ev[1].elapsed_time(ev[2]) / 1e3
+
+    clocks = ClockSampler(local)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    pb.check_device_error()
+    t_local = e0.elapsed_time(e1) / 1e3
+    t = allmax(ws, t_local, dev)
+    total_cross = allsum(ws, float(n_cross) * args.steps, dev)
+    total_cells = allsum(ws, float(pb.ncell) * args.steps, dev)
+
+    hbm, bf16, peak_kind = measured_peaks()
+    alg_bytes = 16.0 * n_cross + 36.0 * pb.nray
+    achieved = alg_bytes / t_march / 1e9
+    launches_per_step = len(pb.groups) * (2 + (0 if single else 1))
+
+    # end to end through the C ABI from pinned host buffers
+    e2e = run_e2e(wl, dev, prec, mode, steps=max(1, min(args.steps, 3))) if not args.no_e2e else None
+
+    line = {
+        "metric": METRIC, "value": total_cross / t, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded lognormal mesh + clustered sources)",
+        "config": {"workload": wl.name, "mesh": f"{wl.edge}^3", "sources": wl.nsrc,
+                   "theta": wl.theta, "rays": pb.nray, "crossings": n_cross,
+                   "march": args.precision, "rates": args.rate, "ray_groups": len(pb.groups),
+                   "l2": "inputs larger than L2 (13 GB rays, 268 MB field); no flush",
+                   "parallelism": f"{ws} independent problems (one per GPU)"},
+        "gamma_cells_per_s": total_cells / t,
+        "split": {"march_s": t_march, "rates_s": t_rates,
+                  "march_crossings_per_s": n_cross / t_march,
+                  "rates_gamma_cells_per_s": pb.ncell / t_rates,
+                  "rates_rays_per_s": pb.nray / t_rates},
+        "roofline": {"kernel": "k_march_rays", "bound": "hbm", "achieved": achieved,
+                     "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_kind": f"{peak_kind} hbm_gbs", "traffic": None,
+                     "algorithmic_bytes": alg_bytes,
+                     "bytes_model": "16 B per crossing + 36 B per ray"},
+        "clocks": clk,
+        "gpu_launches": launches_per_step * args.steps,
+    }
+    if e2e is not None:
+        line["e2e"] = e2e
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            cb = cpu_sample(wl, target_seconds=args.cpu_seconds)
+            cb.pop("_probe_rays", None)
+            line["cpu_baseline"] = cb
+        except Exception as exc:  # the baseline must not hide our own number
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(),
+                                    "kind": "reference", "sample": f"failed: {exc}"}
+    pb.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_e2e(wl, dev, prec, mode, steps=2):
+    """Same metric through the public C ABI with host buffers: each step
+    copies the mesh fields and the source table from pinned host memory,
+    builds the tree, generates the rays on the device, marches, computes the
+    rates and copies the six rate fields back to pinned host memory."""
+    import torch
+    from argot_b200.pipeline import Problem
+    pin = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in wl.fields()]
+    out = torch.empty(6 * wl.ncell, dtype=torch.float32).pin_memory()
+    h2d = sum(p.numel() * 4 for p in pin) + wl.nsrc * (12 + 8 + 8)
+    times = []
+    cross = None
+    for s in range(steps + 1):  # first pass warms the caching allocator
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pb = Problem(wl, dev, host_fields=pin)
+        rays, tau = pb.alloc_group_buffers()
+        rates6 = torch.zeros(6 * pb.ncell, dtype=torch.float32, device=dev)
+        cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        for g in pb.groups:
+            pb.emit(g, rays)
+            pb.march(g, rays, tau, prec, cnt)
+            pb.rates(g, rays, tau, rates6, mode)
+        out.copy_(rates6, non_blocking=True)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        cross = int(cnt.item())
+        pb.close()
+        del rays, tau
+        if s > 0:
+            times.append(dt)
+    t = statistics.median(times)
+    return {"value": cross / t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(out.numel() * 4), "s_per_step": t,
+            "includes": "H2D fields, host tree, device ray generation, march, rates, D2H rates"}
+
+
+# ------------------------------------------------------------ reference arm
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    wl = make_workload(args.config, 0)
+    vals = []
+    info = None
+    for s in range(args.warmup + args.steps):
+        r = cpu_sample(wl, target_seconds=args.ref_seconds, seed=s)
+        if s >= args.warmup:
+            vals.append(r["value"])
+            info = r
+    v = statistics.median(vals)
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "impl": "reference",
+        "data": "synthetic (seeded lognormal mesh + clustered sources)",
+        "config": {"workload": wl.name, "mesh": f"{wl.edge}^3", "sources": wl.nsrc,
+                   "theta": wl.theta},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"], "kind": "reference",
+                         "sample": info["sample"] + " (per step; median over steps)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser(description=__doc__,
+                                formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    p.add_argument("--config", choices=CONFIGS, default="largest")
+    p.add_argument("--precision", choices=("kahan", "reference"), default="kahan")
+    p.add_argument("--rate", choices=("f32", "f64"), default="f32")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--ref-seconds", type=float, default=15.0)
+    args = p.parse_args(argv)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,273 @@
+/*
+ * argot_b200.h -- C ABI of libargot_b200.so, a B200 (sm_100a) implementation
+ * of ARGOT's point-source radiative-transfer hot path:
+ *
+ *   calc_optical_depth   per-segment mesh march -> HI/HeI/HeII columns
+ *   accum_optical_depth  stitching of segment columns into light rays
+ *   calc_photoion_rate   256-bin photo-ionisation / heating integral per cell
+ *
+ * Two layers are exported.
+ *
+ * 1. Drop-in entry points with the reference's exact names and signatures
+ *    (ARGOT src/prototype.h).  The reference's structs are only
+ *    forward-declared here, so a C host that includes ARGOT's own headers can
+ *    include this file too; the library was compiled against byte-identical
+ *    mirrors of those structs for the reference's default flag set
+ *    (-D__HELIUM__ -D__PHOTON_CONSERVING__, no __HYDROGEN_MOL__, no
+ *    __COSMOLOGICAL__, NGRID_NU=256, NSEG_PER_RAY=5, NMAX_CUDA_DEV=4), and
+ *    argot_b200_abi_check() verifies a caller's struct sizes at run time.
+ *    Mesh dimensions are read from run_param at run time, so one library
+ *    serves every NMESH_* build.  These entry points use GPU 0 of the
+ *    caller's cuda_param (one rank, one GPU).
+ *
+ * 2. A device-resident API (argot_b200_*): plain pointers, sizes and a CUDA
+ *    stream; caller-owned device buffers; no reference structs.  This is the
+ *    B200 fast path (rays held as 4-byte words, target-blocked, emitter
+ *    spectra by index), used by the benchmark and callable from any host
+ *    language through the C ABI.
+ *
+ * Every argot_b200_* function returns 0 on success or a negative
+ * ARGOT_B200_E* code; the drop-in void functions record their status, which
+ * argot_b200_last_error() returns.  No function traps the device.
+ */
+#ifndef ARGOT_B200_H
+#define ARGOT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define ARGOT_B200_API __attribute__((visibility("default")))
+#else
+#define ARGOT_B200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define ARGOT_B200_OK 0
+#define ARGOT_B200_EINVAL (-1)      /* bad argument / size / layout         */
+#define ARGOT_B200_ECUDA (-2)       /* a CUDA runtime call failed           */
+#define ARGOT_B200_ENOMEM (-3)      /* device or pinned allocation failed   */
+#define ARGOT_B200_EDEVICE (-4)     /* a kernel reported an internal error  */
+#define ARGOT_B200_ENOTSUP (-5)     /* option not supported                 */
+
+/* status of the last call made by this host thread */
+ARGOT_B200_API int argot_b200_last_error(void);
+ARGOT_B200_API const char *argot_b200_error_string(int code);
+
+/* library / ABI identification */
+ARGOT_B200_API const char *argot_b200_version(void);
+/* sizes[10]: ray_segment, light_ray, light_ray_IO, radiation_src,
+ * fluid_mesh, prim_chem, run_param, cross_section, freq_param,
+ * photoion_rate as the library was compiled */
+ARGOT_B200_API void argot_b200_struct_sizes(uint64_t *sizes);
+/* returns 0 when the caller's sizeof() values (same order) match */
+ARGOT_B200_API int argot_b200_abi_check(const uint64_t *caller_sizes, int n);
+
+/* ============================================================ 1. drop-in */
+struct ray_segment;
+struct light_ray;
+struct light_ray_IO;
+struct fluid_mesh;
+struct run_param;
+struct cuda_mem_space;
+struct cuda_param;
+struct omp_param;
+
+/* Replaces src/calc_optical_depth_cuda.cu:29-144 (declared at
+ * src/prototype.h:152).  Overwrites seg[0..run->nseg).optical_depth_* in
+ * host memory before returning.  Reads the mesh from
+ * cuda_mem[0].mesh_dev (device AoS struct fluid_mesh, filled by the caller's
+ * send_mesh_data) and the domain geometry from *this_run (host copy). */
+ARGOT_B200_API void calc_optical_depth_cuda(struct ray_segment *seg, struct cuda_mem_space *cuda_mem,
+                             struct cuda_param *this_cuda, struct run_param *this_run);
+
+/* Replaces src/calc_photoion_rate_cuda.cu:92-216 (src/prototype.h:153).
+ * Fills ray_IO from ray as the reference does, and ADDS each ray's rates to
+ * cuda_mem[0].mesh_dev[target].prev_chem.{Gamma,Heat}{HI,HeI,HeII}. */
+ARGOT_B200_API void calc_photoion_rate_cuda(struct cuda_mem_space *cuda_mem, struct light_ray *ray,
+                             struct light_ray_IO *ray_IO, struct cuda_param *this_cuda,
+                             struct run_param *this_run);
+
+/* Replaces src/calc_photoion_rate_cuda.cu:45-62 (src/prototype.h:121). */
+ARGOT_B200_API void zero_out_photoion_rate_cuda(struct cuda_mem_space *cuda_mem,
+                                 struct cuda_param *this_cuda, struct run_param *this_run);
+
+/* Replaces src/accum_optical_depth.c:14-167 (src/prototype.h:75) for a
+ * single-rank run: every segment's columns go to ray[seg.ray_indx], rays
+ * without a segment get zero.  A host routine (the columns are already in
+ * host memory after calc_optical_depth_cuda).  An executable that still
+ * links the reference's accum_optical_depth.o keeps using its own: the
+ * executable's definition takes precedence over the shared library's. */
+ARGOT_B200_API void accum_optical_depth(struct light_ray *ray, struct ray_segment *seg,
+                         struct run_param *this_run, struct omp_param *this_omp);
+
+/* Arithmetic mode of the drop-in march: ARGOT_B200_MARCH_REFERENCE (default)
+ * reproduces the reference's FP32 operation order bit for bit;
+ * ARGOT_B200_MARCH_KAHAN uses the parametric FP32 march with compensated
+ * column sums (closer to an FP64 evaluation). */
+#define ARGOT_B200_MARCH_REFERENCE 0
+#define ARGOT_B200_MARCH_KAHAN 1
+ARGOT_B200_API int argot_b200_set_dropin_march_mode(int mode);
+
+/* ================================================= 2. device-resident API */
+
+/* Domain geometry of one rank, in the reference's terms (run_param). */
+typedef struct argot_b200_grid {
+  int nx, ny, nz;                  /* local cells per axis                  */
+  int ix0, iy0, iz0;               /* global index of local cell (0,0,0)    */
+  float xmin, ymin, zmin;          /* global box lower corner               */
+  float xmax, ymax, zmax;          /* global box upper corner               */
+  float xmin_local, ymin_local, zmin_local;
+  float dx, dy, dz;                /* cell size                             */
+  double lunit;                    /* length unit [cm]                      */
+  double denstonh;                 /* code density -> n_H [cm^-3]           */
+} argot_b200_grid;
+
+/* Packed cell fields (32 bytes per cell, 16-byte aligned): first ncell
+ * float4 {n_HI, n_HeI, n_HeII, 0} in code density units, the products
+ * rounded exactly as the reference forms them per crossing
+ * (calc_optical_depth.c:150-155) -- the march reads only these; then ncell
+ * float4 {dens, fHI, fHeI, fHeII}, read by the rate stage at the target
+ * cell.  Cell index iz + nz*(iy + ny*ix). */
+
+/* from separate device arrays (dens, fHI, fHeI, fHeII: ncell floats each) */
+ARGOT_B200_API int argot_b200_pack_fields(const argot_b200_grid *g, const float *dens, const float *fHI,
+                           const float *fHeI, const float *fHeII, void *packed_dev,
+                           void *stream);
+/* from a device array of the reference's struct fluid_mesh (156 B/cell) */
+ARGOT_B200_API int argot_b200_pack_fluid_mesh(const argot_b200_grid *g, const void *mesh_dev,
+                               void *packed_dev, void *stream);
+
+/* ---- emitters (tree nodes and sources) and the oct-tree ---------------- */
+
+/* Host-side oct-tree over the sources, built as the reference's
+ * construct_tree (setup_light_ray_tree.c:465-571): Morton keys of 21 bits
+ * per axis, luminosity-weighted centres, summed spectra.  The tree is then
+ * uploaded and walked on the device. */
+typedef struct argot_b200_tree argot_b200_tree;
+
+/* src_pos: nsrc x 3 floats; spectra: nsrc x 256 photon rates [s^-1 per bin]
+ * (setup_photon_rate output); theta: opening angle. */
+ARGOT_B200_API int argot_b200_tree_build(const argot_b200_grid *g, int nsrc, const float *src_pos,
+                          const double *spectra, float theta, argot_b200_tree **out);
+ARGOT_B200_API void argot_b200_tree_free(argot_b200_tree *t);
+/* number of emitters = tree nodes + sources; nodes come first */
+ARGOT_B200_API int argot_b200_tree_num_emitters(const argot_b200_tree *t);
+ARGOT_B200_API int argot_b200_tree_num_nodes(const argot_b200_tree *t);
+/* emitter table for the kernels, host side:
+ *   pos4:     n_emit x 4 floats (x, y, z, 0)
+ *   spec64:   n_emit x 256 doubles (photon rate per bin)
+ * either pointer may be NULL */
+ARGOT_B200_API int argot_b200_tree_emitters(const argot_b200_tree *t, float *pos4, double *spec64);
+
+/* Device copy of the walkable tree (nodes, leaf source lists) and of the
+ * emitter table; must be freed with argot_b200_dev_tree_free. */
+typedef struct argot_b200_dev_tree argot_b200_dev_tree;
+ARGOT_B200_API int argot_b200_dev_tree_upload(const argot_b200_tree *t, argot_b200_dev_tree **out,
+                               void *stream);
+ARGOT_B200_API void argot_b200_dev_tree_free(argot_b200_dev_tree *d);
+
+/* ---- light rays --------------------------------------------------------- */
+
+/* Rays are generated per BLOCK of 32 target cells (2 x 4 x 4 cells along
+ * x, y, z; lane = lz + 4*ly + 16*lx) by a warp-cooperative walk of the tree
+ * with the reference's opening test r^2 theta^2 > L^2
+ * (setup_light_ray_tree.c:321-395).  A ray is one 32-bit word
+ * (emitter << 5) | lane; a block's rays are contiguous, and the rays of one
+ * target cell appear in the reference's depth-first order.
+ * blk_offsets: nblocks+1 uint64 prefix offsets.  Blocks cover the local
+ * mesh in (bx, by, bz) order with bz fastest; cells outside the mesh in a
+ * partial block have no rays. */
+ARGOT_B200_API int argot_b200_num_blocks(const argot_b200_grid *g, uint64_t *nblocks);
+
+/* Pass 1: ray counts per block (blk_count: nblocks uint64) for blocks
+ * [b0, b1); optional per-cell counts (cell_count: ncell uint32, may be
+ * NULL). */
+ARGOT_B200_API int argot_b200_count_rays(const argot_b200_grid *g, const argot_b200_dev_tree *t,
+                          uint64_t b0, uint64_t b1, uint64_t *blk_count_dev,
+                          uint32_t *cell_count_dev, void *stream);
+/* exclusive prefix sum of blk_count[b0,b1) into blk_offsets[b0..b1] (device),
+ * starting at base; also returns the total on the host if total != NULL. */
+ARGOT_B200_API int argot_b200_scan_blocks(const uint64_t *blk_count_dev, uint64_t nb, uint64_t base,
+                           uint64_t *blk_offsets_dev, uint64_t *total, void *stream);
+/* Pass 2: write the ray words of blocks [b0, b1) at blk_offsets[b] - base. */
+ARGOT_B200_API int argot_b200_emit_rays(const argot_b200_grid *g, const argot_b200_dev_tree *t,
+                         uint64_t b0, uint64_t b1, const uint64_t *blk_offsets_dev,
+                         uint64_t base, uint32_t *rays_dev, void *stream);
+
+/* ---- march + stitch ----------------------------------------------------- */
+
+#define ARGOT_B200_PRECISION_REFERENCE 0  /* reference FP32 order, bit-exact */
+#define ARGOT_B200_PRECISION_KAHAN 1      /* parametric FP32, Kahan columns  */
+
+/* March every ray of blocks [b0, b1): columns (code units) of HI, HeI, HeII
+ * from the ray's start (the emitter, clipped to the box as in
+ * calc_ray_segment.c:107-126) to the target cell centre.  tau_dev: 3 floats
+ * per ray, SoA planes of length nray_group (tau[s*nray_group + r], r
+ * relative to base).  crossings (optional, device uint64[1]) receives the
+ * number of ray-cell crossings. */
+ARGOT_B200_API int argot_b200_march_rays(const argot_b200_grid *g, const void *packed_dev,
+                          const argot_b200_dev_tree *t, uint64_t b0, uint64_t b1,
+                          const uint64_t *blk_offsets_dev, uint64_t base,
+                          const uint32_t *rays_dev, uint64_t nray_group, float *tau_dev,
+                          int precision, unsigned long long *crossings_dev,
+                          void *stream);
+
+/* March explicit segments (pos6: xs,ys,zs,xe,ye,ze per segment, device) to
+ * tau3 (3 floats per segment, AoS).  The drop-in march uses the same
+ * kernels. */
+ARGOT_B200_API int argot_b200_march_segments(const argot_b200_grid *g, const void *packed_dev,
+                              uint64_t nseg, const float *pos6_dev, float *tau3_dev,
+                              int precision, void *stream);
+
+/* Stitch: ray_tau[r] = sum of seg_tau over the segments with ray_indx == r
+ * (segments sorted by ray index; Kahan-compensated segmented sums).  On one
+ * rank, where each ray has one segment per domain, this is the reference's
+ * accum_optical_depth. ray_tau3 is AoS (3 floats per ray) and overwritten. */
+ARGOT_B200_API int argot_b200_stitch(uint64_t nseg, const uint64_t *ray_indx_dev,
+                      const float *seg_tau3_dev, uint64_t nray, float *ray_tau3_dev,
+                      void *stream);
+
+/* ---- photo-ionisation / heating rates ----------------------------------- */
+
+#define ARGOT_B200_RATE_EXACT_F64 0   /* reference algorithm in FP64        */
+#define ARGOT_B200_RATE_EXACT_F32 1   /* FP32, FP64 only for small-dtau phi */
+#define ARGOT_B200_RATE_SURROGATE 2   /* BF16 MLP with exact fallback       */
+
+/* Per-cell rates for the target cells of blocks [b0, b1) from their rays'
+ * columns.  rates6_dev: 6 planes of ncell floats (Gamma HI, HeI, HeII,
+ * Heat HI, HeI, HeII [erg/s]); each cell's sum over its rays is written
+ * (mode EXACT_F64 adds to the existing value in ray order with the
+ * reference's float rounding, the others overwrite).  Deterministic: no
+ * atomics, the rays of a cell are summed in ray order. */
+ARGOT_B200_API int argot_b200_photoion_rays(const argot_b200_grid *g, const void *packed_dev,
+                             const argot_b200_dev_tree *t, uint64_t b0, uint64_t b1,
+                             const uint64_t *blk_offsets_dev, uint64_t base,
+                             const uint32_t *rays_dev, uint64_t nray_group,
+                             const float *tau_dev, int mode, float *rates6_dev,
+                             void *stream);
+
+/* Reads and clears the device-side error flag of the current device (set
+ * when a march exceeded its step bound, which only non-finite input can
+ * cause); synchronises `stream`.  Returns 0 or ARGOT_B200_EDEVICE. */
+ARGOT_B200_API int argot_b200_check_device_error(void *stream);
+
+/* frequency grid and cross sections as the reference tabulates them
+ * (source.c:38-53, cross_section.c:5-22): nu[256] [nu_L], csect[256x3] */
+ARGOT_B200_API void argot_b200_tables(double *nu, float *csect3);
+/* photon rate per bin of one source (source.c:104-138): type 0 blackbody
+ * (param = T [K]) or 1 power law (param = index) */
+ARGOT_B200_API void argot_b200_photon_rate(int type, float param, double total_rate, double *out256);
+/* the two integrals that photon rate is formed from: per-bin photon counts
+ * of the unnormalised shape and their total over [1, 10^1.5] nu_L; the rate
+ * of bin i is counts[i] * (total_rate / norm) */
+ARGOT_B200_API void argot_b200_photon_counts(int type, float param, double *counts256, double *norm);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ARGOT_B200_H */

@@ -1,0 +1,163 @@
+"""Build recipes for the two CPU checkers (test infrastructure only).
+
+1. O1, the parity oracle: ARGOT's own hot-path C, compiled unmodified from the
+   reference tree, one shared library per mesh edge, into
+   ``oracle/_ref/libargot_ref_n<EDGE>.so``.
+2. The restatement (``oracle/argot_oracle.c``, ref-order FP32/FP64 functions and
+   the FP64 precision oracle) into ``oracle/_build/libargot_oracle.so``.
+
+Both directories are git-ignored; the built libraries travel with the working
+tree.  Nothing in the product path (the ``argot_b200`` package) loads them.
+
+The reference fixes the local mesh size at compile time (``NMESH_*_TOTAL`` and
+``NNODE_*`` in ``src/run_param.h:22-69``).  For each edge N the recipe writes a
+copy of ``run_param.h`` with only those two settings changed (N^3 cells, one
+rank) to ``oracle/_ref/inc_N/`` and compiles the reference sources where they
+lie, with ``-I<inc_N> -I-`` so that the patched header is found before the
+original one (``-I-`` also disables the lookup of quoted includes in the
+including file's own directory).  Sources compiled: exactly the hot path and
+what it calls:
+
+  calc_optical_depth.c      (A1, CPU march)
+  accum_optical_depth.c     (A2, stitching)
+  calc_photoion_rate.c      (A3/A4, rate integral, zeroing)
+  calc_ray_segment.c, assign_ray_segment.c, setup_light_ray_tree.c
+                            (ray construction feeding the path)
+  source.c, cross_section.c, prim_chem/cross_section.c
+                            (A5 tables)
+  mpi_rank.c, timing.c      (helpers)
+
+plus two files of ours: ``oracle/shim/mpi.h`` (single-rank MPI) and
+``oracle/ref_driver.c`` (flat-array glue).  Flags follow the reference's
+``src/Makefile`` switches for this path (``-D__HELIUM__ -D__PHOTON_CONSERVING__
+-D__RADIATION_TRANSFER__ -D__ARGOT_PROFILE__``), ``-O2`` without
+``-ffast-math`` (the parity build); ``--fast-math`` adds the reference's own
+``-ffast-math`` for the spread study.  ``-ffp-contract=off`` pins IEEE
+single-operation rounding (the x86-64 baseline target has no FMA anyway).
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import re
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_OUT = os.path.join(HERE, "_ref")
+ORC_OUT = os.path.join(HERE, "_build")
+DEFAULT_REF = os.environ.get("ARGOT_REFERENCE", "/root/reference")
+
+SOURCES = [
+    "calc_optical_depth.c",
+    "accum_optical_depth.c",
+    "calc_photoion_rate.c",
+    "calc_ray_segment.c",
+    "assign_ray_segment.c",
+    "setup_light_ray_tree.c",
+    "source.c",
+    "cross_section.c",
+    "prim_chem/cross_section.c",
+    "mpi_rank.c",
+    "timing.c",
+]
+
+EDGES = (16, 32, 48, 64, 96, 128, 192, 256)
+
+FLAGS = ["-D__HELIUM__", "-D__PHOTON_CONSERVING__", "-D__RADIATION_TRANSFER__",
+         "-D__ARGOT_PROFILE__"]
+
+
+def _cc() -> str:
+    return os.environ.get("ARGOT_CC", "gcc")
+
+
+def patched_run_param(src_text: str, edge: int) -> str:
+    """run_param.h with an N^3 single-rank mesh; nothing else changes."""
+    t = re.sub(r"#define\s+NMESH_([XYZ])_TOTAL\s+\(\d+\)",
+               lambda m: f"#define NMESH_{m.group(1)}_TOTAL ({edge})", src_text)
+    t = re.sub(r"#define\s+NNODE_([XYZ])\s+\(\d+\)",
+               lambda m: f"#define NNODE_{m.group(1)} (1)", t)
+    return t
+
+
+def ref_lib_path(edge: int, fast_math: bool = False) -> str:
+    tag = "_fm" if fast_math else ""
+    return os.path.join(REF_OUT, f"libargot_ref_n{edge}{tag}.so")
+
+
+def oracle_lib_path() -> str:
+    return os.path.join(ORC_OUT, "libargot_oracle.so")
+
+
+def reference_available(ref: str = DEFAULT_REF) -> bool:
+    return os.path.isdir(os.path.join(ref, "src"))
+
+
+def build_ref(edge: int, ref: str = DEFAULT_REF, fast_math: bool = False,
+              verbose: bool = False) -> str:
+    src_dir = os.path.join(ref, "src")
+    if not os.path.isdir(src_dir):
+        raise FileNotFoundError(f"reference sources not found at {src_dir}")
+    inc = os.path.join(REF_OUT, f"inc_{edge}")
+    os.makedirs(inc, exist_ok=True)
+    with open(os.path.join(src_dir, "run_param.h")) as f:
+        text = patched_run_param(f.read(), edge)
+    with open(os.path.join(inc, "run_param.h"), "w") as f:
+        f.write(text)
+    out = ref_lib_path(edge, fast_math)
+    cmd = [_cc(), "-O2", "-std=gnu99", "-fopenmp", "-fPIC", "-shared", "-w",
+           "-fno-strict-aliasing", "-ffp-contract=off"]
+    if fast_math:
+        cmd.append("-ffast-math")
+    cmd += FLAGS
+    cmd += ["-I" + inc, "-I-", "-I" + os.path.join(HERE, "shim"),
+            "-I" + src_dir, "-I" + os.path.join(src_dir, "prim_chem")]
+    cmd += [os.path.join(src_dir, s) for s in SOURCES]
+    cmd += [os.path.join(HERE, "ref_driver.c"), "-o", out, "-lm",
+            "-Wl,--no-undefined"]
+    if verbose:
+        print(" ".join(cmd))
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stderr)
+        raise subprocess.CalledProcessError(r.returncode, cmd)
+    return out
+
+
+def build_oracle(verbose: bool = False) -> str:
+    os.makedirs(ORC_OUT, exist_ok=True)
+    out = oracle_lib_path()
+    cmd = [_cc(), "-O2", "-std=gnu99", "-fopenmp", "-fPIC", "-shared", "-Wall",
+           "-ffp-contract=off", os.path.join(HERE, "argot_oracle.c"), "-o", out,
+           "-lm", "-Wl,--no-undefined"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return out
+
+
+def build_all(edges=EDGES, ref: str = DEFAULT_REF, verbose: bool = False):
+    """Restatement always; the reference builds when its sources are here."""
+    built = [build_oracle(verbose)]
+    if reference_available(ref):
+        for e in edges:
+            built.append(build_ref(e, ref, False, verbose))
+        built.append(build_ref(64, ref, True, verbose))
+    return built
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser(description=__doc__,
+                                formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--ref", default=DEFAULT_REF)
+    p.add_argument("--edges", default=",".join(map(str, EDGES)))
+    p.add_argument("-v", "--verbose", action="store_true")
+    a = p.parse_args(argv)
+    for path in build_all([int(x) for x in a.edges.split(",") if x], a.ref, a.verbose):
+        print(path)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,88 @@
+"""The C-ABI library: builds, loads without a GPU, exports every symbol the
+header declares, and its struct layouts equal the reference's."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, ref_lib
+
+
+def header_functions():
+    text = open(os.path.join(ROOT, "include", "argot_b200.h")).read()
+    return sorted(set(re.findall(r"ARGOT_B200_API\s+[\w\s\*]+?\b(\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from argot_b200 import _lib
+    lib = _lib.load()
+    declared = header_functions()
+    assert len(declared) >= 30
+    for name in declared:
+        assert hasattr(lib, name), name
+    # and the binding covers every declared function
+    assert set(declared) == set(_lib.exported_symbols())
+
+
+def test_struct_layouts_match(tmp_path):
+    from argot_b200 import _lib, abi
+    lib = _lib.load()
+    mine = np.zeros(10, np.uint64)
+    lib.argot_b200_struct_sizes(mine.ctypes.data)
+    assert list(mine) == abi.sizes()
+    assert list(mine) == [56, 2384, 2096, 2072, 156, 52, 5480, 12, 2072, 24]
+    assert lib.argot_b200_abi_check(mine.ctypes.data, 10) == 0
+    bad = mine.copy()
+    bad[1] += 8
+    assert lib.argot_b200_abi_check(bad.ctypes.data, 10) == _lib.EINVAL
+    R = ref_lib(16)
+    assert list(R.struct_sizes()) == abi.sizes()
+    assert list(R.struct_offsets()) == abi.offsets()
+
+
+def test_tables_and_spectra_match_oracle(oracle):
+    from argot_b200 import pipeline
+    nu, cs = pipeline.tables()
+    onu, ocs, _ = oracle.tables()
+    assert np.array_equal(nu, onu) and np.array_equal(cs, ocs)
+    from argot_b200 import _lib
+    lib = _lib.load()
+    out = np.zeros(256)
+    for T, tot in ((1.0e5, 3.0e49), (4.0e4, 1.0e51)):
+        lib.argot_b200_photon_rate(0, T, tot, out.ctypes.data)
+        assert np.array_equal(out, oracle.photon_rate(0, T, tot))
+
+
+def test_tree_builds_on_host():
+    """Tree construction is host code: runs without a GPU."""
+    from argot_b200 import _lib, workload as W
+    from argot_b200.pipeline import photon_counts, unit_box_grid
+    lib = _lib.load()
+    wl = W.tiny(16, 9, seed=4)
+    g = unit_box_grid(16, wl.lunit, wl.denstonh)
+    spec = W.photon_rates(photon_counts, wl.src_type, wl.src_param, wl.src_rate)
+    t = C.c_void_p()
+    assert lib.argot_b200_tree_build(C.byref(g), wl.nsrc, wl.src_pos.ctypes.data,
+                                     spec.ctypes.data, 0.5, C.byref(t)) == 0
+    nn = lib.argot_b200_tree_num_nodes(t)
+    ne = lib.argot_b200_tree_num_emitters(t)
+    assert ne == nn + wl.nsrc and nn >= wl.nsrc
+    pos4 = np.zeros((ne, 4), np.float32)
+    sp = np.zeros((ne, 256))
+    assert lib.argot_b200_tree_emitters(t, pos4.ctypes.data, sp.ctypes.data) == 0
+    # root spectrum = sum of all sources; source emitters carry their own
+    assert np.allclose(sp[0], spec.sum(axis=0), rtol=1e-13)
+    assert np.array_equal(sp[nn:], spec)
+    assert np.array_equal(pos4[nn:, :3], wl.src_pos)
+    lib.argot_b200_tree_free(t)
+
+
+def test_invalid_arguments_rejected_without_gpu():
+    from argot_b200 import _lib
+    lib = _lib.load()
+    assert lib.argot_b200_tree_build(None, 0, None, None, 0.5, None) == _lib.EINVAL
+    nb = C.c_uint64()
+    assert lib.argot_b200_num_blocks(None, C.byref(nb)) == _lib.EINVAL
+    assert lib.argot_b200_last_error() == _lib.EINVAL

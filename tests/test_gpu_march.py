@@ -1,0 +1,123 @@
+"""GPU parity of the march (calc_optical_depth) and the ray generation.
+
+Tolerances: the reference-order kernels are bit-exact against the reference
+(integer/bit work); the Kahan kernel is within 1e-5 relative of the FP64
+oracle per column (the exact-path tolerance for optical depth)."""
+import numpy as np
+import pytest
+
+from conftest import golden, ref_lib
+
+pytestmark = pytest.mark.gpu
+
+KAHAN_RTOL = 1e-5
+
+
+def test_march_segments_reference_bitwise_golden(cuda_ok):
+    from argot_b200 import _lib as L
+    from gpu_util import march_segments
+    g = golden("golden_march.npz")
+    f = tuple(g[k] for k in ("dens", "fHI", "fHeI", "fHeII"))
+    tau = march_segments(int(g["edge"]), f, g["seg"], L.PRECISION_REFERENCE)
+    assert np.array_equal(tau, g["tau"])
+
+
+def test_march_segments_kahan_vs_fp64(cuda_ok, oracle):
+    from argot_b200 import _lib as L
+    from gpu_util import march_segments
+    from oracle.oracle import unit_box_grid
+    g = golden("golden_march.npz")
+    f = tuple(np.ascontiguousarray(g[k]) for k in ("dens", "fHI", "fHeI", "fHeII"))
+    edge = int(g["edge"])
+    tau = march_segments(edge, f, g["seg"], L.PRECISION_KAHAN).astype(np.float64)
+    t64 = oracle.march_f64(unit_box_grid(edge, 1.0, 1.0), f, g["seg"])
+    ok = t64 > 1e-6 * t64.max()
+    rel = np.abs(tau - t64)[ok] / t64[ok]
+    assert rel.max() < KAHAN_RTOL, rel.max()
+
+
+@pytest.mark.parametrize("edge,nsrc,theta", [(16, 6, 0.5), (32, 24, 0.5), (32, 40, 0.7)])
+def test_ray_lists_match_reference_tree(cuda_ok, edge, nsrc, theta):
+    """Device tree walk emits, per target cell, the reference's rays in the
+    reference's order (setup_light_ray_to)."""
+    from argot_b200 import workload as W
+    from argot_b200 import _lib as L
+    from gpu_util import run_problem
+    wl = W.tiny(edge, nsrc, seed=edge + nsrc)
+    wl.theta = theta
+    pb, emit, tgt, tau, _ = run_problem(wl, L.PRECISION_REFERENCE, L.RATE_EXACT_F32)
+    R = ref_lib(edge)
+    R.init(wl.lunit, wl.denstonh, theta, 4)
+    R.set_mesh(*wl.fields())
+    R.set_sources(wl.src_type, wl.src_param, wl.src_pos, wl.src_rate)
+    out = R.run_range(0, edge ** 3, False, want=("tgt", "src", "tau"))
+    assert len(emit) == out["nray"]
+    pos4, _ = pb.emitters()
+    cell = lambda t: (t[:, 0].astype(np.int64) * edge + t[:, 1]) * edge + t[:, 2]  # noqa: E731
+    # stable sort both lists by cell: the order within a cell must agree
+    mine = np.argsort(cell(tgt), kind="stable")
+    ref = np.argsort(cell(out["tgt"]), kind="stable")
+    assert np.array_equal(cell(tgt)[mine], cell(out["tgt"])[ref])
+    assert np.array_equal(pos4[emit[mine], :3], out["src"][ref])
+    # and the columns of the reference-order march are the reference's
+    assert np.array_equal(tau[mine], out["tau"][ref])
+
+
+def test_march_rays_kahan_vs_fp64(cuda_ok, oracle):
+    from argot_b200 import workload as W
+    from argot_b200 import _lib as L
+    from gpu_util import run_problem, ray_segments
+    from oracle.oracle import unit_box_grid
+    wl = W.tiny(32, 20, seed=8, sigma_ln=1.2)
+    pb, emit, tgt, tau, _ = run_problem(wl, L.PRECISION_KAHAN, L.RATE_EXACT_F32)
+    segs = ray_segments(pb, emit, tgt)
+    t64 = oracle.march_f64(unit_box_grid(32, wl.lunit, wl.denstonh), wl.fields(), segs)
+    ok = t64 > 0
+    rel = np.abs(tau.astype(np.float64) - t64)[ok] / t64[ok]
+    assert rel.max() < KAHAN_RTOL, rel.max()
+    # the reference's FP32 order is visibly less accurate on the same rays
+    t32 = oracle.march_f32ref(unit_box_grid(32, wl.lunit, wl.denstonh), wl.fields(), segs)
+    rel32 = np.abs(t32.astype(np.float64) - t64)[ok] / t64[ok]
+    assert rel32.max() > rel.max()
+
+
+def test_grouped_rays_equal_single_pass(cuda_ok):
+    """Memory-bounded groups of target blocks give the same columns."""
+    from argot_b200 import workload as W
+    from argot_b200 import _lib as L
+    from gpu_util import run_problem
+    wl = W.tiny(32, 12, seed=3)
+    _, e1, t1, tau1, r1 = run_problem(wl, L.PRECISION_KAHAN, L.RATE_EXACT_F32)
+    pb, e2, t2, tau2, r2 = run_problem(wl, L.PRECISION_KAHAN, L.RATE_EXACT_F32, max_group_rays=5000)
+    assert len(pb.groups) > 3
+    assert np.array_equal(e1, e2) and np.array_equal(t1, t2)
+    assert np.array_equal(tau1, tau2)
+    assert np.array_equal(r1, r2)
+
+
+def test_stitch_segmented_sum(cuda_ok, oracle):
+    import torch
+    from argot_b200 import _lib as L
+    lib = L.load()
+    rng = np.random.default_rng(5)
+    nray = 3000
+    nseg_per = rng.integers(0, 5, nray)
+    ray_indx = np.repeat(np.arange(nray, dtype=np.uint64), nseg_per)
+    seg_tau = rng.random((len(ray_indx), 3)).astype(np.float32)
+    ri = torch.from_numpy(ray_indx.view(np.int64)).cuda()
+    st = torch.from_numpy(seg_tau).cuda()
+    out = torch.full((nray, 3), 7.0, dtype=torch.float32, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    L.check(lib.argot_b200_stitch(len(ray_indx), ri.data_ptr(), st.data_ptr(), nray, out.data_ptr(), s),
+            "stitch")
+    got = out.cpu().numpy()
+    want = np.zeros((nray, 3))
+    np.add.at(want, ray_indx.astype(np.int64), seg_tau.astype(np.float64))
+    assert np.allclose(got, want, rtol=2e-7, atol=0)
+    # one segment per ray (the reference's single-rank case): exact copy
+    one = np.arange(nray, dtype=np.uint64)
+    t1 = rng.random((nray, 3)).astype(np.float32)
+    L.check(lib.argot_b200_stitch(nray, torch.from_numpy(one.view(np.int64)).cuda().data_ptr(),
+                                  torch.from_numpy(t1).cuda().data_ptr(), nray, out.data_ptr(), s),
+            "stitch")
+    assert np.array_equal(out.cpu().numpy(), oracle.accum(nray, one, t1))

@@ -1,0 +1,164 @@
+"""The CPU restatement (oracle/argot_oracle.c) pinned against ARGOT's own C:
+the committed golden fixtures (made by tests/golden/make_golden.py from the
+reference build) and, when present, the live reference build."""
+import numpy as np
+import pytest
+
+from conftest import golden, ref_lib
+from oracle.oracle import unit_box_grid
+
+
+def _grid(g):
+    return unit_box_grid(int(g["edge"]), float(g["lunit"]), float(g["denstonh"]))
+
+
+def _fields(g):
+    return tuple(np.ascontiguousarray(g[k]) for k in ("dens", "fHI", "fHeI", "fHeII"))
+
+
+def test_tables_match_golden(oracle):
+    g = golden("golden_tables.npz")
+    nu, cs, meta = oracle.tables()
+    assert np.array_equal(nu, g["nu"])
+    assert np.array_equal(cs, g["csect"])
+    assert np.array_equal(meta, g["meta"])
+    for args, want in zip(g["photon_rate_args"], g["photon_rate"]):
+        got = oracle.photon_rate(int(args[0]), float(args[1]), float(args[2]))
+        assert np.array_equal(got, want)
+
+
+def test_photon_rate_is_linear_in_total(oracle):
+    # the per-bin rates scale with the requested total; their sum is not the
+    # total itself, because the reference normalises by a separately
+    # integrated (coarser) total over [1, 10^1.5] nu_L (source.c:114-135)
+    a = oracle.photon_rate(0, 1.0e5, 1.0e50)
+    b = oracle.photon_rate(0, 1.0e5, 2.0e50)
+    assert np.allclose(b, 2.0 * a, rtol=1e-15)
+    assert 0.9 < a.sum() / 1.0e50 < 1.2
+
+
+def test_march_f32ref_bitwise_golden(oracle):
+    g = golden("golden_march.npz")
+    tau = oracle.march_f32ref(_grid(g), _fields(g), g["seg"])
+    assert np.array_equal(tau, g["tau"])
+
+
+def test_march_f64_close_to_reference(oracle):
+    g = golden("golden_march.npz")
+    t64 = oracle.march_f64(_grid(g), _fields(g), g["seg"])
+    ref = g["tau"].astype(np.float64)
+    scale = np.maximum(np.abs(t64), 1e-30)
+    rel = np.abs(ref - t64) / scale
+    # the reference's FP32 march drifts by O(1e-5) over a 16-cell box
+    assert np.nanmax(rel[t64 > 1e-12]) < 3e-4
+    # uniform-density analytic check: column = n * length
+    edge = int(g["edge"])
+    n = edge ** 3
+    ones = np.ones(n, np.float32)
+    f = (ones, ones, np.zeros(n, np.float32), np.zeros(n, np.float32))
+    seg = np.asarray(g["seg"], np.float64)
+    inside = np.all((seg >= 0) & (seg <= 1), axis=1)
+    length = np.linalg.norm(seg[:, 3:] - seg[:, :3], axis=1)
+    t = oracle.march_f64(_grid(g), f, g["seg"])[:, 0]
+    assert np.allclose(t[inside], length[inside], rtol=1e-12, atol=1e-12)
+
+
+def test_path_golden_columns_and_rates(oracle):
+    g = golden("golden_path.npz")
+    grid = _grid(g)
+    tau = oracle.march_f32ref(grid, _fields(g), g["seg"])
+    assert np.array_equal(tau, g["tau"])
+    # rates need the ray spectra: rebuild them from the source list (leaf
+    # rays carry a source's spectrum, node rays the sum over the node); the
+    # spectrum sums recorded by the reference pin that reconstruction
+    from argot_b200.pipeline import photon_counts
+    from argot_b200.workload import photon_rates
+    spectra_src = photon_rates(photon_counts, g["src_type"], g["src_param"], g["src_rate"])
+    per_ray = _ray_spectra(g, spectra_src)
+    assert np.allclose(per_ray.sum(axis=1), g["spec_sum"], rtol=1e-12)
+    # node spectra rebuilt here may differ from the tree's in the last bit
+    # of a double (summation order), so the float per-cell sums agree to a
+    # few float ulps rather than bit for bit
+    rates = oracle.photoion_f64ref(grid, _fields(g), g["tau"], g["tgt"], g["src"], per_ray)
+    assert np.allclose(rates, g["rates"], rtol=1e-6, atol=0)
+
+
+def _ray_spectra(g, spectra_src):
+    """Spectrum of each golden ray: the source whose position it starts at,
+    else the sum of the sources nearest a node centre is not recoverable, so
+    rays from nodes are matched by spectrum sum over subsets of sources."""
+    pos = g["src_pos"]
+    src = g["src"]
+    out = np.zeros((len(src), 256))
+    sums = spectra_src.sum(axis=1)
+    for i, p in enumerate(src):
+        hit = np.where(np.all(pos == p, axis=1))[0]
+        if len(hit):
+            out[i] = spectra_src[hit[0]]
+        else:
+            # node ray: the node's spectrum is the sum over a subset of
+            # sources; find the subset whose total matches the recorded sum
+            target = g["spec_sum"][i]
+            n = len(pos)
+            for mask in range(1, 1 << n):
+                idx = [k for k in range(n) if mask >> k & 1]
+                if len(idx) > 1 and abs(sums[idx].sum() / target - 1.0) < 1e-12:
+                    out[i] = spectra_src[idx].sum(axis=0)
+                    break
+    return out
+
+
+def test_stitch_single_rank(oracle):
+    rng = np.random.default_rng(3)
+    nray = 500
+    ray_indx = rng.permutation(nray).astype(np.uint64)[:400]
+    seg_tau = rng.random((400, 3)).astype(np.float32)
+    out = oracle.accum(nray, ray_indx, seg_tau)
+    want = np.zeros((nray, 3), np.float32)
+    want[ray_indx.astype(np.int64)] = seg_tau
+    assert np.array_equal(out, want)
+
+
+# ---------------------------------------------------------- live reference
+def test_restatement_equals_reference_build(oracle):
+    """Ref-order restatement vs the reference compiled here, bit for bit, on
+    a fresh seeded problem (march, stitching, rates)."""
+    from argot_b200 import workload as W
+    wl = W.tiny(16, 5, seed=99)
+    R = ref_lib(16)
+    R.init(wl.lunit, wl.denstonh, wl.theta, 1)
+    R.set_mesh(*wl.fields())
+    R.set_sources(wl.src_type, wl.src_param, wl.src_pos, wl.src_rate)
+    R.zero_rates()
+    out = R.run_range(0, 16 ** 3, True, want=("tgt", "src", "seg", "tau", "spectra"))
+    grid = unit_box_grid(16, wl.lunit, wl.denstonh)
+    tau = oracle.march_f32ref(grid, wl.fields(), out["seg"])
+    assert np.array_equal(tau, out["tau"])
+    rates = oracle.photoion_f64ref(grid, wl.fields(), out["tau"], out["tgt"], out["src"],
+                                   out["spectra"])
+    assert np.array_equal(rates, R.get_rates())
+    acc = R.accum_segments(len(tau), np.arange(len(tau), dtype=np.uint64), tau)
+    assert np.array_equal(acc, oracle.accum(len(tau), np.arange(len(tau), dtype=np.uint64), tau))
+
+
+def test_reference_fast_math_spread(oracle):
+    """The reference's own -ffast-math build differs from its strict build;
+    record that the spread stays at FP32-rounding level."""
+    from argot_b200 import workload as W
+    from oracle import build
+    import os
+    if not os.path.exists(build.ref_lib_path(64, True)) and not build.reference_available():
+        pytest.skip("fast-math build unavailable")
+    from oracle.oracle import RefLib
+    g = golden("golden_march.npz")
+    wl = W.tiny(64, 4, seed=5)
+    Rf = RefLib(64, fast_math=True)
+    Rf.init(wl.lunit, wl.denstonh, 0.5, 1)
+    Rf.set_mesh(*wl.fields())
+    rng = np.random.default_rng(1)
+    segs = np.concatenate([rng.uniform(0, 1, (3000, 3)), (rng.integers(0, 64, (3000, 3)) + 0.5) / 64],
+                          axis=1).astype(np.float32)
+    tf, _ = Rf.march_segments(segs)
+    ts = oracle.march_f32ref(unit_box_grid(64, wl.lunit, wl.denstonh), wl.fields(), segs)
+    rel = np.abs(tf - ts) / np.maximum(np.abs(ts), 1e-30)
+    assert np.max(rel) < 1e-3
