@@ -102,13 +102,18 @@ static __device__ __noinline__ Tau3 march_reference(const GridDev &g, const floa
 }
 
 // ---------------------------------------------------------------------------
-// Parametric march with compensated sums.  Same cells and the same start /
-// end cell rules as the reference, but the exit distance of every cell is
-// recomputed from the start point, t_axis = (face - x0) / u_axis, instead of
-// advancing a running position, so rounding does not accumulate along the
-// ray; the columns are Kahan-compensated FP32 sums.  The walk also stops
-// once the next exit lies beyond the end point, which keeps it from running
-// past a target it grazes at a corner.
+// Count-down march with compensated sums.  Same start / end cell rules as
+// the reference.  Along each axis the walk must cross exactly
+// |i_end - i_start| faces, so it keeps per axis the number of faces still
+// to cross and the distance along the ray to the next one.  Every step
+// takes the nearest face among the axes that still have faces to cross,
+// resets that axis's distance to the face spacing dX/|u_x| and shortens the
+// others by the step.  Distances therefore stay of cell size, and their
+// rounding scales with the cell rather than with the ray length as a running
+// position or an absolute path parameter would; the walk always ends in the
+// end cell after at most sum|di| steps.  The last chord is measured from
+// the face through which the end cell was entered.  Columns are
+// Kahan-compensated FP32 sums.
 __device__ __forceinline__ void kahan_add(float &s, float &c, float v) {
   const float y = v - c;
   const float tt = s + y;
@@ -117,8 +122,8 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float v) {
 }
 
 static __device__ __noinline__ Tau3 march_kahan(const GridDev &g, const float4 *__restrict__ cells,
-                                         float xs, float ys, float zs, float xe, float ye,
-                                         float ze, int *steps, bool *bad) {
+                                                float xs, float ys, float zs, float xe, float ye,
+                                                float ze, int *steps, bool *bad) {
   const int ixe = axis_cell(xe, g.xminl, g.dx, g.nx);
   const int iye = axis_cell(ye, g.yminl, g.dy, g.ny);
   const int ize = axis_cell(ze, g.zminl, g.dz, g.nz);
@@ -127,42 +132,50 @@ static __device__ __noinline__ Tau3 march_kahan(const GridDev &g, const float4 *
   int iz = axis_cell(zs, g.zminl, g.dz, g.nz);
 
   const float x0 = xs - g.xminl, y0 = ys - g.yminl, z0 = zs - g.zminl;
+  const float x1 = xe - g.xminl, y1 = ye - g.yminl, z1 = ze - g.zminl;
   const float dx = xe - xs, dy = ye - ys, dz = ze - zs;
   const float len = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
   const float il = len > 0.f ? 1.0f / len : 0.f;
   const float ux = cosine_guard(dx * il), uy = cosine_guard(dy * il), uz = cosine_guard(dz * il);
-  const float ivx = 1.0f / ux, ivy = 1.0f / uy, ivz = 1.0f / uz;
-  const int sx = ux > 0.f ? 1 : 0, nxs = ux > 0.f ? 1 : -1;
-  const int sy = uy > 0.f ? 1 : 0, nys = uy > 0.f ? 1 : -1;
-  const int sz = uz > 0.f ? 1 : 0, nzs = uz > 0.f ? 1 : -1;
-  float tx = fmaf(g.dx, (float)(ix + sx), -x0) * ivx;
-  float ty = fmaf(g.dy, (float)(iy + sy), -y0) * ivy;
-  float tz = fmaf(g.dz, (float)(iz + sz), -z0) * ivz;
+  const float ax = fabsf(ux), ay = fabsf(uy), az = fabsf(uz);
+  const float iax = 1.0f / ax, iay = 1.0f / ay, iaz = 1.0f / az;
+  int cx = abs(ixe - ix), cy = abs(iye - iy), cz = abs(ize - iz);
+  const int stx = ixe > ix ? 1 : -1, sty = iye > iy ? 1 : -1, stz = ize > iz ? 1 : -1;
+  // distance to the first face in the stepping direction (>= 0)
+  const float kInf = __int_as_float(0x7f800000);
+  float rx = cx ? fmaxf(fabsf(fmaf(g.dx, (float)(ix + (stx > 0)), -x0)) * iax, 0.f) : kInf;
+  float ry = cy ? fmaxf(fabsf(fmaf(g.dy, (float)(iy + (sty > 0)), -y0)) * iay, 0.f) : kInf;
+  float rz = cz ? fmaxf(fabsf(fmaf(g.dz, (float)(iz + (stz > 0)), -z0)) * iaz, 0.f) : kInf;
+  const float tdx = g.dx * iax, tdy = g.dy * iay, tdz = g.dz * iaz;
 
   float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
-  float t = 0.f;
+  const int total = cx + cy + cz;
+  int last = -1;  // axis of the last face crossed (largest |u| on ties)
   int it = 0;
-  const int cap = g.nx + g.ny + g.nz + 2;
-  while ((ix != ixe || iy != iye || iz != ize) && (unsigned)ix < (unsigned)g.nx &&
-         (unsigned)iy < (unsigned)g.ny && (unsigned)iz < (unsigned)g.nz) {
-    const float tn = fminf(tx, fminf(ty, tz));
-    if (tn >= len) break;  // the segment ends inside this cell
-    if (++it > cap) { *bad = true; break; }
+  for (; it < total && (cx | cy | cz); it++) {
+    const float r = fminf(rx, fminf(ry, rz));
     const float4 n = ld_cell(cells, cell_index(g, ix, iy, iz));
-    const float r = tn - t;
-    if (tn == tx) { ix += nxs; tx = fmaf(g.dx, (float)(ix + sx), -x0) * ivx; }
-    if (tn == ty) { iy += nys; ty = fmaf(g.dy, (float)(iy + sy), -y0) * ivy; }
-    if (tn == tz) { iz += nzs; tz = fmaf(g.dz, (float)(iz + sz), -z0) * ivz; }
-    t = tn;
     kahan_add(s0, c0, r * n.x);
     kahan_add(s1, c1, r * n.y);
     kahan_add(s2, c2, r * n.z);
+    const bool hx = rx == r, hy = ry == r, hz = rz == r;
+    float best = -1.f;
+    if (hx) { ix += stx; cx--; rx = cx ? tdx : kInf; if (ax > best) { best = ax; last = 0; } } else { rx -= r; }
+    if (hy) { iy += sty; cy--; ry = cy ? tdy : kInf; if (ay > best) { best = ay; last = 1; } } else { ry -= r; }
+    if (hz) { iz += stz; cz--; rz = cz ? tdz : kInf; if (az > best) { best = az; last = 2; } } else { rz -= r; }
   }
-  // remaining chord in the cell that contains the end point
-  const float depth = fabsf(len - t);
-  const bool inside = (unsigned)ix < (unsigned)g.nx && (unsigned)iy < (unsigned)g.ny &&
-                      (unsigned)iz < (unsigned)g.nz;
-  const float4 ne = ld_cell(cells, inside ? cell_index(g, ix, iy, iz) : cell_index(g, ixe, iye, ize));
+  if (cx | cy | cz) *bad = true;  // only non-finite input leaves faces uncrossed
+  // chord from the entry face of the end cell to the end point
+  float depth;
+  if (last == 0)
+    depth = fabsf(x1 - g.dx * (float)(ix + (stx < 0))) * iax;
+  else if (last == 1)
+    depth = fabsf(y1 - g.dy * (float)(iy + (sty < 0))) * iay;
+  else if (last == 2)
+    depth = fabsf(z1 - g.dz * (float)(iz + (stz < 0))) * iaz;
+  else
+    depth = len;
+  const float4 ne = ld_cell(cells, cell_index(g, ixe, iye, ize));
   kahan_add(s0, c0, depth * ne.x);
   kahan_add(s1, c1, depth * ne.y);
   kahan_add(s2, c2, depth * ne.z);
