@@ -61,6 +61,7 @@ SIGNATURES = {
     "argot_b200_num_blocks": (i32, [GP, C.POINTER(u64)]),
     "argot_b200_count_rays": (i32, [GP, vp, u64, u64, vp, vp, vp]),
     "argot_b200_scan_blocks": (i32, [vp, u64, u64, vp, C.POINTER(u64), vp]),
+    "argot_b200_scan_blocks_static": (i32, [vp, u64, u64, vp, C.POINTER(u64), vp]),
     "argot_b200_emit_rays": (i32, [GP, vp, u64, u64, vp, u64, vp, vp]),
     "argot_b200_march_rays": (i32, [GP, vp, vp, u64, u64, vp, u64, vp, u64, vp, i32, vp, vp]),
     "argot_b200_march_segments": (i32, [GP, vp, u64, vp, vp, i32, vp]),

@@ -194,6 +194,19 @@ ARGOT_B200_API int argot_b200_count_rays(const argot_b200_grid *g, const argot_b
  * starting at base; also returns the total on the host if total != NULL. */
 ARGOT_B200_API int argot_b200_scan_blocks(const uint64_t *blk_count_dev, uint64_t nb, uint64_t base,
                            uint64_t *blk_offsets_dev, uint64_t *total, void *stream);
+/* The same scan, allocating no memory: for callers that cannot allocate
+ * device memory while the path runs (code inside a stream capture that must
+ * not touch the allocator, hosts that give all device memory to their own
+ * pool, drop-in callers that forbid cudaMalloc after start-up).  No
+ * counterpart in the reference.  Its scratch is a fixed 64 KiB device array
+ * that every GPU loading the library holds until exit: nb is limited to
+ * 16 777 216 blocks (larger requests return ARGOT_B200_EINVAL and launch
+ * nothing).  All calls on a device share that array, so calls that overlap
+ * on the GPU race; serialise them.  The first call on a device looks up the
+ * array's address: make it before any stream capture. */
+ARGOT_B200_API int argot_b200_scan_blocks_static(const uint64_t *blk_count_dev, uint64_t nb,
+                                                 uint64_t base, uint64_t *blk_offsets_dev,
+                                                 uint64_t *total, void *stream);
 /* Pass 2: write the ray words of blocks [b0, b1) at blk_offsets[b] - base. */
 ARGOT_B200_API int argot_b200_emit_rays(const argot_b200_grid *g, const argot_b200_dev_tree *t,
                          uint64_t b0, uint64_t b1, const uint64_t *blk_offsets_dev,
