@@ -121,65 +121,103 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float v) {
   s = tt;
 }
 
-static __device__ __noinline__ Tau3 march_kahan(const GridDev &g, const float4 *__restrict__ cells,
-                                                float xs, float ys, float zs, float xe, float ye,
-                                                float ze, int *steps, bool *bad) {
+// Walk state: yields (chord, cell) for every cell from the start cell to the
+// end cell; the last chord runs from the end cell's entry face to the end
+// point.
+struct CountdownWalk {
+  float rx, ry, rz, tdx, tdy, tdz, iax, iay, iaz, ax, ay, az, len, x1, y1, z1;
+  int ix, iy, iz, cx, cy, cz, stx, sty, stz, last, left;
+};
+
+__device__ __forceinline__ void walk_init(CountdownWalk &w, const GridDev &g, float xs, float ys, float zs,
+                                          float xe, float ye, float ze) {
   const int ixe = axis_cell(xe, g.xminl, g.dx, g.nx);
   const int iye = axis_cell(ye, g.yminl, g.dy, g.ny);
   const int ize = axis_cell(ze, g.zminl, g.dz, g.nz);
-  int ix = axis_cell(xs, g.xminl, g.dx, g.nx);
-  int iy = axis_cell(ys, g.yminl, g.dy, g.ny);
-  int iz = axis_cell(zs, g.zminl, g.dz, g.nz);
-
+  w.ix = axis_cell(xs, g.xminl, g.dx, g.nx);
+  w.iy = axis_cell(ys, g.yminl, g.dy, g.ny);
+  w.iz = axis_cell(zs, g.zminl, g.dz, g.nz);
   const float x0 = xs - g.xminl, y0 = ys - g.yminl, z0 = zs - g.zminl;
-  const float x1 = xe - g.xminl, y1 = ye - g.yminl, z1 = ze - g.zminl;
+  w.x1 = xe - g.xminl; w.y1 = ye - g.yminl; w.z1 = ze - g.zminl;
   const float dx = xe - xs, dy = ye - ys, dz = ze - zs;
-  const float len = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-  const float il = len > 0.f ? 1.0f / len : 0.f;
-  const float ux = cosine_guard(dx * il), uy = cosine_guard(dy * il), uz = cosine_guard(dz * il);
-  const float ax = fabsf(ux), ay = fabsf(uy), az = fabsf(uz);
-  const float iax = 1.0f / ax, iay = 1.0f / ay, iaz = 1.0f / az;
-  int cx = abs(ixe - ix), cy = abs(iye - iy), cz = abs(ize - iz);
-  const int stx = ixe > ix ? 1 : -1, sty = iye > iy ? 1 : -1, stz = ize > iz ? 1 : -1;
-  // distance to the first face in the stepping direction (>= 0)
+  w.len = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+  const float il = w.len > 0.f ? 1.0f / w.len : 0.f;
+  w.ax = fabsf(cosine_guard(dx * il));
+  w.ay = fabsf(cosine_guard(dy * il));
+  w.az = fabsf(cosine_guard(dz * il));
+  w.iax = 1.0f / w.ax; w.iay = 1.0f / w.ay; w.iaz = 1.0f / w.az;
+  w.cx = abs(ixe - w.ix); w.cy = abs(iye - w.iy); w.cz = abs(ize - w.iz);
+  w.stx = ixe > w.ix ? 1 : -1; w.sty = iye > w.iy ? 1 : -1; w.stz = ize > w.iz ? 1 : -1;
   const float kInf = __int_as_float(0x7f800000);
-  float rx = cx ? fmaxf(fabsf(fmaf(g.dx, (float)(ix + (stx > 0)), -x0)) * iax, 0.f) : kInf;
-  float ry = cy ? fmaxf(fabsf(fmaf(g.dy, (float)(iy + (sty > 0)), -y0)) * iay, 0.f) : kInf;
-  float rz = cz ? fmaxf(fabsf(fmaf(g.dz, (float)(iz + (stz > 0)), -z0)) * iaz, 0.f) : kInf;
-  const float tdx = g.dx * iax, tdy = g.dy * iay, tdz = g.dz * iaz;
+  w.rx = w.cx ? fmaxf(fabsf(fmaf(g.dx, (float)(w.ix + (w.stx > 0)), -x0)) * w.iax, 0.f) : kInf;
+  w.ry = w.cy ? fmaxf(fabsf(fmaf(g.dy, (float)(w.iy + (w.sty > 0)), -y0)) * w.iay, 0.f) : kInf;
+  w.rz = w.cz ? fmaxf(fabsf(fmaf(g.dz, (float)(w.iz + (w.stz > 0)), -z0)) * w.iaz, 0.f) : kInf;
+  w.tdx = g.dx * w.iax; w.tdy = g.dy * w.iay; w.tdz = g.dz * w.iaz;
+  w.last = -1;
+  w.left = w.cx + w.cy + w.cz + 1;  // entries still to yield (bounded)
+}
 
-  float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
-  const int total = cx + cy + cz;
-  int last = -1;  // axis of the last face crossed (largest |u| on ties)
-  int it = 0;
-  for (; it < total && (cx | cy | cz); it++) {
-    const float r = fminf(rx, fminf(ry, rz));
-    const float4 n = ld_cell(cells, cell_index(g, ix, iy, iz));
-    kahan_add(s0, c0, r * n.x);
-    kahan_add(s1, c1, r * n.y);
-    kahan_add(s2, c2, r * n.z);
-    const bool hx = rx == r, hy = ry == r, hz = rz == r;
+// Next (chord, cell); false when the walk is exhausted.
+__device__ __forceinline__ bool walk_next(CountdownWalk &w, const GridDev &g, float *r_out, size_t *c_out) {
+  if (w.left <= 0) return false;
+  w.left--;
+  *c_out = cell_index(g, w.ix, w.iy, w.iz);
+  if ((w.cx | w.cy | w.cz) && w.left > 0) {
+    const float kInf = __int_as_float(0x7f800000);
+    const float r = fminf(w.rx, fminf(w.ry, w.rz));
     float best = -1.f;
-    if (hx) { ix += stx; cx--; rx = cx ? tdx : kInf; if (ax > best) { best = ax; last = 0; } } else { rx -= r; }
-    if (hy) { iy += sty; cy--; ry = cy ? tdy : kInf; if (ay > best) { best = ay; last = 1; } } else { ry -= r; }
-    if (hz) { iz += stz; cz--; rz = cz ? tdz : kInf; if (az > best) { best = az; last = 2; } } else { rz -= r; }
+    if (w.rx == r) { w.ix += w.stx; w.cx--; w.rx = w.cx ? w.tdx : kInf; if (w.ax > best) { best = w.ax; w.last = 0; } } else { w.rx -= r; }
+    if (w.ry == r) { w.iy += w.sty; w.cy--; w.ry = w.cy ? w.tdy : kInf; if (w.ay > best) { best = w.ay; w.last = 1; } } else { w.ry -= r; }
+    if (w.rz == r) { w.iz += w.stz; w.cz--; w.rz = w.cz ? w.tdz : kInf; if (w.az > best) { best = w.az; w.last = 2; } } else { w.rz -= r; }
+    // a step that crosses several faces at once (a corner) ends the walk
+    // early; the remaining budget shrinks with it
+    w.left = min(w.left, w.cx + w.cy + w.cz + 1);
+    *r_out = r;
+    return true;
   }
-  if (cx | cy | cz) *bad = true;  // only non-finite input leaves faces uncrossed
-  // chord from the entry face of the end cell to the end point
+  // the end cell: chord from its entry face to the end point
   float depth;
-  if (last == 0)
-    depth = fabsf(x1 - g.dx * (float)(ix + (stx < 0))) * iax;
-  else if (last == 1)
-    depth = fabsf(y1 - g.dy * (float)(iy + (sty < 0))) * iay;
-  else if (last == 2)
-    depth = fabsf(z1 - g.dz * (float)(iz + (stz < 0))) * iaz;
+  if (w.last == 0)
+    depth = fabsf(w.x1 - g.dx * (float)(w.ix + (w.stx < 0))) * w.iax;
+  else if (w.last == 1)
+    depth = fabsf(w.y1 - g.dy * (float)(w.iy + (w.sty < 0))) * w.iay;
+  else if (w.last == 2)
+    depth = fabsf(w.z1 - g.dz * (float)(w.iz + (w.stz < 0))) * w.iaz;
   else
-    depth = len;
-  const float4 ne = ld_cell(cells, cell_index(g, ixe, iye, ize));
-  kahan_add(s0, c0, depth * ne.x);
-  kahan_add(s1, c1, depth * ne.y);
-  kahan_add(s2, c2, depth * ne.z);
-  *steps = it + 1;
+    depth = w.len;
+  w.left = 0;
+  *r_out = depth;
+  return true;
+}
+
+// The walk with a two-deep software pipeline: the gathers of the next two
+// cells are in flight while the current one is accumulated (the cell
+// sequence does not depend on the densities).
+static __device__ __forceinline__ Tau3 march_kahan(const GridDev &g, const float4 *__restrict__ cells,
+                                                   float xs, float ys, float zs, float xe, float ye,
+                                                   float ze, int *steps, bool *bad) {
+  CountdownWalk w;
+  walk_init(w, g, xs, ys, zs, xe, ye, ze);
+  float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
+  float ra = 0.f, rb = 0.f;
+  size_t ca = 0, cb = 0;
+  float4 na = make_float4(0.f, 0.f, 0.f, 0.f), nb = na;
+  bool ha = walk_next(w, g, &ra, &ca);
+  if (ha) na = ld_cell(cells, ca);
+  bool hb = walk_next(w, g, &rb, &cb);
+  if (hb) nb = ld_cell(cells, cb);
+  int n = 0;
+  while (ha) {
+    kahan_add(s0, c0, ra * na.x);
+    kahan_add(s1, c1, ra * na.y);
+    kahan_add(s2, c2, ra * na.z);
+    n++;
+    ha = hb; ra = rb; na = nb;
+    hb = walk_next(w, g, &rb, &cb);
+    if (hb) nb = ld_cell(cells, cb);
+  }
+  if (w.cx | w.cy | w.cz) *bad = true;  // only non-finite input leaves faces uncrossed
+  *steps = n;
   return Tau3{s0, s1, s2};
 }
 
@@ -193,11 +231,22 @@ __device__ __forceinline__ float cell_centre(float lo, int i, float d) {
   return __double2float_rn(__dadd_rn((double)lo, __dmul_rn(__dadd_rn((double)__int2float_rn(i), 0.5), (double)d)));
 }
 
+static __device__ __noinline__ void ray_start_outside(const GridDev &g, float sx, float sy, float sz,
+                                                      float xt, float yt, float zt, float *ox, float *oy,
+                                                      float *oz);
+
 __device__ __forceinline__ void ray_start(const GridDev &g, float sx, float sy, float sz, float xt,
                                           float yt, float zt, float *ox, float *oy, float *oz) {
   *ox = sx; *oy = sy; *oz = sz;
   if (sx >= g.xmin && sx <= g.xmax && sy >= g.ymin && sy <= g.ymax && sz >= g.zmin && sz <= g.zmax)
     return;
+  ray_start_outside(g, sx, sy, sz, xt, yt, zt, ox, oy, oz);
+}
+
+// emitters outside the box (rare: only sources placed outside it)
+static __device__ __noinline__ void ray_start_outside(const GridDev &g, float sx, float sy, float sz,
+                                                      float xt, float yt, float zt, float *ox, float *oy,
+                                                      float *oz) {
   const double tiny = 1.0e-30;
   const float dx = __fsub_rn(xt, sx), dy = __fsub_rn(yt, sy), dz = __fsub_rn(zt, sz);
   const float s3 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));

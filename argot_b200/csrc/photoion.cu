@@ -116,6 +116,130 @@ __global__ void __launch_bounds__(32 * kRateWarps)
   }
 }
 
+// ------------------------------------------------------------ FP32 rates
+// One warp per target block, rays in chunks of 32.  Phase A: lane i forms
+// the FP64 per-ray parameters of ray i of the chunk (geometry, columns,
+// prefactors).  Phase B: the warp splits into four groups of eight lanes;
+// a group takes one ray at a time and its lanes share the 256 frequency
+// bins (lane j: bins j, j+8, ...), reading the frequency tables from shared
+// memory; three butterfly steps sum the eight partial sums.  Phase C: lane
+// j adds the rays that end in cell j of the block, in ray order.
+constexpr int kF32Warps = 4;
+
+__global__ void __launch_bounds__(32 * kF32Warps)
+    k_rate_f32(GridDev g, const float4 *__restrict__ raw, const float4 *__restrict__ emit_pos,
+               const float *__restrict__ specn, const double *__restrict__ total, uint64_t b0, uint64_t b1,
+               const uint64_t *__restrict__ blk_off, uint64_t base, const uint32_t *__restrict__ rays,
+               uint64_t nray, const float *__restrict__ tau, float *__restrict__ rates6) {
+  __shared__ float4 s_tab[3 * kNu];
+  __shared__ float s_nd[kF32Warps][32][6];
+  __shared__ double s_p[kF32Warps][32][3];
+  __shared__ double s_out[kF32Warps][32][6];
+  __shared__ int s_e[kF32Warps][32], s_t[kF32Warps][32];
+  for (int k = threadIdx.x; k < kNu; k += blockDim.x) {
+    s_tab[3 * k + 0] = make_float4(c_tab.cs_l2e[0][k], c_tab.cs_l2e[1][k], c_tab.cs_l2e[2][k], c_tab.cs[0][k]);
+    s_tab[3 * k + 1] = make_float4(c_tab.cs[1][k], c_tab.cs[2][k], c_tab.hw[0][k], c_tab.hw[1][k]);
+    s_tab[3 * k + 2] = make_float4(c_tab.hw[2][k], 0.f, 0.f, 0.f);
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int grp = lane >> 3, j = lane & 7;
+  const unsigned gmask = 0xffu << (8 * grp);
+  const float ln2 = 0.69314718055994531f;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
+  for (uint64_t b = b0 + warp; b < b1; b += nwarp) {
+    int ix, iy, iz;
+    const bool own_valid = block_cell(g, b, lane, &ix, &iy, &iz);
+    const uint64_t own = own_valid ? cell_index(g, ix, iy, iz) : 0;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    int bix, biy, biz;
+    block_cell(g, b, 0, &bix, &biy, &biz);
+    const uint64_t r0 = blk_off[b] - base, r1 = blk_off[b + 1] - base;
+    for (uint64_t rc = r0; rc < r1; rc += 32) {
+      // phase A
+      const uint64_t r = rc + lane;
+      int t = -1;
+      if (r < r1) {
+        const uint32_t w = __ldg(rays + r);
+        const uint32_t e = w >> 5;
+        t = (int)(w & 31u);
+        const int lx = bix + (t >> 4), ly = biy + ((t >> 2) & 3), lz = biz + (t & 3);
+        const float4 ep = __ldg(emit_pos + e);
+        const RayGeom geo = ray_geometry(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z);
+        const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
+        const RayCols cols = ray_columns(g, __ldg(tau + r), __ldg(tau + nray + r), __ldg(tau + 2 * nray + r), rw, geo);
+        const RayParams p = ray_params(cols, __ldg(total + e));
+#pragma unroll
+        for (int s = 0; s < 3; s++) {
+          s_nd[wib][lane][s] = p.N[s];
+          s_nd[wib][lane][3 + s] = p.D[s];
+          s_p[wib][lane][s] = p.P[s];
+        }
+        s_e[wib][lane] = (int)e;
+      }
+      s_t[wib][lane] = t;
+      __syncwarp();
+      const int nk = (int)min((uint64_t)32, r1 - rc);
+      // phase B
+      for (int q = grp; q < nk; q += 4) {
+        const float N0 = s_nd[wib][q][0], N1 = s_nd[wib][q][1], N2 = s_nd[wib][q][2];
+        const float D0 = s_nd[wib][q][3], D1 = s_nd[wib][q][4], D2 = s_nd[wib][q][5];
+        const float *sp = specn + (size_t)s_e[wib][q] * kNu;
+        float g0 = 0.f, g1 = 0.f, g2 = 0.f, h0 = 0.f, h1 = 0.f, h2 = 0.f;
+#pragma unroll 4
+        for (int m = 0; m < kNu / 8; m++) {
+          const int k = j + 8 * m;
+          const float4 A = s_tab[3 * k + 0], B = s_tab[3 * k + 1], Cq = s_tab[3 * k + 2];
+          const float tl2 = fmaf(N0, A.x, fmaf(N1, A.y, N2 * A.z));
+          const float dl2 = fmaf(D0, A.x, fmaf(D1, A.y, D2 * A.z));
+          const float e = ex2_approx(-tl2);
+          const float ed = ex2_approx(-dl2);
+          const float wv = __ldg(sp + k) * e * phi_pc(dl2 * ln2, ed);
+          g0 = fmaf(A.w, wv, g0);
+          g1 = fmaf(B.x, wv, g1);
+          g2 = fmaf(B.y, wv, g2);
+          h0 = fmaf(B.z, wv, h0);
+          h1 = fmaf(B.w, wv, h1);
+          h2 = fmaf(Cq.x, wv, h2);
+        }
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+          g0 += __shfl_xor_sync(gmask, g0, o);
+          g1 += __shfl_xor_sync(gmask, g1, o);
+          g2 += __shfl_xor_sync(gmask, g2, o);
+          h0 += __shfl_xor_sync(gmask, h0, o);
+          h1 += __shfl_xor_sync(gmask, h1, o);
+          h2 += __shfl_xor_sync(gmask, h2, o);
+        }
+        if (j == 0) {
+          const double p0 = s_p[wib][q][0], p1 = s_p[wib][q][1], p2 = s_p[wib][q][2];
+          s_out[wib][q][0] = p0 * g0;
+          s_out[wib][q][1] = p1 * g1;
+          s_out[wib][q][2] = p2 * g2;
+          s_out[wib][q][3] = p0 * h0 * kHNuL;
+          s_out[wib][q][4] = p1 * h1 * kHNuL;
+          s_out[wib][q][5] = p2 * h2 * kHNuL;
+        }
+      }
+      __syncwarp();
+      // phase C
+      for (int k = 0; k < nk; k++) {
+        if (s_t[wib][k] == lane) {
+#pragma unroll
+          for (int s = 0; s < 6; s++) acc[s] += s_out[wib][k][s];
+        }
+      }
+      __syncwarp();
+    }
+    if (own_valid) {
+#pragma unroll
+      for (int s = 0; s < 6; s++) rates6[s * ncell + own] = (float)acc[s];
+    }
+  }
+}
+
 // ------------------------------------------------------------- drop-in rays
 // Per-ray rates of the reference's light_ray_IO array (one thread per ray).
 __global__ void k_rate_rayio(GridDev g, const float4 *__restrict__ raw, const light_ray_IO *__restrict__ rays,
@@ -251,9 +375,8 @@ extern "C" int argot_b200_photoion_rays(const argot_b200_grid *gp, const void *p
         g, raw, t->emit_pos, t->emit_spec64, t->emit_specn, t->emit_total, b0, b1, blk_off, base, rays, nray, tau,
         rates6);
   else
-    k_rate_blocks<ARGOT_B200_RATE_EXACT_F32><<<blocks, threads, 0, st>>>(
-        g, raw, t->emit_pos, t->emit_spec64, t->emit_specn, t->emit_total, b0, b1, blk_off, base, rays, nray, tau,
-        rates6);
+    k_rate_f32<<<grid_blocks_for_rates((b1 - b0) * 32, 32 * kF32Warps), 32 * kF32Warps, 0, st>>>(
+        g, raw, t->emit_pos, t->emit_specn, t->emit_total, b0, b1, blk_off, base, rays, nray, tau, rates6);
   ARGOT_CUDA_TRY(cudaGetLastError());
   set_status(0);
   return 0;

@@ -120,7 +120,26 @@ __device__ __forceinline__ float phi_pc(float x, float e_minus_x) {
     p = fma(d, p, 1.0);
     return (float)p;
   }
-  return (1.0f - e_minus_x) / x;
+  return __fdividef(1.0f - e_minus_x, x);
+}
+
+// Per-ray parameters of the FP32 bin loop: columns to the cell's entry face
+// and of the cell [cm^-2] as floats, and the FP64 prefactors
+// total * dN_s / (n_s V_shell) of the three species.
+struct RayParams {
+  float N[3], D[3];
+  double P[3];
+};
+
+__device__ __forceinline__ RayParams ray_params(const RayCols &c, double total) {
+  RayParams p;
+#pragma unroll
+  for (int s = 0; s < 3; s++) {
+    p.N[s] = (float)c.N[s];
+    p.D[s] = (float)c.dN[s];
+    p.P[s] = total * c.dN[s] * c.rN[s];
+  }
+  return p;
 }
 
 // FP32 rates: the same integral with the spectrum normalised by its total

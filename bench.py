@@ -35,7 +35,7 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-CONFIGS = ("largest", "plain", "precision", "learned", "tiny")
+CONFIGS = ("largest", "plain", "precision", "learned", "tiny", "plain256")
 METRIC = "ray-cell crossings/s (march+stitch+rates, 1 B200)"
 UNIT = "crossings/s"
 
@@ -53,6 +53,9 @@ def make_workload(name: str, rank: int = 0):
         return W.learned(seed=4 + seed_shift)
     if name == "tiny":
         return W.tiny(32, 16, seed=7 + seed_shift)
+    if name == "plain256":
+        # profiling case: a field larger than L2 with few rays (~4 GB on the device)
+        return W.plain(edge=256, nsrc=16, seed=1 + seed_shift)
     raise ValueError(name)
 
 
