@@ -71,6 +71,18 @@ SIGNATURES = {
     "argot_b200_tables": (None, [vp, vp]),
     "argot_b200_photon_rate": (None, [i32, f32, f64, vp]),
     "argot_b200_photon_counts": (None, [i32, f32, vp, vp]),
+    "argot_b200_dev_tree_set_blackbody": (i32, [vp, vp, vp, vp]),
+    "argot_b200_mlp_num_params": (i32, []),
+    "argot_b200_mlp_spectra": (i32, [i32, vp, vp]),
+    "argot_b200_mlp_samples": (i32, [vp, vp, i32, u64, u64, vp, vp, vp]),
+    "argot_b200_mlp_workspace": (u64, [i32]),
+    "argot_b200_mlp_forward": (i32, [vp, vp, i32, vp, vp]),
+    "argot_b200_mlp_train_step": (i32, [vp, vp, vp, vp, vp, i32, f32, i32, vp, vp, vp, vp]),
+    "argot_b200_surrogate_create": (i32, [vp, vp, f32, C.POINTER(vp)]),
+    "argot_b200_surrogate_free": (None, [vp]),
+    "argot_b200_surrogate_eval": (i32, [vp, vp, i32, vp, vp]),
+    "argot_b200_photoion_rays_surrogate": (i32, [GP, vp, vp, vp, u64, u64, vp, u64, vp, u64, vp, vp, vp,
+                                                 vp]),
 }
 
 _lock = threading.Lock()

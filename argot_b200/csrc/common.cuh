@@ -58,6 +58,9 @@ int ensure_tables(int device);
 
 // Host copies of the tables (computed with the reference's formulas).
 void host_tables(double *nu, float *cs3);
+// Weights of the six rate integrals per bin (6 x 256): sigma_s(nu) and
+// sigma_s(nu) * ((float)nu - nu_s)^+ for s = HI, HeI, HeII.
+void host_rate_weights(double *w6);
 
 // Emitters and tree on the device.
 struct DevNode {
@@ -81,4 +84,9 @@ struct argot_b200_dev_tree {
   double *emit_spec64;     // n_emit x 256
   float *emit_specn;       // n_emit x 256: spectrum / total
   double *emit_total;      // n_emit
+  // surrogate inputs (set by argot_b200_dev_tree_set_blackbody): log10 T of
+  // an emitter whose spectrum is a single-temperature blackbody (NaN
+  // otherwise) and its six thin-limit integrals sum_nu w_j(nu) s_nu
+  float *emit_logT;        // n_emit
+  double *emit_i0;         // n_emit x 6
 };

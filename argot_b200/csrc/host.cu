@@ -75,6 +75,21 @@ void host_tables(double *nu, float *cs3) {
   }
 }
 
+void host_rate_weights(double *w6) {
+  double nu[kNu];
+  float cs3[3 * kNu];
+  host_tables(nu, cs3);
+  const double thr[3] = {kThrHI, kThrHeI, kThrHeII};
+  for (int k = 0; k < kNu; k++) {
+    const double nf = (double)(float)nu[k];
+    for (int s = 0; s < 3; s++) {
+      const double c = cs3[3 * k + s];
+      w6[s * kNu + k] = c;
+      w6[(3 + s) * kNu + k] = c * (nf > thr[s] ? nf - thr[s] : 0.0);
+    }
+  }
+}
+
 // ----------------------------------------------------------- photon rates
 // Blackbody (photon-number shape nu^2/(e^{h nu/kT}-1), normalised at the
 // Lyman limit) or power law nu^p; per-bin photon counts by the iterated
@@ -470,7 +485,52 @@ void argot_b200_dev_tree_free(argot_b200_dev_tree *d) {
   cudaFree(d->emit_spec64);
   cudaFree(d->emit_specn);
   cudaFree(d->emit_total);
+  cudaFree(d->emit_logT);
+  cudaFree(d->emit_i0);
   delete d;
+}
+
+// Spectral temperature of every emitter for the surrogate: a node whose
+// sources are all blackbodies of one temperature T (src_T[i] > 0) has the
+// normalised spectrum of that blackbody; any other emitter gets NaN and
+// is always integrated exactly.  Also uploads each emitter's six thin-limit
+// integrals sum_nu w_j(nu) s_nu of its own normalised spectrum.
+int argot_b200_dev_tree_set_blackbody(const argot_b200_tree *t, argot_b200_dev_tree *d, const float *src_T,
+                                      void *stream) {
+  if (!t || !d || !src_T || d->n_src != t->nsrc) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
+  const size_t nn = t->nodes.size(), ne = nn + t->nsrc;
+  std::vector<float> logT(ne);
+  const float qnan = std::nanf("");
+  auto temp_of = [&](float T) { return (T > 0.f) ? (float)std::log10((double)T) : qnan; };
+  for (size_t i = 0; i < nn; i++) {
+    const DevNode &nd = t->nodes[i];
+    float T0 = src_T[t->src_list[nd.src_first]];
+    bool same = T0 > 0.f;
+    for (int j = 1; j < nd.n && same; j++) same = src_T[t->src_list[nd.src_first + j]] == T0;
+    logT[i] = same ? temp_of(T0) : qnan;
+  }
+  for (int j = 0; j < t->nsrc; j++) logT[nn + j] = temp_of(src_T[j]);
+  std::vector<double> w(6 * kNu), i0(6 * ne);
+  host_rate_weights(w.data());
+  std::vector<double> spec(ne * kNu);
+  argot_b200_tree_emitters(t, nullptr, spec.data());
+  for (size_t e = 0; e < ne; e++) {
+    double tot = 0.0;
+    for (int k = 0; k < kNu; k++) tot += spec[e * kNu + k];
+    for (int j = 0; j < 6; j++) {
+      double s = 0.0;
+      for (int k = 0; k < kNu; k++) s += w[j * kNu + k] * (spec[e * kNu + k] / tot);
+      i0[e * 6 + j] = s;
+    }
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!d->emit_logT) ARGOT_CUDA_TRY(cudaMalloc(&d->emit_logT, sizeof(float) * ne));
+  if (!d->emit_i0) ARGOT_CUDA_TRY(cudaMalloc(&d->emit_i0, sizeof(double) * 6 * ne));
+  ARGOT_CUDA_TRY(cudaMemcpyAsync(d->emit_logT, logT.data(), sizeof(float) * ne, cudaMemcpyHostToDevice, st));
+  ARGOT_CUDA_TRY(cudaMemcpyAsync(d->emit_i0, i0.data(), sizeof(double) * 6 * ne, cudaMemcpyHostToDevice, st));
+  ARGOT_CUDA_TRY(cudaStreamSynchronize(st));
+  set_status(0);
+  return 0;
 }
 
 }  // extern "C"

@@ -112,8 +112,8 @@ static __device__ __noinline__ Tau3 march_reference(const GridDev &g, const floa
 // rounding scales with the cell rather than with the ray length as a running
 // position or an absolute path parameter would; the walk always ends in the
 // end cell after at most sum|di| steps.  The last chord is measured from
-// the face through which the end cell was entered.  Columns are
-// Kahan-compensated FP32 sums.
+// the face through which the end cell was entered.  Columns are FP32 with
+// compensated (Kahan) summation.
 __device__ __forceinline__ void kahan_add(float &s, float &c, float v) {
   const float y = v - c;
   const float tt = s + y;
@@ -121,103 +121,90 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float v) {
   s = tt;
 }
 
-// Walk state: yields (chord, cell) for every cell from the start cell to the
-// end cell; the last chord runs from the end cell's entry face to the end
-// point.
-struct CountdownWalk {
-  float rx, ry, rz, tdx, tdy, tdz, iax, iay, iaz, ax, ay, az, len, x1, y1, z1;
-  int ix, iy, iz, cx, cy, cz, stx, sty, stz, last, left;
-};
-
-__device__ __forceinline__ void walk_init(CountdownWalk &w, const GridDev &g, float xs, float ys, float zs,
-                                          float xe, float ye, float ze) {
-  const int ixe = axis_cell(xe, g.xminl, g.dx, g.nx);
-  const int iye = axis_cell(ye, g.yminl, g.dy, g.ny);
-  const int ize = axis_cell(ze, g.zminl, g.dz, g.nz);
-  w.ix = axis_cell(xs, g.xminl, g.dx, g.nx);
-  w.iy = axis_cell(ys, g.yminl, g.dy, g.ny);
-  w.iz = axis_cell(zs, g.zminl, g.dz, g.nz);
-  const float x0 = xs - g.xminl, y0 = ys - g.yminl, z0 = zs - g.zminl;
-  w.x1 = xe - g.xminl; w.y1 = ye - g.yminl; w.z1 = ze - g.zminl;
-  const float dx = xe - xs, dy = ye - ys, dz = ze - zs;
-  w.len = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-  const float il = w.len > 0.f ? 1.0f / w.len : 0.f;
-  w.ax = fabsf(cosine_guard(dx * il));
-  w.ay = fabsf(cosine_guard(dy * il));
-  w.az = fabsf(cosine_guard(dz * il));
-  w.iax = 1.0f / w.ax; w.iay = 1.0f / w.ay; w.iaz = 1.0f / w.az;
-  w.cx = abs(ixe - w.ix); w.cy = abs(iye - w.iy); w.cz = abs(ize - w.iz);
-  w.stx = ixe > w.ix ? 1 : -1; w.sty = iye > w.iy ? 1 : -1; w.stz = ize > w.iz ? 1 : -1;
-  const float kInf = __int_as_float(0x7f800000);
-  w.rx = w.cx ? fmaxf(fabsf(fmaf(g.dx, (float)(w.ix + (w.stx > 0)), -x0)) * w.iax, 0.f) : kInf;
-  w.ry = w.cy ? fmaxf(fabsf(fmaf(g.dy, (float)(w.iy + (w.sty > 0)), -y0)) * w.iay, 0.f) : kInf;
-  w.rz = w.cz ? fmaxf(fabsf(fmaf(g.dz, (float)(w.iz + (w.stz > 0)), -z0)) * w.iaz, 0.f) : kInf;
-  w.tdx = g.dx * w.iax; w.tdy = g.dy * w.iay; w.tdz = g.dz * w.iaz;
-  w.last = -1;
-  w.left = w.cx + w.cy + w.cz + 1;  // entries still to yield (bounded)
-}
-
-// Next (chord, cell); false when the walk is exhausted.
-__device__ __forceinline__ bool walk_next(CountdownWalk &w, const GridDev &g, float *r_out, size_t *c_out) {
-  if (w.left <= 0) return false;
-  w.left--;
-  *c_out = cell_index(g, w.ix, w.iy, w.iz);
-  if ((w.cx | w.cy | w.cz) && w.left > 0) {
-    const float kInf = __int_as_float(0x7f800000);
-    const float r = fminf(w.rx, fminf(w.ry, w.rz));
-    float best = -1.f;
-    if (w.rx == r) { w.ix += w.stx; w.cx--; w.rx = w.cx ? w.tdx : kInf; if (w.ax > best) { best = w.ax; w.last = 0; } } else { w.rx -= r; }
-    if (w.ry == r) { w.iy += w.sty; w.cy--; w.ry = w.cy ? w.tdy : kInf; if (w.ay > best) { best = w.ay; w.last = 1; } } else { w.ry -= r; }
-    if (w.rz == r) { w.iz += w.stz; w.cz--; w.rz = w.cz ? w.tdz : kInf; if (w.az > best) { best = w.az; w.last = 2; } } else { w.rz -= r; }
-    // a step that crosses several faces at once (a corner) ends the walk
-    // early; the remaining budget shrinks with it
-    w.left = min(w.left, w.cx + w.cy + w.cz + 1);
-    *r_out = r;
-    return true;
-  }
-  // the end cell: chord from its entry face to the end point
-  float depth;
-  if (w.last == 0)
-    depth = fabsf(w.x1 - g.dx * (float)(w.ix + (w.stx < 0))) * w.iax;
-  else if (w.last == 1)
-    depth = fabsf(w.y1 - g.dy * (float)(w.iy + (w.sty < 0))) * w.iay;
-  else if (w.last == 2)
-    depth = fabsf(w.z1 - g.dz * (float)(w.iz + (w.stz < 0))) * w.iaz;
-  else
-    depth = w.len;
-  w.left = 0;
-  *r_out = depth;
-  return true;
-}
-
-// The walk with a two-deep software pipeline: the gathers of the next two
-// cells are in flight while the current one is accumulated (the cell
-// sequence does not depend on the densities).
+// The walk.  Per step: the nearest face among the axes with faces left;
+// the chord belongs to the current cell; the crossed axes advance the
+// 32-bit cell index by their precomputed strides and reset their distance
+// to the face spacing, the others shorten theirs.  The gather of the next
+// cell is issued before the current one is accumulated.  Chords are summed
+// with FMA into per-species partial sums that are folded into Kahan sums
+// every 16 steps (compensated summation over blocks of 16 terms).  The last
+// chord runs from the end cell's entry face -- on the crossed axis with the
+// largest |u| -- to the end point.
 static __device__ __forceinline__ Tau3 march_kahan(const GridDev &g, const float4 *__restrict__ cells,
                                                    float xs, float ys, float zs, float xe, float ye,
                                                    float ze, int *steps, bool *bad) {
-  CountdownWalk w;
-  walk_init(w, g, xs, ys, zs, xe, ye, ze);
+  const int ixe = axis_cell(xe, g.xminl, g.dx, g.nx);
+  const int iye = axis_cell(ye, g.yminl, g.dy, g.ny);
+  const int ize = axis_cell(ze, g.zminl, g.dz, g.nz);
+  const int ix = axis_cell(xs, g.xminl, g.dx, g.nx);
+  const int iy = axis_cell(ys, g.yminl, g.dy, g.ny);
+  const int iz = axis_cell(zs, g.zminl, g.dz, g.nz);
+  const float x0 = xs - g.xminl, y0 = ys - g.yminl, z0 = zs - g.zminl;
+  const float dx = xe - xs, dy = ye - ys, dz = ze - zs;
+  const float len = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+  const float il = len > 0.f ? 1.0f / len : 0.f;
+  const float ax = fabsf(cosine_guard(dx * il)), ay = fabsf(cosine_guard(dy * il)),
+              az = fabsf(cosine_guard(dz * il));
+  const float iax = 1.0f / ax, iay = 1.0f / ay, iaz = 1.0f / az;
+  int cx = abs(ixe - ix), cy = abs(iye - iy), cz = abs(ize - iz);
+  const int stx = ixe > ix ? 1 : -1, sty = iye > iy ? 1 : -1, stz = ize > iz ? 1 : -1;
+  const float kInf = __int_as_float(0x7f800000);
+  float rx = cx ? fmaxf(fabsf(fmaf(g.dx, (float)(ix + (stx > 0)), -x0)) * iax, 0.f) : kInf;
+  float ry = cy ? fmaxf(fabsf(fmaf(g.dy, (float)(iy + (sty > 0)), -y0)) * iay, 0.f) : kInf;
+  float rz = cz ? fmaxf(fabsf(fmaf(g.dz, (float)(iz + (stz > 0)), -z0)) * iaz, 0.f) : kInf;
+  const float tdx = g.dx * iax, tdy = g.dy * iay, tdz = g.dz * iaz;
+  const int dsz = stz, dsy = sty * g.nz, dsx = stx * g.nz * g.ny;
+  int idx = iz + g.nz * (iy + g.ny * ix);
+
+  float4 n = __ldg(cells + idx);
+  float p0 = 0.f, p1 = 0.f, p2 = 0.f;
   float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
-  float ra = 0.f, rb = 0.f;
-  size_t ca = 0, cb = 0;
-  float4 na = make_float4(0.f, 0.f, 0.f, 0.f), nb = na;
-  bool ha = walk_next(w, g, &ra, &ca);
-  if (ha) na = ld_cell(cells, ca);
-  bool hb = walk_next(w, g, &rb, &cb);
-  if (hb) nb = ld_cell(cells, cb);
-  int n = 0;
-  while (ha) {
-    kahan_add(s0, c0, ra * na.x);
-    kahan_add(s1, c1, ra * na.y);
-    kahan_add(s2, c2, ra * na.z);
-    n++;
-    ha = hb; ra = rb; na = nb;
-    hb = walk_next(w, g, &rb, &cb);
-    if (hb) nb = ld_cell(cells, cb);
+  const int cap = cx + cy + cz;  // every finite step crosses at least one face
+  int it = 0, lastmask = 0;
+  while ((cx | cy | cz) && it < cap) {
+    const float r = fminf(rx, fminf(ry, rz));
+    const bool hx = rx == r, hy = ry == r, hz = rz == r;
+    idx += (hx ? dsx : 0) + (hy ? dsy : 0) + (hz ? dsz : 0);
+    const float4 nn = __ldg(cells + idx);
+    p0 = fmaf(r, n.x, p0);
+    p1 = fmaf(r, n.y, p1);
+    p2 = fmaf(r, n.z, p2);
+    cx -= hx; cy -= hy; cz -= hz;
+    rx = hx ? (cx ? tdx : kInf) : rx - r;
+    ry = hy ? (cy ? tdy : kInf) : ry - r;
+    rz = hz ? (cz ? tdz : kInf) : rz - r;
+    lastmask = (hx ? 1 : 0) | (hy ? 2 : 0) | (hz ? 4 : 0);
+    n = nn;
+    if ((++it & 15) == 0) {
+      kahan_add(s0, c0, p0);
+      kahan_add(s1, c1, p1);
+      kahan_add(s2, c2, p2);
+      p0 = p1 = p2 = 0.f;
+    }
   }
-  if (w.cx | w.cy | w.cz) *bad = true;  // only non-finite input leaves faces uncrossed
-  *steps = n;
+  if (cx | cy | cz) *bad = true;  // only non-finite input leaves faces uncrossed
+  float depth = len;
+  if (lastmask) {
+    // among the axes crossed last, the one with the largest |u|
+    int a = -1;
+    float best = -1.f;
+    if ((lastmask & 1) && ax > best) { best = ax; a = 0; }
+    if ((lastmask & 2) && ay > best) { best = ay; a = 1; }
+    if ((lastmask & 4) && az > best) { best = az; a = 2; }
+    if (a == 0)
+      depth = fabsf((xe - g.xminl) - g.dx * (float)(ixe + (stx < 0))) * iax;
+    else if (a == 1)
+      depth = fabsf((ye - g.yminl) - g.dy * (float)(iye + (sty < 0))) * iay;
+    else
+      depth = fabsf((ze - g.zminl) - g.dz * (float)(ize + (stz < 0))) * iaz;
+  }
+  p0 = fmaf(depth, n.x, p0);
+  p1 = fmaf(depth, n.y, p1);
+  p2 = fmaf(depth, n.z, p2);
+  kahan_add(s0, c0, p0);
+  kahan_add(s1, c1, p1);
+  kahan_add(s2, c2, p2);
+  *steps = it + 1;
   return Tau3{s0, s1, s2};
 }
 

@@ -3,39 +3,12 @@
 #include "photoion.cuh"
 #include "ref_layout.h"
 
-#include <mutex>
-
 namespace argot {
 
 int grid_blocks_for_rates(uint64_t n, int threads);
 
-int ensure_tables(int device) {
-  static std::mutex mu;
-  static bool done[64] = {false};
-  std::lock_guard<std::mutex> lock(mu);
-  if (device < 0 || device >= 64) return ARGOT_B200_EINVAL;
-  if (done[device]) return 0;
-  double nu[kNu];
-  float cs3[3 * kNu];
-  host_tables(nu, cs3);
-  RateTables t;
-  const double thr[3] = {kThrHI, kThrHeI, kThrHeII};
-  const double l2e = 1.4426950408889634074;
-  for (int i = 0; i < kNu; i++) {
-    const float nf = (float)nu[i];
-    t.nu_f[i] = nf;
-    for (int s = 0; s < 3; s++) {
-      const float c = cs3[3 * i + s];
-      t.cs[s][i] = c;
-      t.cs_l2e[s][i] = (float)((double)c * l2e);
-      const double w = ((double)nf > thr[s]) ? ((double)nf - thr[s]) : 0.0;
-      t.hw[s][i] = (float)((double)c * w);
-    }
-  }
-  ARGOT_CUDA_TRY(cudaMemcpyToSymbol(c_tab, &t, sizeof(t)));
-  done[device] = true;
-  return 0;
-}
+// the tables of this translation unit's rate kernels
+int ensure_tables(int device) { return ensure_rate_tables(device); }
 
 constexpr int kRateWarps = 4;  // warps per CTA in the block-rate kernel
 

@@ -1,14 +1,46 @@
 // photoion.cuh -- per-ray photo-ionisation / heating rates
 // (calc_photoion_rate, photon-conserving branch, H + He, not cosmological).
 #pragma once
+#include <mutex>
+
 #include "march.cuh"
 
 namespace argot {
 
 constexpr double kHNuL = kHPlanck * kNuL;  // hplanck*nuL, double
 
-// Frequency tables of the rate kernels (filled by ensure_tables).
+// Frequency tables of the rate kernels.  Every translation unit that
+// includes this header has its own copy in its constant bank, filled by its
+// own ensure_rate_tables().
 __constant__ RateTables c_tab;
+
+static int ensure_rate_tables(int device) {
+  static std::mutex mu;
+  static bool done[64] = {false};
+  std::lock_guard<std::mutex> lock(mu);
+  if (device < 0 || device >= 64) return ARGOT_B200_EINVAL;
+  if (done[device]) return 0;
+  double nu[kNu];
+  float cs3[3 * kNu];
+  host_tables(nu, cs3);
+  RateTables t;
+  const double thr[3] = {kThrHI, kThrHeI, kThrHeII};
+  const double l2e = 1.4426950408889634074;
+  for (int i = 0; i < kNu; i++) {
+    const float nf = (float)nu[i];
+    t.nu_f[i] = nf;
+    for (int s = 0; s < 3; s++) {
+      const float c = cs3[3 * i + s];
+      t.cs[s][i] = c;
+      t.cs_l2e[s][i] = (float)((double)c * l2e);
+      const double w = ((double)nf > thr[s]) ? ((double)nf - thr[s]) : 0.0;
+      t.hw[s][i] = (float)((double)c * w);
+    }
+  }
+  ARGOT_CUDA_TRY(cudaMemcpyToSymbol(c_tab, &t, sizeof(t)));
+  done[device] = true;
+  return 0;
+}
 
 // Geometry shared by both precisions (calc_photoion_rate.c:176-246, FP32
 // where the reference uses float): target centre, distance, and the cell

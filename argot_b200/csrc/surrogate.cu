@@ -1,0 +1,553 @@
+// surrogate.cu -- per-cell rates with the BF16 MLP surrogate of the
+// frequency integral, evaluated on the tensor cores, and the exact FP32
+// quadrature as fallback.
+//
+// Photon-conserving cell factor.  For every frequency
+//   e^{-tau} (1 - e^{-dtau}) / dtau = int_0^1 e^{-(tau + u dtau)} du,
+// so the reference's sum over bins (calc_photoion_rate.c:327-386) equals
+//   Gamma_s = P_s int_0^1 I_s(N + u dN) du,  P_s = Ndot dN_s / (n_s V_shell),
+// with I_j(M) the thin-cell integral of mlp.cuh at column M.  The integral
+// over u is taken by Gauss-Legendre quadrature with 1, 2 or 3 nodes chosen
+// from the cell's largest optical depth dtau_max (quadrature error < 3e-5);
+// the network gives I_j / I_j0 at each node and the emitter's exact thin
+// integrals I_j0 restore the scale.
+//
+// A ray takes the exact FP32 quadrature instead when its emitter is not a
+// single-temperature blackbody in [1e4, 10^5.5] K, when dtau_max > 2, when a
+// node's log10 tau lies above 3, or when the validated error bound of the
+// network at the predicted outputs (the envelope measured on held-out
+// samples) exceeds the tolerance.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "mlp.cuh"
+#include "photoion.cuh"
+
+namespace argot {
+
+int grid_blocks_for_rates(uint64_t n, int threads);
+
+constexpr int kEnvBins = 64;
+constexpr float kEnvTMax = 6.0f;
+constexpr int kSurWarps = 4;
+constexpr int kMaxEval = 96;  // 32 rays x 3 quadrature nodes
+
+// B-fragments of the four layers (mma.m16n8k16, BF16), biases, envelope.
+struct SurWeights {
+  uint2 f1[8][32];        // layer 1: 8 N-tiles x 1 K-step (input hi|lo in k 0..7)
+  uint2 f2[8][4][32];     // layer 2: 8 N-tiles x 4 K-steps
+  uint2 f3[8][4][32];     // layer 3
+  uint2 f4[8][32];        // layer 4: 1 N-tile x 8 K-steps (hidden hi | lo)
+  float b1[64], b2[64], b3[64], b4[8];
+  float env[6][kEnvBins];
+  float sig0[3];
+  float tol;
+};
+
+struct SurSmem {
+  SurWeights w;
+  float4 tab[3 * kNu];
+  // per warp
+  float x[kSurWarps][kMaxEval][4];     // normalised network inputs
+  float tout[kSurWarps][kMaxEval][6];  // network outputs t_j
+  float nd[kSurWarps][32][6];          // N_s, dN_s (cm^-2, float)
+  double p[kSurWarps][32][3];          // prefactors
+  double out[kSurWarps][32][6];        // per-ray rates
+  int e[kSurWarps][32], t[kSurWarps][32], ev0[kSurWarps][32], nq[kSurWarps][32];
+};
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint2 b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b.x), "r"(b.y));
+}
+
+// The network on 16 evaluations (rows r0..r0+15 of the warp's list).  The
+// m16n8 accumulator of one layer is, register for register, the A fragment
+// of the next (N-tiles 2kk, 2kk+1 -> K-step kk), so activations never leave
+// the registers.
+__device__ __forceinline__ void mlp_tile16(const SurWeights &W, const float (*x)[4], float (*tout)[6],
+                                           int r0, int lane) {
+  const int g = lane >> 2, tq = lane & 3;
+  // layer 1: A = [hi(x) | lo(x) | 0] (k = 0..3 | 4..7 | 8..15)
+  uint32_t a[4];
+  {
+    const int c0 = (2 * tq) & 3;  // columns 2tq, 2tq+1 of the 8 used
+    const bool lo = tq >= 2;
+    float v[4];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const float *xr = x[r0 + g + 8 * h];
+      const float x0 = xr[c0], x1 = xr[c0 + 1];
+      const float h0 = bf16_round(x0), h1 = bf16_round(x1);
+      v[2 * h + 0] = lo ? x0 - h0 : h0;
+      v[2 * h + 1] = lo ? x1 - h1 : h1;
+    }
+    a[0] = pack_bf16x2(v[0], v[1]);
+    a[1] = pack_bf16x2(v[2], v[3]);
+    a[2] = 0u;
+    a[3] = 0u;
+  }
+  float acc[8][4];
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const float bb0 = W.b1[8 * j + 2 * tq], bb1 = W.b1[8 * j + 2 * tq + 1];
+    acc[j][0] = bb0; acc[j][1] = bb1; acc[j][2] = bb0; acc[j][3] = bb1;
+    mma_bf16(acc[j], a, W.f1[j][lane]);
+  }
+  // layers 2 and 3
+  uint32_t A[4][4];
+#pragma unroll
+  for (int layer = 0; layer < 2; layer++) {
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+      A[kk][0] = pack_bf16x2(silu_fast(acc[2 * kk][0]), silu_fast(acc[2 * kk][1]));
+      A[kk][1] = pack_bf16x2(silu_fast(acc[2 * kk][2]), silu_fast(acc[2 * kk][3]));
+      A[kk][2] = pack_bf16x2(silu_fast(acc[2 * kk + 1][0]), silu_fast(acc[2 * kk + 1][1]));
+      A[kk][3] = pack_bf16x2(silu_fast(acc[2 * kk + 1][2]), silu_fast(acc[2 * kk + 1][3]));
+    }
+    const float *bias = layer == 0 ? W.b2 : W.b3;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const float bb0 = bias[8 * j + 2 * tq], bb1 = bias[8 * j + 2 * tq + 1];
+      acc[j][0] = bb0; acc[j][1] = bb1; acc[j][2] = bb0; acc[j][3] = bb1;
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++)
+        mma_bf16(acc[j], A[kk], layer == 0 ? W.f2[j][kk][lane] : W.f3[j][kk][lane]);
+    }
+  }
+  // layer 4 on the last hidden layer split as hi | lo
+  float o[4] = {W.b4[2 * tq], W.b4[2 * tq + 1], W.b4[2 * tq], W.b4[2 * tq + 1]};
+#pragma unroll
+  for (int kk = 0; kk < 4; kk++) {
+    float s[8];
+    s[0] = silu_fast(acc[2 * kk][0]); s[1] = silu_fast(acc[2 * kk][1]);
+    s[2] = silu_fast(acc[2 * kk][2]); s[3] = silu_fast(acc[2 * kk][3]);
+    s[4] = silu_fast(acc[2 * kk + 1][0]); s[5] = silu_fast(acc[2 * kk + 1][1]);
+    s[6] = silu_fast(acc[2 * kk + 1][2]); s[7] = silu_fast(acc[2 * kk + 1][3]);
+    uint32_t hi[4], lo[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const float h0 = bf16_round(s[2 * q]), h1 = bf16_round(s[2 * q + 1]);
+      hi[q] = pack_bf16x2(h0, h1);
+      lo[q] = pack_bf16x2(s[2 * q] - h0, s[2 * q + 1] - h1);
+    }
+    mma_bf16(o, hi, W.f4[kk][lane]);
+    mma_bf16(o, lo, W.f4[4 + kk][lane]);
+  }
+  if (tq < 3) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      tout[r0 + g + 8 * h][2 * tq] = fmaf(o[2 * h], kOutScale, kOutShift);
+      tout[r0 + g + 8 * h][2 * tq + 1] = fmaf(o[2 * h + 1], kOutScale, kOutShift);
+    }
+  }
+}
+
+// Gauss-Legendre nodes and weights on [0, 1]
+__device__ __forceinline__ void gl_node(int n, int i, float *u, float *w) {
+  if (n == 1) { *u = 0.5f; *w = 1.f; return; }
+  if (n == 2) { *u = i ? 0.78867513459481287f : 0.21132486540518713f; *w = 0.5f; return; }
+  const float uu[3] = {0.11270166537925831f, 0.5f, 0.88729833462074169f};
+  const float ww[3] = {5.f / 18.f, 8.f / 18.f, 5.f / 18.f};
+  *u = uu[i];
+  *w = ww[i];
+}
+
+__global__ void __launch_bounds__(32 * kSurWarps)
+    k_rate_sur(GridDev g, const float4 *__restrict__ raw, const float4 *__restrict__ emit_pos,
+               const float *__restrict__ specn, const double *__restrict__ total, const float *__restrict__ emit_logT,
+               const double *__restrict__ emit_i0, const SurWeights *__restrict__ wts, uint64_t b0, uint64_t b1,
+               const uint64_t *__restrict__ blk_off, uint64_t base, const uint32_t *__restrict__ rays, uint64_t nray,
+               const float *__restrict__ tau, float *__restrict__ rates6, unsigned long long *__restrict__ counters) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SurSmem &S = *reinterpret_cast<SurSmem *>(smem_raw);
+  {
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(wts);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(&S.w);
+    for (int i = threadIdx.x; i < (int)(sizeof(SurWeights) / 4); i += blockDim.x) dst[i] = src[i];
+    for (int k = threadIdx.x; k < kNu; k += blockDim.x) {
+      S.tab[3 * k + 0] = make_float4(c_tab.cs_l2e[0][k], c_tab.cs_l2e[1][k], c_tab.cs_l2e[2][k], c_tab.cs[0][k]);
+      S.tab[3 * k + 1] = make_float4(c_tab.cs[1][k], c_tab.cs[2][k], c_tab.hw[0][k], c_tab.hw[1][k]);
+      S.tab[3 * k + 2] = make_float4(c_tab.hw[2][k], 0.f, 0.f, 0.f);
+    }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int grp = lane >> 3, jj = lane & 7;
+  const unsigned gmask = 0xffu << (8 * grp);
+  const float ln2 = 0.69314718055994531f;
+  const float s00 = c_tab.cs[0][0];
+  const float s0a = c_tab.cs[0][44], s1a = c_tab.cs[1][44];
+  const float s0b = c_tab.cs[0][103], s1b = c_tab.cs[1][103], s2b = c_tab.cs[2][103];
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
+  unsigned long long n_sur = 0, n_exact = 0;
+  for (uint64_t b = b0 + warp; b < b1; b += nwarp) {
+    int ix, iy, iz;
+    const bool own_valid = block_cell(g, b, lane, &ix, &iy, &iz);
+    const uint64_t own = own_valid ? cell_index(g, ix, iy, iz) : 0;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    int bix, biy, biz;
+    block_cell(g, b, 0, &bix, &biy, &biz);
+    const uint64_t r0 = blk_off[b] - base, r1 = blk_off[b + 1] - base;
+    for (uint64_t rc = r0; rc < r1; rc += 32) {
+      // ---- phase A: per-ray parameters and quadrature nodes
+      const uint64_t r = rc + lane;
+      int tl = -1, nq = 0;
+      float xin[3][4];
+      if (r < r1) {
+        const uint32_t w = __ldg(rays + r);
+        const uint32_t e = w >> 5;
+        tl = (int)(w & 31u);
+        const int lx = bix + (tl >> 4), ly = biy + ((tl >> 2) & 3), lz = biz + (tl & 3);
+        const float4 ep = __ldg(emit_pos + e);
+        const RayGeom geo = ray_geometry(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z);
+        const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
+        const RayCols cols = ray_columns(g, __ldg(tau + r), __ldg(tau + nray + r), __ldg(tau + 2 * nray + r), rw, geo);
+        const RayParams p = ray_params(cols, __ldg(total + e));
+#pragma unroll
+        for (int s = 0; s < 3; s++) {
+          S.nd[wib][lane][s] = p.N[s];
+          S.nd[wib][lane][3 + s] = p.D[s];
+          S.p[wib][lane][s] = p.P[s];
+        }
+        S.e[wib][lane] = (int)e;
+        const float lT = __ldg(emit_logT + e);
+        const float dt0 = p.D[0] * s00;
+        const float dt1 = fmaf(p.D[0], s0a, p.D[1] * s1a);
+        const float dt2 = fmaf(p.D[0], s0b, fmaf(p.D[1], s1b, p.D[2] * s2b));
+        const float dtm = fmaxf(dt0, fmaxf(dt1, dt2));
+        nq = (lT >= kTLo && lT <= kTHi) ? (dtm <= 0.02f ? 1 : dtm <= 0.5f ? 2 : dtm <= 2.f ? 3 : 0) : 0;
+        for (int i = 0; i < nq; i++) {
+          float u, wq;
+          gl_node(nq, i, &u, &wq);
+#pragma unroll
+          for (int s = 0; s < 3; s++) {
+            const float m = fmaf(u, p.D[s], p.N[s]);
+            float lt = log10f(fmaxf(m * S.w.sig0[s], 1e-30f));
+            // beyond the trained range, or a negative entry column (a ray
+            // that starts inside its target cell): exact quadrature
+            if (lt > kTauHi || m < 0.f) nq = 0;
+            lt = fmaxf(lt, kTauLo);
+            xin[i][s] = (lt - 0.5f * (kTauLo + kTauHi)) * (2.f / (kTauHi - kTauLo));
+          }
+          xin[i][3] = (lT - 0.5f * (kTLo + kTHi)) * (2.f / (kTHi - kTLo));
+        }
+      }
+      // exclusive scan of the node counts -> positions in the evaluation list
+      int pos = nq;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, pos, o);
+        if (lane >= o) pos += v;
+      }
+      const int nev = __shfl_sync(0xffffffffu, pos, 31);
+      pos -= nq;
+      for (int i = 0; i < nq; i++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) S.x[wib][pos + i][c] = xin[i][c];
+      S.t[wib][lane] = tl;
+      S.ev0[wib][lane] = pos;
+      S.nq[wib][lane] = nq;
+      // pad the last tile with valid inputs
+      for (int q = nev + lane; q < ((nev + 15) & ~15); q += 32)
+#pragma unroll
+        for (int c = 0; c < 4; c++) S.x[wib][q][c] = 0.f;
+      __syncwarp();
+      // ---- phase B: the network on the tensor cores
+      for (int r16 = 0; r16 < nev; r16 += 16) mlp_tile16(S.w, S.x[wib], S.tout[wib], r16, lane);
+      __syncwarp();
+      // ---- phase C: surrogate rates and their error bound
+      bool need_exact = (tl >= 0) && (nq == 0);
+      if (tl >= 0 && nq > 0) {
+        const int e = S.e[wib][lane];
+        double G[6] = {0, 0, 0, 0, 0, 0};
+        float err = 0.f;
+        for (int i = 0; i < nq; i++) {
+          float u, wq;
+          gl_node(nq, i, &u, &wq);
+#pragma unroll
+          for (int j = 0; j < 6; j++) {
+            const float tt = S.tout[wib][pos + i][j];
+            const int bin = min(kEnvBins - 1, max(0, (int)(tt * (kEnvBins / kEnvTMax))));
+            err = fmaxf(err, S.w.env[j][bin]);
+            const float y = 1.f - __expf(tt);       // ln(I/I0)
+            G[j] += (double)wq * (double)__expf(y);  // I/I0 at the node
+          }
+        }
+        if (err <= S.w.tol) {
+#pragma unroll
+          for (int s = 0; s < 3; s++) {
+            const double pp = S.p[wib][lane][s];
+            S.out[wib][lane][s] = pp * G[s] * __ldg(emit_i0 + 6 * (size_t)e + s);
+            S.out[wib][lane][3 + s] = pp * G[3 + s] * __ldg(emit_i0 + 6 * (size_t)e + 3 + s) * kHNuL;
+          }
+          n_sur++;
+        } else {
+          need_exact = true;
+        }
+      }
+      // ---- phase D: exact FP32 quadrature for the rays that need it
+      unsigned mexact = __ballot_sync(0xffffffffu, need_exact);
+      n_exact += need_exact;
+      while (mexact) {
+        // four rays at a time, eight lanes each
+        int q[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          q[k] = mexact ? __ffs(mexact) - 1 : -1;
+          if (mexact) mexact &= mexact - 1;
+        }
+        const int qq = q[grp];
+        if (qq >= 0) {
+          const float N0 = S.nd[wib][qq][0], N1 = S.nd[wib][qq][1], N2 = S.nd[wib][qq][2];
+          const float D0 = S.nd[wib][qq][3], D1 = S.nd[wib][qq][4], D2 = S.nd[wib][qq][5];
+          const float *sp = specn + (size_t)S.e[wib][qq] * kNu;
+          float g0 = 0.f, g1 = 0.f, g2 = 0.f, h0 = 0.f, h1 = 0.f, h2 = 0.f;
+#pragma unroll 4
+          for (int m = 0; m < kNu / 8; m++) {
+            const int k = jj + 8 * m;
+            const float4 A4 = S.tab[3 * k + 0], B4 = S.tab[3 * k + 1], C4 = S.tab[3 * k + 2];
+            const float tl2 = fmaf(N0, A4.x, fmaf(N1, A4.y, N2 * A4.z));
+            const float dl2 = fmaf(D0, A4.x, fmaf(D1, A4.y, D2 * A4.z));
+            const float ee = ex2_approx(-tl2), ed = ex2_approx(-dl2);
+            const float wv = __ldg(sp + k) * ee * phi_pc(dl2 * ln2, ed);
+            g0 = fmaf(A4.w, wv, g0); g1 = fmaf(B4.x, wv, g1); g2 = fmaf(B4.y, wv, g2);
+            h0 = fmaf(B4.z, wv, h0); h1 = fmaf(B4.w, wv, h1); h2 = fmaf(C4.x, wv, h2);
+          }
+#pragma unroll
+          for (int o = 1; o < 8; o <<= 1) {
+            g0 += __shfl_xor_sync(gmask, g0, o); g1 += __shfl_xor_sync(gmask, g1, o);
+            g2 += __shfl_xor_sync(gmask, g2, o); h0 += __shfl_xor_sync(gmask, h0, o);
+            h1 += __shfl_xor_sync(gmask, h1, o); h2 += __shfl_xor_sync(gmask, h2, o);
+          }
+          if (jj == 0) {
+            const double p0 = S.p[wib][qq][0], p1 = S.p[wib][qq][1], p2 = S.p[wib][qq][2];
+            S.out[wib][qq][0] = p0 * g0; S.out[wib][qq][1] = p1 * g1; S.out[wib][qq][2] = p2 * g2;
+            S.out[wib][qq][3] = p0 * h0 * kHNuL; S.out[wib][qq][4] = p1 * h1 * kHNuL;
+            S.out[wib][qq][5] = p2 * h2 * kHNuL;
+          }
+        }
+        __syncwarp();
+      }
+      __syncwarp();
+      // ---- phase E: per-cell sums in ray order
+      const int nk = (int)min((uint64_t)32, r1 - rc);
+      for (int k = 0; k < nk; k++) {
+        if (S.t[wib][k] == lane) {
+#pragma unroll
+          for (int s = 0; s < 6; s++) acc[s] += S.out[wib][k][s];
+        }
+      }
+      __syncwarp();
+    }
+    if (own_valid) {
+#pragma unroll
+      for (int s = 0; s < 6; s++) rates6[s * ncell + own] = (float)acc[s];
+    }
+  }
+  if (counters) {
+    for (int o = 16; o; o >>= 1) {
+      n_sur += __shfl_xor_sync(0xffffffffu, n_sur, o);
+      n_exact += __shfl_xor_sync(0xffffffffu, n_exact, o);
+    }
+    if (lane == 0) {
+      atomicAdd(counters + 0, n_sur);
+      atomicAdd(counters + 1, n_exact);
+    }
+  }
+}
+
+// The network on a list of raw inputs (log10 tau x3, log10 T), one warp per
+// 16 evaluations, with the inference numerics of k_rate_sur.
+__global__ void __launch_bounds__(128) k_sur_eval(const SurWeights *__restrict__ wts, const float *__restrict__ X,
+                                                  int n, float *__restrict__ T) {
+  __shared__ SurWeights W;
+  __shared__ float xs[4][16][4];
+  __shared__ float ts[4][16][6];
+  {
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(wts);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(&W);
+    for (int i = threadIdx.x; i < (int)(sizeof(SurWeights) / 4); i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int nt = (n + 15) / 16;
+  for (int tile = blockIdx.x * 4 + wib; tile < nt; tile += gridDim.x * 4) {
+    if (lane < 16) {
+      const int i = tile * 16 + lane;
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        float v = i < n ? X[4 * (size_t)i + c] : 0.f;
+        if (c < 3) {
+          v = fminf(fmaxf(v, kTauLo), kTauHi);
+          v = (v - 0.5f * (kTauLo + kTauHi)) * (2.f / (kTauHi - kTauLo));
+        } else {
+          v = (v - 0.5f * (kTLo + kTHi)) * (2.f / (kTHi - kTLo));
+        }
+        xs[wib][lane][c] = v;
+      }
+    }
+    __syncwarp();
+    mlp_tile16(W, xs[wib], ts[wib], 0, lane);
+    __syncwarp();
+    for (int q = lane; q < 16 * 6; q += 32) {
+      const int i = tile * 16 + q / 6;
+      if (i < n) T[6 * (size_t)i + q % 6] = ts[wib][q / 6][q % 6];
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace argot
+
+using namespace argot;
+
+// ------------------------------------------------------------- host side
+struct argot_b200_surrogate {
+  int device;
+  SurWeights *dev;
+};
+
+namespace {
+
+uint16_t bf16_bits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  const uint32_t r = u + 0x7FFFu + ((u >> 16) & 1u);
+  return (uint16_t)(r >> 16);
+}
+uint32_t pack2(float lo, float hi) { return (uint32_t)bf16_bits(lo) | ((uint32_t)bf16_bits(hi) << 16); }
+
+// B fragment of N-tile j, K-step kk for W[n][k] (rows n, cols k, getter)
+template <class F>
+uint2 frag(F w, int j, int kk, int lane) {
+  const int gq = lane >> 2, tq = lane & 3;
+  const int n = 8 * j + gq, k = 16 * kk + 2 * tq;
+  uint2 r;
+  r.x = pack2(w(n, k), w(n, k + 1));
+  r.y = pack2(w(n, k + 8), w(n, k + 9));
+  return r;
+}
+
+}  // namespace
+
+extern "C" {
+
+// params: the 9030 FP32 network parameters (host); env: 6 x 64 error bound
+// of ln(I/I0) in bins of predicted t over [0, 6) (host); tol: largest bound
+// accepted per ray.
+int argot_b200_surrogate_create(const float *params, const float *env, float tol, argot_b200_surrogate **out) {
+  if (!params || !env || !out || !(tol > 0.f)) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
+  auto *h = new (std::nothrow) SurWeights();
+  if (!h) { set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
+  const float *W1 = params + kOffW1, *W2 = params + kOffW2, *W3 = params + kOffW3, *W4 = params + kOffW4;
+  for (int j = 0; j < 8; j++)
+    for (int l = 0; l < 32; l++) {
+      h->f1[j][l] = frag([&](int n, int k) { return k < 8 ? W1[n * kMlpIn + (k & 3)] : 0.f; }, j, 0, l);
+      for (int kk = 0; kk < 4; kk++) {
+        h->f2[j][kk][l] = frag([&](int n, int k) { return W2[n * kMlpH + k]; }, j, kk, l);
+        h->f3[j][kk][l] = frag([&](int n, int k) { return W3[n * kMlpH + k]; }, j, kk, l);
+      }
+    }
+  for (int kk = 0; kk < 8; kk++)
+    for (int l = 0; l < 32; l++)
+      h->f4[kk][l] = frag([&](int n, int k) { return n < kMlpOut ? W4[n * kMlpH + (k & 63)] : 0.f; }, 0, kk, l);
+  std::memcpy(h->b1, params + kOffB1, sizeof(float) * 64);
+  std::memcpy(h->b2, params + kOffB2, sizeof(float) * 64);
+  std::memcpy(h->b3, params + kOffB3, sizeof(float) * 64);
+  for (int j = 0; j < 8; j++) h->b4[j] = j < kMlpOut ? params[kOffB4 + j] : 0.f;
+  std::memcpy(h->env, env, sizeof(float) * 6 * kEnvBins);
+  double w6[6 * kNu];
+  host_rate_weights(w6);
+  for (int s = 0; s < 3; s++) {
+    h->sig0[s] = 0.f;
+    for (int k = 0; k < kNu && h->sig0[s] == 0.f; k++) h->sig0[s] = (float)w6[s * kNu + k];
+  }
+  h->tol = tol;
+  auto *s = new (std::nothrow) argot_b200_surrogate();
+  if (!s) { delete h; set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
+  cudaError_t e = cudaGetDevice(&s->device);
+  if (e == cudaSuccess) e = cudaMalloc(&s->dev, sizeof(SurWeights));
+  if (e == cudaSuccess) e = cudaMemcpy(s->dev, h, sizeof(SurWeights), cudaMemcpyHostToDevice);
+  delete h;
+  if (e != cudaSuccess) { delete s; return status_from_cuda(e); }
+  *out = s;
+  set_status(0);
+  return 0;
+}
+
+void argot_b200_surrogate_free(argot_b200_surrogate *s) {
+  if (!s) return;
+  cudaFree(s->dev);
+  delete s;
+}
+
+// t_j predictions (n x 6) for raw inputs X (n x 4: log10 tau_HI, tau_HeI,
+// tau_HeII, log10 T) with the tensor-core inference numerics.
+int argot_b200_surrogate_eval(const argot_b200_surrogate *s, const float *X, int n, float *T, void *stream) {
+  if (!s || (n && (!X || !T))) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
+  if (n) {
+    const int tiles = (n + 15) / 16;
+    const int blocks = (tiles + 3) / 4 < 4096 ? (tiles + 3) / 4 : 4096;
+    k_sur_eval<<<blocks, 128, 0, (cudaStream_t)stream>>>(s->dev, X, n, T);
+    ARGOT_CUDA_TRY(cudaGetLastError());
+  }
+  set_status(0);
+  return 0;
+}
+
+// Rates of blocks [b0, b1) with the surrogate (see argot_b200_photoion_rays;
+// counters, optional device uint64[2], receive the numbers of rays taken by
+// the surrogate and by the exact quadrature).
+int argot_b200_photoion_rays_surrogate(const argot_b200_grid *gp, const void *packed, const argot_b200_dev_tree *t,
+                                       const argot_b200_surrogate *sur, uint64_t b0, uint64_t b1,
+                                       const uint64_t *blk_off, uint64_t base, const uint32_t *rays, uint64_t nray,
+                                       const float *tau, float *rates6, unsigned long long *counters, void *stream) {
+  uint64_t nb = 0;
+  if (!grid_valid(gp) || !packed || !t || !sur || !blk_off || !rates6 || (nray && (!rays || !tau)) ||
+      !t->emit_logT || !t->emit_i0 || argot_b200_num_blocks(gp, &nb) || b0 > b1 || b1 > nb) {
+    set_status(ARGOT_B200_EINVAL);
+    return ARGOT_B200_EINVAL;
+  }
+  if (b0 == b1) { set_status(0); return 0; }
+  int dev = 0;
+  ARGOT_CUDA_TRY(cudaGetDevice(&dev));
+  int rc = ensure_rate_tables(dev);
+  if (rc) return rc;
+  static std::mutex mu;
+  static bool attr[64] = {false};
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (!attr[dev]) {
+      ARGOT_CUDA_TRY(cudaFuncSetAttribute(k_rate_sur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SurSmem)));
+      attr[dev] = true;
+    }
+  }
+  GridDev g = make_grid(*gp);
+  const uint64_t ncell = (uint64_t)gp->nx * gp->ny * gp->nz;
+  const float4 *raw = (const float4 *)packed + ncell;
+  const int threads = 32 * kSurWarps;
+  k_rate_sur<<<grid_blocks_for_rates((b1 - b0) * 32, threads), threads, sizeof(SurSmem), (cudaStream_t)stream>>>(
+      g, raw, t->emit_pos, t->emit_specn, t->emit_total, t->emit_logT, t->emit_i0, sur->dev, b0, b1, blk_off, base,
+      rays, nray, tau, rates6, counters);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  set_status(0);
+  return 0;
+}
+
+}  // extern "C"

@@ -166,6 +166,19 @@ class Problem:
                                                   _p(rays), group.nray, _p(tau), int(mode),
                                                   _p(rates6), self.sp), "photoion_rays")
 
+    def set_blackbody(self):
+        """Spectral temperatures of the sources (blackbodies) for the
+        surrogate; other spectrum types are marked for exact integration."""
+        T = np.where(self.wl.src_type == 0, self.wl.src_param, -1.0).astype(np.float32)
+        L.check(self.lib.argot_b200_dev_tree_set_blackbody(self._tree, self._dtree, T.ctypes.data,
+                                                           self.sp), "dev_tree_set_blackbody")
+
+    def rates_surrogate(self, group: RayGroup, rays, tau, rates6, surrogate, counters=None):
+        L.check(self.lib.argot_b200_photoion_rays_surrogate(
+            C.byref(self.grid), _p(self.packed), self._dtree, surrogate.handle, group.b0, group.b1,
+            _p(self.blk_off), group.base, _p(rays), group.nray, _p(tau), _p(rates6), _p(counters),
+            self.sp), "photoion_rays_surrogate")
+
     def check_device_error(self):
         L.check(self.lib.argot_b200_check_device_error(self.sp), "device error flag")
 

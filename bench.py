@@ -167,28 +167,40 @@ def allsum(ws, x: float, device=None) -> float:
 
 
 # ------------------------------------------------------------ CPU baseline
-def cpu_sample(wl, target_seconds: float = 15.0, max_cells: int = 4096, threads: int | None = None,
-               seed: int = 0):
-    """ARGOT's own C (the reference build for this mesh edge) on a bounded,
-    seeded sample of target cells: one contiguous group of target cells,
-    the reference's own grouping unit.  Returns crossings/s over the hot
-    path (calc_optical_depth + accum_optical_depth + calc_photoion_rate)."""
-    from oracle.oracle import Oracle, RefLib, unit_box_grid
+def reference_setup(wl, threads: int | None = None):
+    """ARGOT's own C (the reference build for this mesh edge) loaded with the
+    workload's mesh and sources; the reference builds its own tree."""
+    from oracle.oracle import RefLib
     threads = threads or os.cpu_count() or 1
     R = RefLib(wl.edge)
     R.init(wl.lunit, wl.denstonh, wl.theta, threads)
     R.set_mesh(*wl.fields())
     R.set_sources(wl.src_type, wl.src_param, wl.src_pos, wl.src_rate)
+    R.threads = threads
+    return R
+
+
+def cpu_sample(wl, target_seconds: float = 15.0, max_cells: int = 1 << 20, R=None, seed: int = 0):
+    """The reference's hot path on a bounded, seeded sample of target cells:
+    one contiguous group of target cells, the reference's own grouping unit,
+    sized by a short probe to take about `target_seconds`.  Returns
+    crossings/s over calc_optical_depth + accum_optical_depth +
+    calc_photoion_rate."""
+    from oracle.oracle import Oracle, unit_box_grid
+    if R is None:
+        R = reference_setup(wl)
+    threads = R.threads
     rng = np.random.default_rng(seed)
     ncell = wl.edge ** 3
     # size the group by a short probe, then run it
-    ncells = 64
-    im0 = int(rng.integers(0, ncell - max_cells))
+    ncells = min(256, ncell)
+    im0 = int(rng.integers(0, ncell - ncells + 1))
     R.zero_rates()
     t0 = time.time()
     probe = R.run_range(im0, im0 + ncells, True, want=("seg",))
     dt = max(time.time() - t0, 1e-3)
-    ncells = int(min(max_cells, max(64, ncells * target_seconds / dt)))
+    ncells = int(min(max_cells, ncell, max(64, ncells * target_seconds / dt)))
+    im0 = int(rng.integers(0, ncell - ncells + 1))
     R.zero_rates()
     out = R.run_range(im0, im0 + ncells, True, want=("seg",))
     times = out["times"]
@@ -314,7 +326,7 @@ def run_ours(args):
         line["e2e"] = e2e
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
-            cb = cpu_sample(wl, target_seconds=args.cpu_seconds)
+            cb = cpu_sample(wl, target_seconds=args.cpu_seconds, R=reference_setup(wl))
             cb.pop("_probe_rays", None)
             line["cpu_baseline"] = cb
         except Exception as exc:  # the baseline must not hide our own number
@@ -371,10 +383,11 @@ def run_reference(args):
     if rank != 0:
         return
     wl = make_workload(args.config, 0)
+    R = reference_setup(wl)
     vals = []
     info = None
     for s in range(args.warmup + args.steps):
-        r = cpu_sample(wl, target_seconds=args.ref_seconds, seed=s)
+        r = cpu_sample(wl, target_seconds=args.ref_seconds, R=R, seed=s)
         if s >= args.warmup:
             vals.append(r["value"])
             info = r

@@ -264,6 +264,60 @@ ARGOT_B200_API int argot_b200_photoion_rays(const argot_b200_grid *g, const void
                              const float *tau_dev, int mode, float *rates6_dev,
                              void *stream);
 
+/* ---- surrogate of the frequency integral (BF16 MLP, tensor cores) ------- */
+/* No counterpart in the reference: its unimplemented Gamma(tau) table
+ * (multi_freq_bin.h:11-17, prim_chem/calc_gamma_of_tau.c:5-17) is the
+ * closest.  The network (4 -> 64 -> 64 -> 64 -> 6, SiLU, BF16 weights and
+ * activations, FP32 accumulation) predicts t_j = ln(1 - ln(I_j/I_j0)) of the
+ * six thin-cell integrals I_j (Gamma and heating of HI, HeI, HeII) from
+ * (log10 tau_HI, log10 tau_HeI, log10 tau_HeII, log10 T). */
+typedef struct argot_b200_surrogate argot_b200_surrogate;
+
+/* Marks every emitter whose spectrum is a single-temperature blackbody
+ * (src_T[i] > 0: the temperature of source i, <= 0: other spectrum) and
+ * uploads each emitter's thin-cell integrals, which the surrogate needs. */
+ARGOT_B200_API int argot_b200_dev_tree_set_blackbody(const argot_b200_tree *t, argot_b200_dev_tree *d,
+                                                     const float *src_T, void *stream);
+ARGOT_B200_API int argot_b200_mlp_num_params(void);
+/* normalised blackbody spectra on log10 T = 4 + 1.5 k/(nT-1) (nT x 256) and
+ * their thin-cell integrals (nT x 6), host arrays */
+ARGOT_B200_API int argot_b200_mlp_spectra(int nT, double *spec, double *i0);
+/* n training samples of the exact quadrature on the device: X (n x 4),
+ * Y (n x 6) = t_j; spec_dev / i0_dev as from argot_b200_mlp_spectra */
+ARGOT_B200_API int argot_b200_mlp_samples(const double *spec_dev, const double *i0_dev, int nT, uint64_t n,
+                                          uint64_t seed, float *X, float *Y, void *stream);
+/* device floats of workspace a training step on nb samples needs */
+ARGOT_B200_API uint64_t argot_b200_mlp_workspace(int nb);
+/* forward pass (CUDA cores, the training numerics): normalised outputs O
+ * (6 x n, output-major); t_j = 2.75 * O + 2.75 */
+ARGOT_B200_API int argot_b200_mlp_forward(const float *params, const float *X, int n, float *O, void *stream);
+/* one training step (forward, backward, deterministic gradient sums,
+ * Adam on the FP32 master parameters); lr == 0 computes the gradient into
+ * grad_out without updating */
+ARGOT_B200_API int argot_b200_mlp_train_step(float *params, float *m, float *v, const float *X, const float *Y,
+                                             int nb, float lr, int step, float *work, float *grad_out,
+                                             double *loss_out, void *stream);
+/* inference weights on the current device from the FP32 parameters (host),
+ * the validated error envelope (6 x 64 bins of predicted t over [0, 6),
+ * bound of |error of ln(I/I0)|) and the per-ray tolerance */
+ARGOT_B200_API int argot_b200_surrogate_create(const float *params, const float *env, float tol,
+                                               argot_b200_surrogate **out);
+ARGOT_B200_API void argot_b200_surrogate_free(argot_b200_surrogate *s);
+/* the network on raw inputs X (n x 4) with the tensor-core inference
+ * numerics: t_j predictions T (n x 6) */
+ARGOT_B200_API int argot_b200_surrogate_eval(const argot_b200_surrogate *s, const float *X, int n, float *T,
+                                             void *stream);
+/* argot_b200_photoion_rays with the surrogate and exact FP32 fallback;
+ * counters (device uint64[2], optional) receive the numbers of rays taken
+ * by the surrogate and by the exact quadrature */
+ARGOT_B200_API int argot_b200_photoion_rays_surrogate(const argot_b200_grid *g, const void *packed_dev,
+                                                      const argot_b200_dev_tree *t,
+                                                      const argot_b200_surrogate *sur, uint64_t b0, uint64_t b1,
+                                                      const uint64_t *blk_offsets_dev, uint64_t base,
+                                                      const uint32_t *rays_dev, uint64_t nray_group,
+                                                      const float *tau_dev, float *rates6_dev,
+                                                      unsigned long long *counters_dev, void *stream);
+
 /* Reads and clears the device-side error flag of the current device (set
  * when a march exceeded its step bound, which only non-finite input can
  * cause); synchronises `stream`.  Returns 0 or ARGOT_B200_EDEVICE. */
