@@ -130,21 +130,30 @@ class Problem:
         self.nray = tot.value
         self.blk_off_host = self.blk_off.cpu().numpy()
 
-    def _make_groups(self, max_rays):
-        if not max_rays or self.nray <= max_rays:
-            return [RayGroup(0, self.nblocks, 0, self.nray)]
-        groups, b0 = [], 0
+    def restrict(self, b0: int, b1: int, max_rays: int | None = None):
+        """Only the target blocks [b0, b1) from now on (one rank's shard)."""
+        self.groups = self._make_groups(max_rays, b0, b1)
+        return self.groups
+
+    def _make_groups(self, max_rays, blk0: int = 0, blk1: int | None = None):
         off = self.blk_off_host
-        while b0 < self.nblocks:
+        blk1 = self.nblocks if blk1 is None else blk1
+        if blk1 <= blk0:
+            return []
+        nray = int(off[blk1] - off[blk0])
+        if not max_rays or nray <= max_rays:
+            return [RayGroup(blk0, blk1, int(off[blk0]), nray)]
+        groups, b0 = [], blk0
+        while b0 < blk1:
             b1 = int(np.searchsorted(off, off[b0] + max_rays, side="right")) - 1
             b1 = max(b1, b0 + 1)
-            b1 = min(b1, self.nblocks)
+            b1 = min(b1, blk1)
             groups.append(RayGroup(b0, b1, int(off[b0]), int(off[b1] - off[b0])))
             b0 = b1
         return groups
 
     def alloc_group_buffers(self, group: RayGroup | None = None):
-        n = max(g.nray for g in self.groups) if group is None else group.nray
+        n = max((g.nray for g in self.groups), default=0) if group is None else group.nray
         rays = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
         tau = torch.empty(3 * max(n, 1), dtype=torch.float32, device=self.device)
         return rays, tau

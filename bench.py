@@ -217,6 +217,72 @@ def cpu_sample(wl, target_seconds: float = 15.0, max_cells: int = 1 << 20, R=Non
             "_probe_rays": probe["nray"]}
 
 
+# ------------------------------------------------------------ rate modes
+def load_surrogate(pb):
+    """The trained weights (argot_b200/data/surrogate.npz) on the device and
+    the emitters' blackbody integrals; None when no weights are present."""
+    from argot_b200 import surrogate as S
+    if not os.path.exists(S.WEIGHTS):
+        return None
+    pb.set_blackbody()
+    return S.Surrogate.from_file()
+
+
+def compare_rate_modes(pb, rays, tau, prec, sur):
+    """One pass of each rate kernel over every group after the same march:
+    device time of each (CUDA events around the rate launches only) and the
+    per-cell error of the FP32 and surrogate fields against the FP64
+    reference-order field (the same algorithm as the reference's FP64
+    arithmetic, itself held to the FP64 oracle by the GPU tests)."""
+    import torch
+    from argot_b200 import _lib as L
+    dev = pb.device
+    modes = [("exact_f64", L.RATE_EXACT_F64), ("exact_f32", L.RATE_EXACT_F32)]
+    if sur is not None:
+        modes.append(("surrogate", None))
+    fields = {m: torch.zeros(6 * pb.ncell, dtype=torch.float32, device=dev) for m, _ in modes}
+    t = {m: 0.0 for m, _ in modes}
+    counters = torch.zeros(2, dtype=torch.int64, device=dev)
+    single = len(pb.groups) == 1
+    for g in pb.groups:
+        if not single:
+            pb.emit(g, rays)
+        pb.march(g, rays, tau, prec)
+        for m, code in modes:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(pb.stream)
+            if code is None:
+                pb.rates_surrogate(g, rays, tau, fields[m], sur, counters)
+            else:
+                pb.rates(g, rays, tau, fields[m], code)
+            e1.record(pb.stream)
+            e1.synchronize()
+            t[m] += e0.elapsed_time(e1) / 1e3
+    pb.check_device_error()
+    ref = fields["exact_f64"].view(6, -1).double()
+    out = {}
+    names = ("gamma_HI", "gamma_HeI", "gamma_HeII", "heat_HI", "heat_HeI", "heat_HeII")
+    for m, _ in modes:
+        d = {"s": t[m], "gamma_cells_per_s": pb.ncell / t[m], "rays_per_s": pb.nray / t[m],
+             "speedup_vs_exact_f64": t["exact_f64"] / t[m]}
+        if m != "exact_f64":
+            x = fields[m].view(6, -1).double()
+            err = {}
+            for j, nm in enumerate(names):
+                r = ref[j]
+                pos = r > 0
+                rel = ((x[j] - r).abs()[pos] / r[pos])
+                err[nm] = float(rel.max().item()) if rel.numel() else 0.0
+            d["max_rel_err_vs_f64"] = err
+        out[m] = d
+    if sur is not None:
+        c = counters.cpu().numpy()
+        out["surrogate"]["rays_surrogate"] = int(c[0])
+        out["surrogate"]["rays_exact_fallback"] = int(c[1])
+        out["surrogate"]["fallback_frac"] = float(c[1] / max(1, c[0] + c[1]))
+    return out
+
+
 # ------------------------------------------------------------ our arm
 def run_ours(args):
     import torch
@@ -229,7 +295,7 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     wl = make_workload(args.config, rank)
     prec = L.PRECISION_KAHAN if args.precision == "kahan" else L.PRECISION_REFERENCE
-    mode = {"f32": L.RATE_EXACT_F32, "f64": L.RATE_EXACT_F64}[args.rate]
+    mode = {"f32": L.RATE_EXACT_F32, "f64": L.RATE_EXACT_F64, "surrogate": L.RATE_SURROGATE}[args.rate]
 
     free, _ = torch.cuda.mem_get_info(dev)
     pb = Problem(wl, dev, max_group_rays=None)
@@ -243,13 +309,22 @@ def run_ours(args):
     if single:
         pb.emit(pb.groups[0], rays)
     crossings = torch.zeros(1, dtype=torch.int64, device=dev)
+    sur = load_surrogate(pb) if (mode == L.RATE_SURROGATE or not args.no_rate_modes) else None
+    if mode == L.RATE_SURROGATE and sur is None:
+        raise SystemExit("--rate surrogate needs trained weights (python -m argot_b200.train_surrogate)")
+
+    def rate_pass(g):
+        if mode == L.RATE_SURROGATE:
+            pb.rates_surrogate(g, rays, tau, rates6, sur)
+        else:
+            pb.rates(g, rays, tau, rates6, mode)
 
     def step(count=None):
         for g in pb.groups:
             if not single:
                 pb.emit(g, rays)
             pb.march(g, rays, tau, prec, count)
-            pb.rates(g, rays, tau, rates6, mode)
+            rate_pass(g)
 
     # warm-up (the first one also counts the crossings)
     for w in range(args.warmup):
@@ -267,11 +342,12 @@ def run_ours(args):
         pb.march(g, rays, tau, prec)
     ev[1].record(stream)
     for g in pb.groups:
-        pb.rates(g, rays, tau, rates6, mode)
+        rate_pass(g)
     ev[2].record(stream)
     torch.cuda.synchronize()
     t_march = ev[0].elapsed_time(ev[1]) / 1e3
     t_rates = ev[1].elapsed_time(ev[2]) / 1e3
+    rate_modes = None if args.no_rate_modes else compare_rate_modes(pb, rays, tau, prec, sur)
 
     clocks = ClockSampler(local)
     barrier(ws)
@@ -322,6 +398,8 @@ def run_ours(args):
         "clocks": clk,
         "gpu_launches": launches_per_step * args.steps,
     }
+    if rate_modes is not None:
+        line["rate_modes"] = rate_modes
     if e2e is not None:
         line["e2e"] = e2e
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -346,23 +424,33 @@ def run_e2e(wl, dev, prec, mode, steps=2):
     builds the tree, generates the rays on the device, marches, computes the
     rates and copies the six rate fields back to pinned host memory."""
     import torch
+    from argot_b200 import _lib as L
     from argot_b200.pipeline import Problem
     pin = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in wl.fields()]
     out = torch.empty(6 * wl.ncell, dtype=torch.float32).pin_memory()
     h2d = sum(p.numel() * 4 for p in pin) + wl.nsrc * (12 + 8 + 8)
     times = []
     cross = None
+    sur = None
+    if mode == L.RATE_SURROGATE:
+        from argot_b200 import surrogate as S
+        sur = S.Surrogate.from_file()  # weights stay resident, like a solver's
     for s in range(steps + 1):  # first pass warms the caching allocator
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         pb = Problem(wl, dev, host_fields=pin)
+        if sur is not None:
+            pb.set_blackbody()
         rays, tau = pb.alloc_group_buffers()
         rates6 = torch.zeros(6 * pb.ncell, dtype=torch.float32, device=dev)
         cnt = torch.zeros(1, dtype=torch.int64, device=dev)
         for g in pb.groups:
             pb.emit(g, rays)
             pb.march(g, rays, tau, prec, cnt)
-            pb.rates(g, rays, tau, rates6, mode)
+            if sur is not None:
+                pb.rates_surrogate(g, rays, tau, rates6, sur)
+            else:
+                pb.rates(g, rays, tau, rates6, mode)
         out.copy_(rates6, non_blocking=True)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
@@ -415,7 +503,9 @@ def main(argv=None):
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
     p.add_argument("--config", choices=CONFIGS, default="largest")
     p.add_argument("--precision", choices=("kahan", "reference"), default="kahan")
-    p.add_argument("--rate", choices=("f32", "f64"), default="f32")
+    p.add_argument("--rate", choices=("f32", "f64", "surrogate"), default="f32")
+    p.add_argument("--no-rate-modes", action="store_true",
+                   help="skip the one-pass comparison of the three rate kernels")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
