@@ -38,6 +38,22 @@ class Grid(C.Structure):
 
 GP = C.POINTER(Grid)
 
+
+class BatchProblem(C.Structure):
+    """argot_b200_batch_problem"""
+    _fields_ = [("grid", Grid), ("packed_dev", C.c_void_p), ("tree", C.c_void_p),
+                ("blk_offsets_dev", C.c_void_p), ("blk_offsets_host", C.c_void_p),
+                ("rays_dev", C.c_void_p), ("rates6_dev", C.c_void_p)]
+
+
+class BatchConfig(C.Structure):
+    """argot_b200_batch_config"""
+    _fields_ = [("warps_per_cta", C.c_int), ("ctas_per_sm", C.c_int), ("blocks_per_item", C.c_int),
+                ("order", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
 SIGNATURES = {
     "argot_b200_last_error": (i32, []),
     "argot_b200_error_string": (C.c_char_p, [i32]),
@@ -81,8 +97,17 @@ SIGNATURES = {
     "argot_b200_surrogate_create": (i32, [vp, vp, f32, C.POINTER(vp)]),
     "argot_b200_surrogate_free": (None, [vp]),
     "argot_b200_surrogate_eval": (i32, [vp, vp, i32, vp, vp]),
+    "argot_b200_surrogate_workspace": (u64, [u64]),
+    "argot_b200_batch_create": (i32, [C.POINTER(BatchProblem), i32, C.POINTER(vp)]),
+    "argot_b200_batch_free": (None, [vp]),
+    "argot_b200_batch_configure": (i32, [vp, C.POINTER(BatchConfig)]),
+    "argot_b200_batch_get_config": (i32, [vp, C.POINTER(BatchConfig)]),
+    "argot_b200_batch_num_items": (i32, [vp]),
+    "argot_b200_batch_run": (i32, [vp, vp, vp]),
+    "argot_b200_batch_graph_launch": (i32, [vp, vp]),
+    "argot_b200_batch_tune": (i32, [vp, i32, C.POINTER(BatchConfig), C.POINTER(f32), vp]),
     "argot_b200_photoion_rays_surrogate": (i32, [GP, vp, vp, vp, u64, u64, vp, u64, vp, u64, vp, vp, vp,
-                                                 vp]),
+                                                 vp, vp]),
 }
 
 _lock = threading.Lock()

@@ -1,0 +1,467 @@
+// batch.cu -- many independent problems (meshes + source sets of uneven
+// size) in one persistent launch, replayable as a CUDA graph.
+//
+// The unit of work is a run of consecutive target blocks of one problem (a
+// "tile").  Each warp of the persistent grid takes tiles from a device
+// queue (one atomic counter) and, for every block of its tile, marches the
+// block's rays 32 at a time (one lane per ray, the count-down march with
+// Kahan columns) and integrates their rates at once (exact FP32 quadrature,
+// eight lanes per ray), so the columns never leave the registers; lane j
+// sums the rays of cell j of the block in ray order.  The arithmetic is
+// that of argot_b200_march_rays + argot_b200_photoion_rays (EXACT_F32), so
+// every problem's rates equal those of the problem run alone, bit for bit.
+//
+// Tiles are queued largest first (estimated cost: rays x (mesh edge + a
+// constant for the quadrature)), so the long tiles of the big meshes start
+// early and the short ones fill the tail.  The tile length, warps per CTA
+// and CTAs per SM are chosen by argot_b200_batch_tune, which times
+// candidate configurations on the batch itself.
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <new>
+#include <numeric>
+#include <vector>
+
+#include "march.cuh"
+#include "photoion.cuh"
+
+namespace argot {
+
+int *err_flag(int dev);
+
+struct BatchProb {
+  GridDev g;
+  const float4 *cells;  // packed products (the march's gathers)
+  const float4 *raw;    // packed raw fields (target cells of the rates)
+  const float4 *emit_pos;
+  const float *specn;
+  const double *total;
+  const uint64_t *blk_off;
+  const uint32_t *rays;  // every ray of the problem, base 0
+  float *rates6;
+  uint64_t nray;
+};
+
+struct BatchItem {
+  uint32_t prob, b0, b1, pad;
+};
+
+template <int kWarps>
+__global__ void __launch_bounds__(32 * kWarps)
+    k_batch(const BatchProb *__restrict__ probs, const BatchItem *__restrict__ items, uint32_t nitems,
+            uint32_t *__restrict__ next, unsigned long long *__restrict__ crossings, int *__restrict__ err) {
+  __shared__ float4 s_tab[3 * kNu];
+  __shared__ float s_nd[kWarps][32][6];
+  __shared__ double s_p[kWarps][32][3];
+  __shared__ double s_out[kWarps][32][6];
+  __shared__ int s_e[kWarps][32], s_t[kWarps][32];
+  for (int k = threadIdx.x; k < kNu; k += blockDim.x) {
+    s_tab[3 * k + 0] = make_float4(c_tab.cs_l2e[0][k], c_tab.cs_l2e[1][k], c_tab.cs_l2e[2][k], c_tab.cs[0][k]);
+    s_tab[3 * k + 1] = make_float4(c_tab.cs[1][k], c_tab.cs[2][k], c_tab.hw[0][k], c_tab.hw[1][k]);
+    s_tab[3 * k + 2] = make_float4(c_tab.hw[2][k], 0.f, 0.f, 0.f);
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int grp = lane >> 3, j = lane & 7;
+  const unsigned gmask = 0xffu << (8 * grp);
+  const float ln2 = 0.69314718055994531f;
+  unsigned long long steps_total = 0;
+  bool bad = false;
+  for (;;) {
+    uint32_t it = 0;
+    if (lane == 0) it = atomicAdd(next, 1u);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it >= nitems) break;
+    const BatchItem wi = items[it];
+    const BatchProb &P = probs[wi.prob];
+    const GridDev g = P.g;
+    const float4 *__restrict__ cells = P.cells;
+    const float4 *__restrict__ raw = P.raw;
+    const float4 *__restrict__ emit_pos = P.emit_pos;
+    const float *__restrict__ specn = P.specn;
+    const double *__restrict__ total = P.total;
+    const uint32_t *__restrict__ rays = P.rays;
+    float *__restrict__ rates6 = P.rates6;
+    const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
+    for (uint64_t b = wi.b0; b < wi.b1; b++) {
+      int ix, iy, iz;
+      const bool own_valid = block_cell(g, b, lane, &ix, &iy, &iz);
+      const uint64_t own = own_valid ? cell_index(g, ix, iy, iz) : 0;
+      double acc[6] = {0, 0, 0, 0, 0, 0};
+      int bix, biy, biz;
+      block_cell(g, b, 0, &bix, &biy, &biz);
+      const uint64_t r0 = P.blk_off[b], r1 = P.blk_off[b + 1];
+      for (uint64_t rc = r0; rc < r1; rc += 32) {
+        const uint64_t r = rc + lane;
+        int t = -1;
+        if (r < r1) {
+          const uint32_t w = __ldg(rays + r);
+          const uint32_t e = w >> 5;
+          t = (int)(w & 31u);
+          const int lx = bix + (t >> 4), ly = biy + ((t >> 2) & 3), lz = biz + (t & 3);
+          // the march (as argot_b200_march_rays, Kahan columns)
+          const float xe = cell_centre(g.xmin, g.ix0 + lx, g.dx);
+          const float ye = cell_centre(g.ymin, g.iy0 + ly, g.dy);
+          const float ze = cell_centre(g.zmin, g.iz0 + lz, g.dz);
+          const float4 ep = __ldg(emit_pos + e);
+          float xs, ys, zs;
+          ray_start(g, ep.x, ep.y, ep.z, xe, ye, ze, &xs, &ys, &zs);
+          int steps = 0;
+          const Tau3 tt = march_kahan(g, cells, xs, ys, zs, xe, ye, ze, &steps, &bad);
+          steps_total += (unsigned long long)steps;
+          // the rate parameters (as argot_b200_photoion_rays)
+          const RayGeom geo = ray_geometry(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z);
+          const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
+          const RayCols cols = ray_columns(g, tt.hi, tt.hei, tt.heii, rw, geo);
+          const RayParams p = ray_params(cols, __ldg(total + e));
+#pragma unroll
+          for (int s = 0; s < 3; s++) {
+            s_nd[wib][lane][s] = p.N[s];
+            s_nd[wib][lane][3 + s] = p.D[s];
+            s_p[wib][lane][s] = p.P[s];
+          }
+          s_e[wib][lane] = (int)e;
+        }
+        s_t[wib][lane] = t;
+        __syncwarp();
+        const int nk = (int)min((uint64_t)32, r1 - rc);
+        for (int q = grp; q < nk; q += 4) {
+          const float N0 = s_nd[wib][q][0], N1 = s_nd[wib][q][1], N2 = s_nd[wib][q][2];
+          const float D0 = s_nd[wib][q][3], D1 = s_nd[wib][q][4], D2 = s_nd[wib][q][5];
+          const float *sp = specn + (size_t)s_e[wib][q] * kNu;
+          float g0 = 0.f, g1 = 0.f, g2 = 0.f, h0 = 0.f, h1 = 0.f, h2 = 0.f;
+#pragma unroll 4
+          for (int m = 0; m < kNu / 8; m++) {
+            const int k = j + 8 * m;
+            const float4 A = s_tab[3 * k + 0], B = s_tab[3 * k + 1], Cq = s_tab[3 * k + 2];
+            const float tl2 = fmaf(N0, A.x, fmaf(N1, A.y, N2 * A.z));
+            const float dl2 = fmaf(D0, A.x, fmaf(D1, A.y, D2 * A.z));
+            const float ee = ex2_approx(-tl2);
+            const float ed = ex2_approx(-dl2);
+            const float wv = __ldg(sp + k) * ee * phi_pc(dl2 * ln2, ed);
+            g0 = fmaf(A.w, wv, g0);
+            g1 = fmaf(B.x, wv, g1);
+            g2 = fmaf(B.y, wv, g2);
+            h0 = fmaf(B.z, wv, h0);
+            h1 = fmaf(B.w, wv, h1);
+            h2 = fmaf(Cq.x, wv, h2);
+          }
+#pragma unroll
+          for (int o = 1; o < 8; o <<= 1) {
+            g0 += __shfl_xor_sync(gmask, g0, o);
+            g1 += __shfl_xor_sync(gmask, g1, o);
+            g2 += __shfl_xor_sync(gmask, g2, o);
+            h0 += __shfl_xor_sync(gmask, h0, o);
+            h1 += __shfl_xor_sync(gmask, h1, o);
+            h2 += __shfl_xor_sync(gmask, h2, o);
+          }
+          if (j == 0) {
+            const double p0 = s_p[wib][q][0], p1 = s_p[wib][q][1], p2 = s_p[wib][q][2];
+            s_out[wib][q][0] = p0 * g0;
+            s_out[wib][q][1] = p1 * g1;
+            s_out[wib][q][2] = p2 * g2;
+            s_out[wib][q][3] = p0 * h0 * kHNuL;
+            s_out[wib][q][4] = p1 * h1 * kHNuL;
+            s_out[wib][q][5] = p2 * h2 * kHNuL;
+          }
+        }
+        __syncwarp();
+        for (int k = 0; k < nk; k++) {
+          if (s_t[wib][k] == lane) {
+#pragma unroll
+            for (int s = 0; s < 6; s++) acc[s] += s_out[wib][k][s];
+          }
+        }
+        __syncwarp();
+      }
+      if (own_valid) {
+#pragma unroll
+        for (int s = 0; s < 6; s++) rates6[s * ncell + own] = (float)acc[s];
+      }
+    }
+  }
+  if (crossings) {
+    for (int o = 16; o; o >>= 1) steps_total += __shfl_xor_sync(0xffffffffu, steps_total, o);
+    if (lane == 0 && steps_total) atomicAdd(crossings, steps_total);
+  }
+  if (bad) atomicExch(err, 1);
+}
+
+}  // namespace argot
+
+using namespace argot;
+
+struct argot_b200_batch {
+  int device = 0;
+  int sms = 148;
+  std::vector<BatchProb> probs;
+  std::vector<std::vector<uint64_t>> blk_off;  // host copies (tiles and costs)
+  BatchProb *probs_dev = nullptr;
+  BatchItem *items_dev = nullptr;
+  size_t items_cap = 0;
+  uint32_t nitems = 0;
+  uint32_t *next_dev = nullptr;
+  int *err = nullptr;
+  argot_b200_batch_config cfg{8, 0, 4, 0};
+  int grid = 0;
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+void drop_graph(argot_b200_batch *b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+int max_ctas_per_sm(int warps) {
+  int n = 0;
+  cudaError_t e = warps == 4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch<4>, 128, 0)
+                             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch<8>, 256, 0);
+  return e == cudaSuccess ? n : 0;
+}
+
+bool config_valid(const argot_b200_batch_config &c) {
+  return (c.warps_per_cta == 4 || c.warps_per_cta == 8) && c.ctas_per_sm >= 0 && c.ctas_per_sm <= 16 &&
+         c.blocks_per_item >= 1 && c.blocks_per_item <= 4096 && (c.order == 0 || c.order == 1);
+}
+
+// Work list of the configuration: tiles of blocks_per_item consecutive
+// blocks, in problem order or by estimated cost (largest first; ties keep
+// problem order, so the list is deterministic).
+int build_items(argot_b200_batch *b) {
+  std::vector<BatchItem> items;
+  std::vector<double> cost;
+  const uint32_t L = (uint32_t)b->cfg.blocks_per_item;
+  for (size_t p = 0; p < b->probs.size(); p++) {
+    const std::vector<uint64_t> &off = b->blk_off[p];
+    const uint32_t nb = (uint32_t)(off.size() - 1);
+    const double per_ray = (double)b->probs[p].g.nx + 64.0;  // march steps + quadrature, in march steps
+    for (uint32_t b0 = 0; b0 < nb; b0 += L) {
+      const uint32_t b1 = std::min(nb, b0 + L);
+      items.push_back({(uint32_t)p, b0, b1, 0u});
+      cost.push_back((double)(off[b1] - off[b0]) * per_ray + 1.0);
+    }
+  }
+  if (b->cfg.order == 0) {
+    std::vector<size_t> idx(items.size());
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t c) { return cost[a] > cost[c]; });
+    std::vector<BatchItem> sorted(items.size());
+    for (size_t i = 0; i < idx.size(); i++) sorted[i] = items[idx[i]];
+    items.swap(sorted);
+  }
+  if (items.size() > 0xffffffffull) return ARGOT_B200_EINVAL;
+  if (items.size() > b->items_cap) {
+    cudaFree(b->items_dev);
+    b->items_dev = nullptr;
+    b->items_cap = 0;
+    ARGOT_CUDA_TRY(cudaMalloc(&b->items_dev, sizeof(BatchItem) * std::max<size_t>(items.size(), 1)));
+    b->items_cap = items.size();
+  }
+  if (!items.empty())
+    ARGOT_CUDA_TRY(cudaMemcpy(b->items_dev, items.data(), sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice));
+  b->nitems = (uint32_t)items.size();
+  const int occ = max_ctas_per_sm(b->cfg.warps_per_cta);
+  if (occ <= 0) return ARGOT_B200_ECUDA;
+  const int per_sm = b->cfg.ctas_per_sm > 0 ? std::min(b->cfg.ctas_per_sm, occ) : occ;
+  const uint64_t warps_needed = std::max<uint64_t>(1, b->nitems);
+  const uint64_t ctas_needed = (warps_needed + b->cfg.warps_per_cta - 1) / b->cfg.warps_per_cta;
+  b->grid = (int)std::min<uint64_t>((uint64_t)b->sms * per_sm, ctas_needed);
+  drop_graph(b);
+  return 0;
+}
+
+int launch(argot_b200_batch *b, unsigned long long *crossings, cudaStream_t st) {
+  ARGOT_CUDA_TRY(cudaMemsetAsync(b->next_dev, 0, sizeof(uint32_t), st));
+  if (b->cfg.warps_per_cta == 4)
+    k_batch<4><<<b->grid, 128, 0, st>>>(b->probs_dev, b->items_dev, b->nitems, b->next_dev, crossings, b->err);
+  else
+    k_batch<8><<<b->grid, 256, 0, st>>>(b->probs_dev, b->items_dev, b->nitems, b->next_dev, crossings, b->err);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int argot_b200_batch_create(const argot_b200_batch_problem *p, int n, argot_b200_batch **out) {
+  if (!p || n <= 0 || !out) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
+  for (int i = 0; i < n; i++) {
+    uint64_t nb = 0;
+    const argot_b200_dev_tree *t = p[i].tree;
+    if (!grid_valid(&p[i].grid) || !p[i].packed_dev || !t || !p[i].blk_offsets_dev || !p[i].blk_offsets_host ||
+        !p[i].rates6_dev || argot_b200_num_blocks(&p[i].grid, &nb) || nb >= 0xffffffffull ||
+        (p[i].blk_offsets_host[nb] && !p[i].rays_dev) || p[i].blk_offsets_host[0] != 0) {
+      set_status(ARGOT_B200_EINVAL);
+      return ARGOT_B200_EINVAL;
+    }
+  }
+  auto *b = new (std::nothrow) argot_b200_batch();
+  if (!b) { set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
+  auto fail = [&](int rc) {
+    argot_b200_batch_free(b);
+    set_status(rc);
+    return rc;
+  };
+  if (cudaGetDevice(&b->device) != cudaSuccess) return fail(ARGOT_B200_ECUDA);
+  cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
+  int rc = ensure_rate_tables(b->device);
+  if (rc) return fail(rc);
+  b->err = err_flag(b->device);
+  if (!b->err) return fail(ARGOT_B200_ENOMEM);
+  for (int i = 0; i < n; i++) {
+    uint64_t nb = 0;
+    argot_b200_num_blocks(&p[i].grid, &nb);
+    const uint64_t ncell = (uint64_t)p[i].grid.nx * p[i].grid.ny * p[i].grid.nz;
+    BatchProb q;
+    q.g = make_grid(p[i].grid);
+    q.cells = (const float4 *)p[i].packed_dev;
+    q.raw = (const float4 *)p[i].packed_dev + ncell;
+    q.emit_pos = p[i].tree->emit_pos;
+    q.specn = p[i].tree->emit_specn;
+    q.total = p[i].tree->emit_total;
+    q.blk_off = p[i].blk_offsets_dev;
+    q.rays = p[i].rays_dev;
+    q.rates6 = p[i].rates6_dev;
+    q.nray = p[i].blk_offsets_host[nb];
+    b->probs.push_back(q);
+    b->blk_off.emplace_back(p[i].blk_offsets_host, p[i].blk_offsets_host + nb + 1);
+  }
+  if (cudaMalloc(&b->probs_dev, sizeof(BatchProb) * n) != cudaSuccess) return fail(ARGOT_B200_ENOMEM);
+  if (cudaMemcpy(b->probs_dev, b->probs.data(), sizeof(BatchProb) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(ARGOT_B200_ECUDA);
+  if (cudaMalloc(&b->next_dev, sizeof(uint32_t)) != cudaSuccess) return fail(ARGOT_B200_ENOMEM);
+  if (cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess) return fail(ARGOT_B200_ECUDA);
+  rc = build_items(b);
+  if (rc) return fail(rc);
+  *out = b;
+  set_status(0);
+  return 0;
+}
+
+void argot_b200_batch_free(argot_b200_batch *b) {
+  if (!b) return;
+  drop_graph(b);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  cudaFree(b->probs_dev);
+  cudaFree(b->items_dev);
+  cudaFree(b->next_dev);
+  delete b;
+}
+
+int argot_b200_batch_configure(argot_b200_batch *b, const argot_b200_batch_config *c) {
+  if (!b || !c || !config_valid(*c)) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
+  b->cfg = *c;
+  const int rc = build_items(b);
+  set_status(rc);
+  return rc;
+}
+
+int argot_b200_batch_get_config(const argot_b200_batch *b, argot_b200_batch_config *c) {
+  if (!b || !c) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
+  *c = b->cfg;
+  set_status(0);
+  return 0;
+}
+
+int argot_b200_batch_num_items(const argot_b200_batch *b) { return b ? (int)b->nitems : -1; }
+
+int argot_b200_batch_run(argot_b200_batch *b, unsigned long long *crossings_dev, void *stream) {
+  if (!b) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
+  const int rc = launch(b, crossings_dev, (cudaStream_t)stream);
+  set_status(rc);
+  return rc;
+}
+
+int argot_b200_batch_graph_launch(argot_b200_batch *b, void *stream) {
+  if (!b) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
+  if (!b->exec) {
+    ARGOT_CUDA_TRY(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+    const int rc = launch(b, nullptr, b->cap);
+    cudaGraph_t gr = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->cap, &gr);
+    if (rc || e != cudaSuccess) {
+      if (gr) cudaGraphDestroy(gr);
+      const int r = rc ? rc : status_from_cuda(e);
+      set_status(r);
+      return r;
+    }
+    b->graph = gr;
+    ARGOT_CUDA_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  }
+  ARGOT_CUDA_TRY(cudaGraphLaunch(b->exec, (cudaStream_t)stream));
+  set_status(0);
+  return 0;
+}
+
+// Coordinate search over the configuration: starting from the current one,
+// each parameter in turn takes every candidate value with the others held;
+// a candidate is timed by CUDA events around `reps` launches after one
+// warm-up launch.  Leaves the best configuration set.
+int argot_b200_batch_tune(argot_b200_batch *b, int reps, argot_b200_batch_config *best_out, float *best_ms,
+                          void *stream) {
+  if (!b || reps < 1) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaEvent_t e0, e1;
+  ARGOT_CUDA_TRY(cudaEventCreate(&e0));
+  ARGOT_CUDA_TRY(cudaEventCreate(&e1));
+  auto time_cfg = [&](const argot_b200_batch_config &c, float *ms) -> int {
+    b->cfg = c;
+    int rc = build_items(b);
+    if (rc) return rc;
+    if ((rc = launch(b, nullptr, st))) return rc;
+    ARGOT_CUDA_TRY(cudaEventRecord(e0, st));
+    for (int i = 0; i < reps; i++)
+      if ((rc = launch(b, nullptr, st))) return rc;
+    ARGOT_CUDA_TRY(cudaEventRecord(e1, st));
+    ARGOT_CUDA_TRY(cudaEventSynchronize(e1));
+    ARGOT_CUDA_TRY(cudaEventElapsedTime(ms, e0, e1));
+    *ms /= (float)reps;
+    return 0;
+  };
+  argot_b200_batch_config best = b->cfg;
+  float t_best = 0.f;
+  int rc = time_cfg(best, &t_best);
+  const int warps[] = {4, 8};
+  const int per_sm[] = {1, 2, 3, 4, 6, 8};
+  const int tiles[] = {1, 2, 4, 8, 16, 64};
+  const int orders[] = {0, 1};
+  for (int pass = 0; pass < 2 && !rc; pass++) {
+    for (int dim = 0; dim < 4 && !rc; dim++) {
+      const int *vals = dim == 0 ? warps : dim == 1 ? per_sm : dim == 2 ? tiles : orders;
+      const int nv = dim == 0 ? 2 : dim == 1 ? 6 : dim == 2 ? 6 : 2;
+      for (int k = 0; k < nv && !rc; k++) {
+        argot_b200_batch_config c = best;
+        int *field = dim == 0 ? &c.warps_per_cta : dim == 1 ? &c.ctas_per_sm : dim == 2 ? &c.blocks_per_item : &c.order;
+        if (*field == vals[k]) continue;
+        *field = vals[k];
+        if (dim == 1 && vals[k] > max_ctas_per_sm(c.warps_per_cta)) continue;
+        float t = 0.f;
+        rc = time_cfg(c, &t);
+        if (!rc && t < t_best) {
+          t_best = t;
+          best = c;
+        }
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) { set_status(rc); return rc; }
+  b->cfg = best;
+  rc = build_items(b);
+  if (rc) { set_status(rc); return rc; }
+  if (best_out) *best_out = best;
+  if (best_ms) *best_ms = t_best;
+  set_status(0);
+  return 0;
+}
+
+}  // extern "C"

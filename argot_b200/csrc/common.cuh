@@ -86,7 +86,9 @@ struct argot_b200_dev_tree {
   double *emit_total;      // n_emit
   // surrogate inputs (set by argot_b200_dev_tree_set_blackbody): log10 T of
   // an emitter whose spectrum is a single-temperature blackbody (NaN
-  // otherwise) and its six thin-limit integrals sum_nu w_j(nu) s_nu
+  // otherwise), its six thin-limit integrals I_j0 = sum_nu w_j(nu) s_nu and
+  // the first moments m_js = sum_nu w_j s_nu sigma_s / sigma_s0 / I_j0
   float *emit_logT;        // n_emit
   double *emit_i0;         // n_emit x 6
+  float *emit_m;           // n_emit x 18 (j-major: m[3 j + s])
 };

@@ -487,6 +487,7 @@ void argot_b200_dev_tree_free(argot_b200_dev_tree *d) {
   cudaFree(d->emit_total);
   cudaFree(d->emit_logT);
   cudaFree(d->emit_i0);
+  cudaFree(d->emit_m);
   delete d;
 }
 
@@ -494,7 +495,8 @@ void argot_b200_dev_tree_free(argot_b200_dev_tree *d) {
 // sources are all blackbodies of one temperature T (src_T[i] > 0) has the
 // normalised spectrum of that blackbody; any other emitter gets NaN and
 // is always integrated exactly.  Also uploads each emitter's six thin-limit
-// integrals sum_nu w_j(nu) s_nu of its own normalised spectrum.
+// integrals I_j0 = sum_nu w_j(nu) s_nu of its own normalised spectrum and
+// the first moments m_js = sum_nu w_j s_nu sigma_s(nu) / sigma_s0 / I_j0.
 int argot_b200_dev_tree_set_blackbody(const argot_b200_tree *t, argot_b200_dev_tree *d, const float *src_T,
                                       void *stream) {
   if (!t || !d || !src_T || d->n_src != t->nsrc) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
@@ -511,23 +513,36 @@ int argot_b200_dev_tree_set_blackbody(const argot_b200_tree *t, argot_b200_dev_t
   }
   for (int j = 0; j < t->nsrc; j++) logT[nn + j] = temp_of(src_T[j]);
   std::vector<double> w(6 * kNu), i0(6 * ne);
+  std::vector<float> mom(18 * ne);
   host_rate_weights(w.data());
+  double sig0[3];
+  for (int s = 0; s < 3; s++) {
+    sig0[s] = 0.0;
+    for (int k = 0; k < kNu && sig0[s] == 0.0; k++) sig0[s] = w[s * kNu + k];
+  }
   std::vector<double> spec(ne * kNu);
   argot_b200_tree_emitters(t, nullptr, spec.data());
   for (size_t e = 0; e < ne; e++) {
     double tot = 0.0;
     for (int k = 0; k < kNu; k++) tot += spec[e * kNu + k];
     for (int j = 0; j < 6; j++) {
-      double s = 0.0;
-      for (int k = 0; k < kNu; k++) s += w[j * kNu + k] * (spec[e * kNu + k] / tot);
-      i0[e * 6 + j] = s;
+      double s0 = 0.0, m[3] = {0.0, 0.0, 0.0};
+      for (int k = 0; k < kNu; k++) {
+        const double a = w[j * kNu + k] * (spec[e * kNu + k] / tot);
+        s0 += a;
+        for (int s = 0; s < 3; s++) m[s] += a * (w[s * kNu + k] / sig0[s]);
+      }
+      i0[e * 6 + j] = s0;
+      for (int s = 0; s < 3; s++) mom[e * 18 + 3 * j + s] = s0 > 0.0 ? (float)(m[s] / s0) : 0.f;
     }
   }
   cudaStream_t st = (cudaStream_t)stream;
   if (!d->emit_logT) ARGOT_CUDA_TRY(cudaMalloc(&d->emit_logT, sizeof(float) * ne));
   if (!d->emit_i0) ARGOT_CUDA_TRY(cudaMalloc(&d->emit_i0, sizeof(double) * 6 * ne));
+  if (!d->emit_m) ARGOT_CUDA_TRY(cudaMalloc(&d->emit_m, sizeof(float) * 18 * ne));
   ARGOT_CUDA_TRY(cudaMemcpyAsync(d->emit_logT, logT.data(), sizeof(float) * ne, cudaMemcpyHostToDevice, st));
   ARGOT_CUDA_TRY(cudaMemcpyAsync(d->emit_i0, i0.data(), sizeof(double) * 6 * ne, cudaMemcpyHostToDevice, st));
+  ARGOT_CUDA_TRY(cudaMemcpyAsync(d->emit_m, mom.data(), sizeof(float) * 18 * ne, cudaMemcpyHostToDevice, st));
   ARGOT_CUDA_TRY(cudaStreamSynchronize(st));
   set_status(0);
   return 0;

@@ -64,8 +64,8 @@ __device__ __forceinline__ double u01(uint64_t x) { return (double)(x >> 11) * (
 
 // -------------------------------------------------------- training samples
 // x = (log10 tau_HI, log10 tau_HeI, log10 tau_HeII) uniform in [-6, 3],
-// log10 T on the grid of the given spectra; y = t_j = ln(1 - ln(I_j/I_j0))
-// from the exact 256-bin sum in FP64.
+// log10 T on the grid of the given spectra; y = q_j = ln(y_j / ylin_j)
+// (mlp.cuh) from the exact 256-bin sums in FP64.
 __global__ void k_mlp_samples(const double *__restrict__ spec, const double *__restrict__ i0, int nT,
                               uint64_t n, uint64_t seed, float *__restrict__ X, float *__restrict__ Y) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
@@ -77,10 +77,15 @@ __global__ void k_mlp_samples(const double *__restrict__ spec, const double *__r
     const double tau[3] = {exp10(lt[0]), exp10(lt[1]), exp10(lt[2])};
     const double *sp = spec + (size_t)it * kNu;
     double I[kMlpOut] = {0, 0, 0, 0, 0, 0};
+    double lin[kMlpOut] = {0, 0, 0, 0, 0, 0};  // sum_nu w_j s_nu (tau . shat)
     for (int k = 0; k < kNu; k++) {
-      const double a = exp(-(tau[0] * c_mt.shat[0][k] + tau[1] * c_mt.shat[1][k] + tau[2] * c_mt.shat[2][k])) * sp[k];
+      const double ts = tau[0] * c_mt.shat[0][k] + tau[1] * c_mt.shat[1][k] + tau[2] * c_mt.shat[2][k];
+      const double a = exp(-ts) * sp[k];
 #pragma unroll
-      for (int j = 0; j < kMlpOut; j++) I[j] = fma(c_mt.w[j][k], a, I[j]);
+      for (int j = 0; j < kMlpOut; j++) {
+        I[j] = fma(c_mt.w[j][k], a, I[j]);
+        lin[j] = fma(c_mt.w[j][k] * sp[k], ts, lin[j]);
+      }
     }
     X[4 * i + 0] = (float)lt[0];
     X[4 * i + 1] = (float)lt[1];
@@ -88,8 +93,10 @@ __global__ void k_mlp_samples(const double *__restrict__ spec, const double *__r
     X[4 * i + 3] = (float)(kTLo + (kTHi - kTLo) * (double)it / (double)(nT - 1));
 #pragma unroll
     for (int j = 0; j < kMlpOut; j++) {
-      const double y = (I[j] > 0.0 && i0[(size_t)it * kMlpOut + j] > 0.0) ? log(I[j] / i0[(size_t)it * kMlpOut + j]) : -700.0;
-      Y[kMlpOut * i + j] = (float)log1p(-y);
+      const double z = i0[(size_t)it * kMlpOut + j];
+      const double y = (I[j] > 0.0 && z > 0.0) ? log(I[j] / z) : -700.0;
+      const double ylin = -lin[j] / z;
+      Y[kMlpOut * i + j] = (float)log(y / ylin);
     }
   }
 }
@@ -127,8 +134,8 @@ __device__ void load_weights(SmemW &s, const float *__restrict__ p) {
 }
 
 // One thread per sample.  Stores the pre-activations z1..z3 and the
-// activations a1..a3 (a1, a2 rounded to BF16; a3 kept in FP32 because it
-// enters the last layer as a hi + lo pair) in [unit][sample] layout for the
+// activations a1..a3 (FP32: the tensor-core inference carries every
+// activation as a BF16 pair hi + lo) in [unit][sample] layout for the
 // backward pass, and the normalised outputs o.
 template <bool kStore>
 __global__ void __launch_bounds__(128) k_mlp_fwd(const float *__restrict__ p, const float *__restrict__ X,
@@ -148,7 +155,7 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(const float *__restrict__ p, co
     float z = s.b1[j];
 #pragma unroll
     for (int c = 0; c < kMlpIn; c++) z = fmaf(s.w1[j * kMlpIn + c], x[c], z);
-    a[j] = bf16_round(silu_ref(z));
+    a[j] = silu_ref(z);
     if (kStore) { Z[(size_t)j * nb + i] = z; A[(size_t)j * nb + i] = a[j]; }
   }
 #pragma unroll 4
@@ -156,7 +163,7 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(const float *__restrict__ p, co
     float z = s.b2[j];
 #pragma unroll
     for (int k = 0; k < kMlpH; k++) z = fmaf(s.w2[j * kMlpH + k], a[k], z);
-    h[j] = bf16_round(silu_ref(z));
+    h[j] = silu_ref(z);
     if (kStore) { Z[(size_t)(kMlpH + j) * nb + i] = z; A[(size_t)(kMlpH + j) * nb + i] = h[j]; }
   }
 #pragma unroll 4
@@ -182,7 +189,7 @@ __device__ __forceinline__ float silu_grad(float z) {
 }
 
 // dO = 2 (o - target_norm) / (nb * 6); back through the layers (straight
-// through the BF16 rounding).  Writes dZ4 (= dO), dZ3, dZ2, dZ1 in
+// through the BF16 rounding of the weights).  Writes dZ4 (= dO), dZ3, dZ2, dZ1 in
 // [unit][sample] layout and each sample's squared error.
 __global__ void __launch_bounds__(128) k_mlp_bwd(const float *__restrict__ p, const float *__restrict__ Yt,
                                                  int nb, const float *__restrict__ Z, const float *__restrict__ O,

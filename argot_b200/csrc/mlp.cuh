@@ -6,19 +6,24 @@
 //   w_j = sigma_s (j = s) or sigma_s (nu - nu_s)^+ (j = 3 + s),
 // are what the reference's 256-bin loop sums (calc_photoion_rate.c:285-387)
 // once the photon-conserving cell factor is written as an integral across
-// the cell (see photoion_surrogate in photoion.cu).  The network predicts
-//   t_j = ln(1 - ln(I_j(M) / I_j(0)))          (t >= 0, range ~[0, 5.5])
-// from x = (log10 tau_HI, log10 tau_HeI, log10 tau_HeII, log10 T), with
-// tau_s = M_s sigma_s at the species' first absorbing bin; the log-compressed
-// target keeps every output O(1) while a thin ray (small ln I/I0) keeps an
-// absolute error in ln I equal to that in t.
+// the cell (see surrogate.cu).  With tau_s = M_s sigma_s at the species'
+// first absorbing bin, y_j = ln(I_j(M) / I_j(0)) is the cumulant generating
+// function of the normalised cross sections under the weight w_j s_nu, so
+//   ylin_j = -sum_s tau_s m_js <= y_j <= 0   (Jensen),
+// with m_js the first moments of sigma_s / sigma_s(first bin) under that
+// weight.  The network predicts
+//   q_j = ln(y_j / ylin_j)                     (q <= 0, range ~[-7, 0])
+// from x = (log10 tau_HI, log10 tau_HeI, log10 tau_HeII, log10 T).  An
+// error dq of the network is a relative error |y| dq of I: it vanishes for
+// thin rays (the bright ones) instead of staying at the size of dq.
 //
 // Architecture: 4 -> 64 -> 64 -> 64 -> 6, SiLU, BF16 weights and activations
-// with FP32 accumulation.  The network's input (normalised x) and its last
-// hidden layer enter the tensor cores as a BF16 pair hi + lo (an exact
-// split of the FP32 value to 16 mantissa bits), so that the two ends that
-// set the output's precision are not limited by BF16 rounding; the inner
-// activations are single BF16 values.
+// with FP32 accumulation.  Every activation (and the normalised input)
+// enters the tensor cores as a BF16 pair hi + lo, the FP32 value split to
+// 16 mantissa bits, so that the output is not limited by the 8-bit BF16
+// rounding of the activations: single-BF16 activations left a floor of
+// ~5e-3 in q, which no training removes.  The weights are single BF16
+// values (the network is trained with them rounded).
 #pragma once
 #include <cuda_bf16.h>
 
@@ -42,22 +47,15 @@ constexpr int kMlpParams = kOffB4 + kMlpOut;
 // input / output normalisation
 constexpr float kTauLo = -6.f, kTauHi = 3.f;     // log10 tau range
 constexpr float kTLo = 4.f, kTHi = 5.5f;         // log10 T range
-constexpr float kOutShift = 2.75f, kOutScale = 2.75f;
+constexpr float kOutShift = -3.5f, kOutScale = 3.5f;  // q = 3.5 o - 3.5
 
 __device__ __forceinline__ float bf16_round(float x) {
   return __bfloat162float(__float2bfloat16_rn(x));
 }
 
-// SiLU as the inference kernel evaluates it: z * sigmoid(z) with the
-// hardware tanh, sigmoid(z) = (1 + tanh(z/2)) / 2.
-__device__ __forceinline__ float tanh_approx(float x) {
-  float y;
-  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-__device__ __forceinline__ float silu_fast(float z) {
-  const float h = 0.5f * z;
-  return fmaf(h, tanh_approx(h), h);
-}
+// SiLU as the inference kernel evaluates it: z / (1 + e^-z) with the fast
+// exponential and division (relative error a few 1e-7, far below the
+// network's own; the hardware tanh, 2^-11, would set a floor of its own).
+__device__ __forceinline__ float silu_acc(float z) { return __fdividef(z, 1.f + __expf(-z)); }
 
 }  // namespace argot

@@ -8,15 +8,21 @@
 //   Gamma_s = P_s int_0^1 I_s(N + u dN) du,  P_s = Ndot dN_s / (n_s V_shell),
 // with I_j(M) the thin-cell integral of mlp.cuh at column M.  The integral
 // over u is taken by Gauss-Legendre quadrature with 1, 2 or 3 nodes chosen
-// from the cell's largest optical depth dtau_max (quadrature error < 3e-5);
+// from the cell's largest optical depth dtau_max (relative error below
+// dtau^2/24, dtau^4/4320 and dtau^6/2016000: < 4e-5 at the switch points);
 // the network gives I_j / I_j0 at each node and the emitter's exact thin
 // integrals I_j0 restore the scale.
 //
-// A ray takes the exact FP32 quadrature instead when its emitter is not a
-// single-temperature blackbody in [1e4, 10^5.5] K, when dtau_max > 2, when a
-// node's log10 tau lies above 3, or when the validated error bound of the
-// network at the predicted outputs (the envelope measured on held-out
-// samples) exceeds the tolerance.
+// Error control per cell.  Kernel 1 predicts every ray's six contributions
+// c_j with a relative error bound eps (from the validated envelope of the
+// network's error, measured on held-out samples) and a lower bound S_j of
+// each cell's total, sum c_j (1 - eps).  Kernel 2 keeps the predictions of the rays with the smallest
+// shares beta = eps max_j c_j / S_j while their sum stays within the cell's
+// budget tol, so that the surrogate's error is at most tol S_j per cell and
+// output; the other rays take the exact FP32 quadrature.  A ray always
+// takes the exact quadrature when its emitter is not a single-temperature
+// blackbody in [1e4, 10^5.5] K, when dtau_max > 2, or when a node's
+// log10 tau lies above 3.
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -32,8 +38,11 @@ namespace argot {
 
 int grid_blocks_for_rates(uint64_t n, int threads);
 
-constexpr int kEnvBins = 64;
-constexpr float kEnvTMax = 6.0f;
+constexpr int kEnvBins = 64;        // error envelope bins over predicted q
+constexpr float kEnvQLo = -7.0f;     // ... in [-7, 0]
+constexpr int kHistBins = 64;        // half-octave bins of a ray's budget share
+constexpr float kGLErr = 4e-5f;      // relative error of the Gauss-Legendre cell factor
+constexpr int kWorkPlanes = 7;       // c_0..c_5, eps per ray
 constexpr int kSurWarps = 4;
 constexpr int kMaxEval = 96;  // 32 rays x 3 quadrature nodes
 
@@ -44,21 +53,30 @@ struct SurWeights {
   uint2 f3[8][4][32];     // layer 3
   uint2 f4[8][32];        // layer 4: 1 N-tile x 8 K-steps (hidden hi | lo)
   float b1[64], b2[64], b3[64], b4[8];
-  float env[6][kEnvBins];
+  float env[6][kEnvBins]; // e^dq - 1, dq the bound of |error of q| per output and bin of q^
   float sig0[3];
-  float tol;
+  float tol;              // per-cell relative error budget
 };
 
-struct SurSmem {
+struct PredSmem {
   SurWeights w;
-  float4 tab[3 * kNu];
   // per warp
   float x[kSurWarps][kMaxEval][4];     // normalised network inputs
-  float tout[kSurWarps][kMaxEval][6];  // network outputs t_j
-  float nd[kSurWarps][32][6];          // N_s, dN_s (cm^-2, float)
-  double p[kSurWarps][32][3];          // prefactors
-  double out[kSurWarps][32][6];        // per-ray rates
-  int e[kSurWarps][32], t[kSurWarps][32], ev0[kSurWarps][32], nq[kSurWarps][32];
+  float tout[kSurWarps][kMaxEval][6];  // network outputs q_j
+  float c[kSurWarps][32][6];           // predicted per-ray contributions
+  int t[kSurWarps][32];
+};
+
+struct FinSmem {
+  float4 tab[3 * kNu];
+  // per warp
+  float Sc[kSurWarps][32][6];                // lower bounds of the cell totals
+  unsigned hist[kSurWarps][32][kHistBins];   // budget-share histogram per cell
+  int thr[kSurWarps][32];                    // last accepted bin per cell
+  float nd[kSurWarps][32][6];                // N_s, dN_s (cm^-2, float)
+  double p[kSurWarps][32][3];                // prefactors
+  double out[kSurWarps][32][6];              // per-ray rates
+  int e[kSurWarps][32], t[kSurWarps][32];
 };
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
@@ -72,6 +90,23 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], 
       "{%0,%1,%2,%3};\n"
       : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b.x), "r"(b.y));
+}
+
+// x -> BF16 pair (hi, lo) with hi + lo = x to 16 mantissa bits, packed two
+// values per register as the mma fragments want them.
+__device__ __forceinline__ void split_bf16x2(float x0, float x1, uint32_t *hi, uint32_t *lo) {
+  const float h0 = bf16_round(x0), h1 = bf16_round(x1);
+  *hi = pack_bf16x2(h0, h1);
+  *lo = pack_bf16x2(x0 - h0, x1 - h1);
+}
+
+// SiLU of the 8 accumulator values of two N-tiles, in fragment order.
+__device__ __forceinline__ void silu8(const float (&a)[4], const float (&b)[4], float (&s)[8]) {
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    s[i] = silu_acc(a[i]);
+    s[4 + i] = silu_acc(b[i]);
+  }
 }
 
 // The network on 16 evaluations (rows r0..r0+15 of the warp's list).  The
@@ -107,16 +142,17 @@ __device__ __forceinline__ void mlp_tile16(const SurWeights &W, const float (*x)
     acc[j][0] = bb0; acc[j][1] = bb1; acc[j][2] = bb0; acc[j][3] = bb1;
     mma_bf16(acc[j], a, W.f1[j][lane]);
   }
-  // layers 2 and 3
-  uint32_t A[4][4];
+  // layers 2 and 3: each activation as a BF16 pair hi + lo, both against
+  // the same weight fragment
 #pragma unroll
   for (int layer = 0; layer < 2; layer++) {
+    uint32_t Ah[4][4], Al[4][4];
 #pragma unroll
     for (int kk = 0; kk < 4; kk++) {
-      A[kk][0] = pack_bf16x2(silu_fast(acc[2 * kk][0]), silu_fast(acc[2 * kk][1]));
-      A[kk][1] = pack_bf16x2(silu_fast(acc[2 * kk][2]), silu_fast(acc[2 * kk][3]));
-      A[kk][2] = pack_bf16x2(silu_fast(acc[2 * kk + 1][0]), silu_fast(acc[2 * kk + 1][1]));
-      A[kk][3] = pack_bf16x2(silu_fast(acc[2 * kk + 1][2]), silu_fast(acc[2 * kk + 1][3]));
+      float s[8];
+      silu8(acc[2 * kk], acc[2 * kk + 1], s);
+#pragma unroll
+      for (int q = 0; q < 4; q++) split_bf16x2(s[2 * q], s[2 * q + 1], &Ah[kk][q], &Al[kk][q]);
     }
     const float *bias = layer == 0 ? W.b2 : W.b3;
 #pragma unroll
@@ -124,8 +160,11 @@ __device__ __forceinline__ void mlp_tile16(const SurWeights &W, const float (*x)
       const float bb0 = bias[8 * j + 2 * tq], bb1 = bias[8 * j + 2 * tq + 1];
       acc[j][0] = bb0; acc[j][1] = bb1; acc[j][2] = bb0; acc[j][3] = bb1;
 #pragma unroll
-      for (int kk = 0; kk < 4; kk++)
-        mma_bf16(acc[j], A[kk], layer == 0 ? W.f2[j][kk][lane] : W.f3[j][kk][lane]);
+      for (int kk = 0; kk < 4; kk++) {
+        const uint2 bf = layer == 0 ? W.f2[j][kk][lane] : W.f3[j][kk][lane];
+        mma_bf16(acc[j], Ah[kk], bf);
+        mma_bf16(acc[j], Al[kk], bf);
+      }
     }
   }
   // layer 4 on the last hidden layer split as hi | lo
@@ -133,17 +172,10 @@ __device__ __forceinline__ void mlp_tile16(const SurWeights &W, const float (*x)
 #pragma unroll
   for (int kk = 0; kk < 4; kk++) {
     float s[8];
-    s[0] = silu_fast(acc[2 * kk][0]); s[1] = silu_fast(acc[2 * kk][1]);
-    s[2] = silu_fast(acc[2 * kk][2]); s[3] = silu_fast(acc[2 * kk][3]);
-    s[4] = silu_fast(acc[2 * kk + 1][0]); s[5] = silu_fast(acc[2 * kk + 1][1]);
-    s[6] = silu_fast(acc[2 * kk + 1][2]); s[7] = silu_fast(acc[2 * kk + 1][3]);
+    silu8(acc[2 * kk], acc[2 * kk + 1], s);
     uint32_t hi[4], lo[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const float h0 = bf16_round(s[2 * q]), h1 = bf16_round(s[2 * q + 1]);
-      hi[q] = pack_bf16x2(h0, h1);
-      lo[q] = pack_bf16x2(s[2 * q] - h0, s[2 * q + 1] - h1);
-    }
+    for (int q = 0; q < 4; q++) split_bf16x2(s[2 * q], s[2 * q + 1], &hi[q], &lo[q]);
     mma_bf16(o, hi, W.f4[kk][lane]);
     mma_bf16(o, lo, W.f4[4 + kk][lane]);
   }
@@ -166,36 +198,64 @@ __device__ __forceinline__ void gl_node(int n, int i, float *u, float *w) {
   *w = ww[i];
 }
 
+// Phase A of both kernels: the ray's target lane, emitter and rate
+// parameters (columns at cell entry N_s, cell columns D_s, prefactors P_s).
+struct RayTask {
+  int tl, e;
+  RayParams p;
+};
+__device__ __forceinline__ RayTask ray_task(const GridDev &g, const float4 *__restrict__ raw,
+                                            const float4 *__restrict__ emit_pos, const double *__restrict__ total,
+                                            const uint32_t *__restrict__ rays, const float *__restrict__ tau,
+                                            uint64_t nray, uint64_t r, int bix, int biy, int biz) {
+  RayTask t;
+  const uint32_t w = __ldg(rays + r);
+  t.e = (int)(w >> 5);
+  t.tl = (int)(w & 31u);
+  const int lx = bix + (t.tl >> 4), ly = biy + ((t.tl >> 2) & 3), lz = biz + (t.tl & 3);
+  const float4 ep = __ldg(emit_pos + t.e);
+  const RayGeom geo = ray_geometry(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z);
+  const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
+  const RayCols cols = ray_columns(g, __ldg(tau + r), __ldg(tau + nray + r), __ldg(tau + 2 * nray + r), rw, geo);
+  t.p = ray_params(cols, __ldg(total + t.e));
+  return t;
+}
+
+// Kernel 1 of the surrogate rates: for every ray of blocks [b0, b1) the
+// network's prediction of its six contributions c_j and a relative error
+// bound eps (work planes 0..5 and 6; eps = +inf for a ray that must take
+// the exact quadrature), and per cell a lower bound S_j = sum c_j (1 - eps)
+// of the true total of its surrogate-capable rays (written to rates6,
+// which kernel 2 overwrites).
+//
+// Error bound of one ray: at quadrature node i the network's q has the
+// validated error bound dq = env_j(q^) (largest error on held-out samples in
+// bins of predicted q, times a safety factor), so with y^ = ylin e^q^,
+// |y - y^| <= |y^| (e^dq - 1) = x and |I - I^| <= I^ (e^x - 1) <= I^ x e^x;
+// the node bounds add up over the nodes.
 __global__ void __launch_bounds__(32 * kSurWarps)
-    k_rate_sur(GridDev g, const float4 *__restrict__ raw, const float4 *__restrict__ emit_pos,
-               const float *__restrict__ specn, const double *__restrict__ total, const float *__restrict__ emit_logT,
-               const double *__restrict__ emit_i0, const SurWeights *__restrict__ wts, uint64_t b0, uint64_t b1,
-               const uint64_t *__restrict__ blk_off, uint64_t base, const uint32_t *__restrict__ rays, uint64_t nray,
-               const float *__restrict__ tau, float *__restrict__ rates6, unsigned long long *__restrict__ counters) {
+    k_sur_predict(GridDev g, const float4 *__restrict__ raw, const float4 *__restrict__ emit_pos,
+                  const double *__restrict__ total, const float *__restrict__ emit_logT,
+                  const double *__restrict__ emit_i0, const float *__restrict__ emit_m,
+                  const SurWeights *__restrict__ wts, uint64_t b0, uint64_t b1, const uint64_t *__restrict__ blk_off,
+                  uint64_t base, const uint32_t *__restrict__ rays, uint64_t nray, const float *__restrict__ tau,
+                  float *__restrict__ rates6, float *__restrict__ work) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  SurSmem &S = *reinterpret_cast<SurSmem *>(smem_raw);
+  PredSmem &S = *reinterpret_cast<PredSmem *>(smem_raw);
   {
     const uint32_t *src = reinterpret_cast<const uint32_t *>(wts);
     uint32_t *dst = reinterpret_cast<uint32_t *>(&S.w);
     for (int i = threadIdx.x; i < (int)(sizeof(SurWeights) / 4); i += blockDim.x) dst[i] = src[i];
-    for (int k = threadIdx.x; k < kNu; k += blockDim.x) {
-      S.tab[3 * k + 0] = make_float4(c_tab.cs_l2e[0][k], c_tab.cs_l2e[1][k], c_tab.cs_l2e[2][k], c_tab.cs[0][k]);
-      S.tab[3 * k + 1] = make_float4(c_tab.cs[1][k], c_tab.cs[2][k], c_tab.hw[0][k], c_tab.hw[1][k]);
-      S.tab[3 * k + 2] = make_float4(c_tab.hw[2][k], 0.f, 0.f, 0.f);
-    }
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int grp = lane >> 3, jj = lane & 7;
-  const unsigned gmask = 0xffu << (8 * grp);
-  const float ln2 = 0.69314718055994531f;
   const float s00 = c_tab.cs[0][0];
   const float s0a = c_tab.cs[0][44], s1a = c_tab.cs[1][44];
   const float s0b = c_tab.cs[0][103], s1b = c_tab.cs[1][103], s2b = c_tab.cs[2][103];
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
-  unsigned long long n_sur = 0, n_exact = 0;
+  const float kInf = __int_as_float(0x7f800000);
   for (uint64_t b = b0 + warp; b < b1; b += nwarp) {
     int ix, iy, iz;
     const bool own_valid = block_cell(g, b, lane, &ix, &iy, &iz);
@@ -207,25 +267,14 @@ __global__ void __launch_bounds__(32 * kSurWarps)
     for (uint64_t rc = r0; rc < r1; rc += 32) {
       // ---- phase A: per-ray parameters and quadrature nodes
       const uint64_t r = rc + lane;
-      int tl = -1, nq = 0;
+      int tl = -1, nq = 0, e = 0;
+      RayParams p;
       float xin[3][4];
       if (r < r1) {
-        const uint32_t w = __ldg(rays + r);
-        const uint32_t e = w >> 5;
-        tl = (int)(w & 31u);
-        const int lx = bix + (tl >> 4), ly = biy + ((tl >> 2) & 3), lz = biz + (tl & 3);
-        const float4 ep = __ldg(emit_pos + e);
-        const RayGeom geo = ray_geometry(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z);
-        const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
-        const RayCols cols = ray_columns(g, __ldg(tau + r), __ldg(tau + nray + r), __ldg(tau + 2 * nray + r), rw, geo);
-        const RayParams p = ray_params(cols, __ldg(total + e));
-#pragma unroll
-        for (int s = 0; s < 3; s++) {
-          S.nd[wib][lane][s] = p.N[s];
-          S.nd[wib][lane][3 + s] = p.D[s];
-          S.p[wib][lane][s] = p.P[s];
-        }
-        S.e[wib][lane] = (int)e;
+        const RayTask t = ray_task(g, raw, emit_pos, total, rays, tau, nray, r, bix, biy, biz);
+        tl = t.tl;
+        e = t.e;
+        p = t.p;
         const float lT = __ldg(emit_logT + e);
         const float dt0 = p.D[0] * s00;
         const float dt1 = fmaf(p.D[0], s0a, p.D[1] * s1a);
@@ -261,8 +310,6 @@ __global__ void __launch_bounds__(32 * kSurWarps)
 #pragma unroll
         for (int c = 0; c < 4; c++) S.x[wib][pos + i][c] = xin[i][c];
       S.t[wib][lane] = tl;
-      S.ev0[wib][lane] = pos;
-      S.nq[wib][lane] = nq;
       // pad the last tile with valid inputs
       for (int q = nev + lane; q < ((nev + 15) & ~15); q += 32)
 #pragma unroll
@@ -271,41 +318,194 @@ __global__ void __launch_bounds__(32 * kSurWarps)
       // ---- phase B: the network on the tensor cores
       for (int r16 = 0; r16 < nev; r16 += 16) mlp_tile16(S.w, S.x[wib], S.tout[wib], r16, lane);
       __syncwarp();
-      // ---- phase C: surrogate rates and their error bound
-      bool need_exact = (tl >= 0) && (nq == 0);
-      if (tl >= 0 && nq > 0) {
-        const int e = S.e[wib][lane];
-        double G[6] = {0, 0, 0, 0, 0, 0};
-        float err = 0.f;
-        for (int i = 0; i < nq; i++) {
-          float u, wq;
-          gl_node(nq, i, &u, &wq);
+      // ---- phase C: predicted contributions and their error bound
+      if (tl >= 0) {
+        float cj[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float eps = kInf;
+        if (nq > 0) {
+          float mj[18];
 #pragma unroll
-          for (int j = 0; j < 6; j++) {
-            const float tt = S.tout[wib][pos + i][j];
-            const int bin = min(kEnvBins - 1, max(0, (int)(tt * (kEnvBins / kEnvTMax))));
-            err = fmaxf(err, S.w.env[j][bin]);
-            const float y = 1.f - __expf(tt);       // ln(I/I0)
-            G[j] += (double)wq * (double)__expf(y);  // I/I0 at the node
+          for (int k = 0; k < 18; k++) mj[k] = __ldg(emit_m + 18 * (size_t)e + k);
+          float G[6] = {0, 0, 0, 0, 0, 0}, dG[6] = {0, 0, 0, 0, 0, 0};
+          for (int i = 0; i < nq; i++) {
+            float u, wq;
+            gl_node(nq, i, &u, &wq);
+            float ts[3];
+#pragma unroll
+            for (int s = 0; s < 3; s++) ts[s] = fmaxf(fmaf(u, p.D[s], p.N[s]), 0.f) * S.w.sig0[s];
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+              const float qh = S.tout[wib][pos + i][j];
+              const float ylin = -fmaf(ts[0], mj[3 * j], fmaf(ts[1], mj[3 * j + 1], ts[2] * mj[3 * j + 2]));
+              const float yh = ylin * __expf(fminf(qh, 0.f));
+              const int bin = min(kEnvBins - 1, max(0, (int)((qh - kEnvQLo) * (kEnvBins / -kEnvQLo))));
+              const float x = -yh * S.w.env[j][bin];
+              const float a = wq * __expf(yh);
+              G[j] += a;
+              dG[j] = fmaf(a, x * __expf(x), dG[j]);
+            }
           }
-        }
-        if (err <= S.w.tol) {
+          eps = 0.f;
+#pragma unroll
+          for (int j = 0; j < 6; j++) eps = fmaxf(eps, G[j] > 0.f ? dG[j] / G[j] : (dG[j] > 0.f ? kInf : 0.f));
+          // plus the Gauss-Legendre quadrature error of the cell factor
+          eps += kGLErr;
 #pragma unroll
           for (int s = 0; s < 3; s++) {
-            const double pp = S.p[wib][lane][s];
-            S.out[wib][lane][s] = pp * G[s] * __ldg(emit_i0 + 6 * (size_t)e + s);
-            S.out[wib][lane][3 + s] = pp * G[3 + s] * __ldg(emit_i0 + 6 * (size_t)e + 3 + s) * kHNuL;
+            cj[s] = (float)(p.P[s] * (double)G[s] * __ldg(emit_i0 + 6 * (size_t)e + s));
+            cj[3 + s] = (float)(p.P[s] * (double)G[3 + s] * __ldg(emit_i0 + 6 * (size_t)e + 3 + s) * kHNuL);
           }
+        }
+        // the cell budget is taken from a lower bound of the true total:
+        // c_true >= c (1 - eps)
+        const float lowf = fmaxf(0.f, 1.f - eps);
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+          work[j * nray + r] = cj[j];
+          S.c[wib][lane][j] = cj[j] * lowf;
+        }
+        work[6 * nray + r] = eps;
+      }
+      __syncwarp();
+      // ---- phase E: per-cell predicted totals in ray order
+      const int nk = (int)min((uint64_t)32, r1 - rc);
+      for (int k = 0; k < nk; k++) {
+        if (S.t[wib][k] == lane) {
+#pragma unroll
+          for (int s = 0; s < 6; s++) acc[s] += S.c[wib][k][s];
+        }
+      }
+      __syncwarp();
+    }
+    if (own_valid) {
+#pragma unroll
+      for (int s = 0; s < 6; s++) rates6[s * ncell + own] = (float)acc[s];
+    }
+  }
+}
+
+// Histogram bin of a ray's share of its cell's error budget,
+//   beta = eps * max_j c_j / S_j,
+// in half-octaves: bin 64 + k holds beta in [2^(k/2), 2^((k+1)/2)), bin 0
+// everything below 2^-31.5; -1 = the ray takes the exact quadrature.  Exact
+// in float (frexpf), so both passes of kernel 2 agree bit for bit.
+__device__ __forceinline__ int beta_bin(const float *c, float eps, const float *Sc) {
+  if (!(eps < 1.f)) return -1;
+  float mx = 0.f;
+#pragma unroll
+  for (int j = 0; j < 6; j++) {
+    if (c[j] > 0.f) {
+      if (!(Sc[j] > 0.f)) return -1;
+      mx = fmaxf(mx, c[j] / Sc[j]);
+    }
+  }
+  const float beta = eps * mx;
+  if (!(beta < 1.f)) return -1;
+  if (beta <= 0.f) return 0;
+  int E;
+  const float f = frexpf(beta, &E);  // beta = f 2^E, f in [0.5, 1)
+  const int k = 2 * (E - 1) + (f >= 0.70710678f ? 1 : 0);
+  return max(0, k + kHistBins);
+}
+// upper edge of bin b
+__device__ __forceinline__ double beta_edge(int b) { return exp2(0.5 * (double)(b - kHistBins + 1)); }
+
+// Kernel 2: per cell, the rays whose error bounds fit the budget
+// tol * S_j (the smallest bounds first, by the histogram of beta; the sum
+// of a bin is bounded by its count times its upper edge) keep the
+// network's contributions; every other ray takes the exact FP32
+// quadrature.  Per-cell sums in ray order, as the exact kernels.
+__global__ void __launch_bounds__(32 * kSurWarps)
+    k_sur_finish(GridDev g, const float4 *__restrict__ raw, const float4 *__restrict__ emit_pos,
+                 const float *__restrict__ specn, const double *__restrict__ total, float tol, uint64_t b0,
+                 uint64_t b1, const uint64_t *__restrict__ blk_off, uint64_t base, const uint32_t *__restrict__ rays,
+                 uint64_t nray, const float *__restrict__ tau, const float *__restrict__ work,
+                 float *__restrict__ rates6, unsigned long long *__restrict__ counters) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FinSmem &S = *reinterpret_cast<FinSmem *>(smem_raw);
+  for (int k = threadIdx.x; k < kNu; k += blockDim.x) {
+    S.tab[3 * k + 0] = make_float4(c_tab.cs_l2e[0][k], c_tab.cs_l2e[1][k], c_tab.cs_l2e[2][k], c_tab.cs[0][k]);
+    S.tab[3 * k + 1] = make_float4(c_tab.cs[1][k], c_tab.cs[2][k], c_tab.hw[0][k], c_tab.hw[1][k]);
+    S.tab[3 * k + 2] = make_float4(c_tab.hw[2][k], 0.f, 0.f, 0.f);
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int grp = lane >> 3, jj = lane & 7;
+  const unsigned gmask = 0xffu << (8 * grp);
+  const float ln2 = 0.69314718055994531f;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
+  unsigned long long n_sur = 0, n_exact = 0;
+  for (uint64_t b = b0 + warp; b < b1; b += nwarp) {
+    int ix, iy, iz;
+    const bool own_valid = block_cell(g, b, lane, &ix, &iy, &iz);
+    const uint64_t own = own_valid ? cell_index(g, ix, iy, iz) : 0;
+#pragma unroll
+    for (int s = 0; s < 6; s++) S.Sc[wib][lane][s] = own_valid ? rates6[s * ncell + own] : 0.f;
+    for (int k = 0; k < kHistBins; k++) S.hist[wib][lane][k] = 0u;
+    int bix, biy, biz;
+    block_cell(g, b, 0, &bix, &biy, &biz);
+    const uint64_t r0 = blk_off[b] - base, r1 = blk_off[b + 1] - base;
+    __syncwarp();
+    // ---- pass 1: histogram of beta per cell
+    for (uint64_t r = r0 + lane; r < r1; r += 32) {
+      const int tl = (int)(__ldg(rays + r) & 31u);
+      float c[6];
+#pragma unroll
+      for (int j = 0; j < 6; j++) c[j] = __ldg(work + j * nray + r);
+      const int bin = beta_bin(c, __ldg(work + 6 * nray + r), S.Sc[wib][tl]);
+      if (bin >= 0) atomicAdd(&S.hist[wib][tl][bin], 1u);
+    }
+    __syncwarp();
+    {
+      double cum = 0.0;
+      int thr = -1;
+      for (int k = 0; k < kHistBins; k++) {
+        const unsigned n = S.hist[wib][lane][k];
+        if (n) {
+          cum += (double)n * beta_edge(k);
+          if (cum > (double)tol) break;
+        }
+        thr = k;
+      }
+      S.thr[wib][lane] = thr;
+    }
+    __syncwarp();
+    // ---- pass 2: accepted rays keep the prediction, the rest go exact
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (uint64_t rc = r0; rc < r1; rc += 32) {
+      const uint64_t r = rc + lane;
+      int tl = -1;
+      bool need_exact = false;
+      if (r < r1) {
+        tl = (int)(__ldg(rays + r) & 31u);
+        float c[6];
+#pragma unroll
+        for (int j = 0; j < 6; j++) c[j] = __ldg(work + j * nray + r);
+        const int bin = beta_bin(c, __ldg(work + 6 * nray + r), S.Sc[wib][tl]);
+        if (bin >= 0 && bin <= S.thr[wib][tl]) {
+#pragma unroll
+          for (int j = 0; j < 6; j++) S.out[wib][lane][j] = (double)c[j];
           n_sur++;
         } else {
+          const RayTask t = ray_task(g, raw, emit_pos, total, rays, tau, nray, r, bix, biy, biz);
+#pragma unroll
+          for (int s = 0; s < 3; s++) {
+            S.nd[wib][lane][s] = t.p.N[s];
+            S.nd[wib][lane][3 + s] = t.p.D[s];
+            S.p[wib][lane][s] = t.p.P[s];
+          }
+          S.e[wib][lane] = t.e;
           need_exact = true;
         }
       }
-      // ---- phase D: exact FP32 quadrature for the rays that need it
+      S.t[wib][lane] = tl;
+      __syncwarp();
+      // exact FP32 quadrature, four rays at a time, eight lanes each
       unsigned mexact = __ballot_sync(0xffffffffu, need_exact);
       n_exact += need_exact;
       while (mexact) {
-        // four rays at a time, eight lanes each
         int q[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
@@ -345,7 +545,7 @@ __global__ void __launch_bounds__(32 * kSurWarps)
         __syncwarp();
       }
       __syncwarp();
-      // ---- phase E: per-cell sums in ray order
+      // ---- per-cell sums in ray order
       const int nk = (int)min((uint64_t)32, r1 - rc);
       for (int k = 0; k < nk; k++) {
         if (S.t[wib][k] == lane) {
@@ -359,6 +559,7 @@ __global__ void __launch_bounds__(32 * kSurWarps)
 #pragma unroll
       for (int s = 0; s < 6; s++) rates6[s * ncell + own] = (float)acc[s];
     }
+    __syncwarp();
   }
   if (counters) {
     for (int o = 16; o; o >>= 1) {
@@ -421,6 +622,7 @@ using namespace argot;
 struct argot_b200_surrogate {
   int device;
   SurWeights *dev;
+  float tol;  // host copy of the per-cell budget (kernel 2 argument)
 };
 
 namespace {
@@ -448,9 +650,9 @@ uint2 frag(F w, int j, int kk, int lane) {
 
 extern "C" {
 
-// params: the 9030 FP32 network parameters (host); env: 6 x 64 error bound
-// of ln(I/I0) in bins of predicted t over [0, 6) (host); tol: largest bound
-// accepted per ray.
+// params: the 9030 FP32 network parameters (host); env: 6 x 64 bound of
+// |error of q| in bins of predicted q over [-7, 0] (host); tol: per-cell
+// relative error budget of the surrogate's contributions.
 int argot_b200_surrogate_create(const float *params, const float *env, float tol, argot_b200_surrogate **out) {
   if (!params || !env || !out || !(tol > 0.f)) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
   auto *h = new (std::nothrow) SurWeights();
@@ -471,7 +673,9 @@ int argot_b200_surrogate_create(const float *params, const float *env, float tol
   std::memcpy(h->b2, params + kOffB2, sizeof(float) * 64);
   std::memcpy(h->b3, params + kOffB3, sizeof(float) * 64);
   for (int j = 0; j < 8; j++) h->b4[j] = j < kMlpOut ? params[kOffB4 + j] : 0.f;
-  std::memcpy(h->env, env, sizeof(float) * 6 * kEnvBins);
+  // kernel 1 uses e^dq - 1: |q - q^| <= dq gives |y - y^| <= |y^| (e^dq - 1)
+  for (int j = 0; j < 6; j++)
+    for (int b = 0; b < kEnvBins; b++) h->env[j][b] = (float)std::expm1((double)env[j * kEnvBins + b]);
   double w6[6 * kNu];
   host_rate_weights(w6);
   for (int s = 0; s < 3; s++) {
@@ -481,6 +685,7 @@ int argot_b200_surrogate_create(const float *params, const float *env, float tol
   h->tol = tol;
   auto *s = new (std::nothrow) argot_b200_surrogate();
   if (!s) { delete h; set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
+  s->tol = tol;
   cudaError_t e = cudaGetDevice(&s->device);
   if (e == cudaSuccess) e = cudaMalloc(&s->dev, sizeof(SurWeights));
   if (e == cudaSuccess) e = cudaMemcpy(s->dev, h, sizeof(SurWeights), cudaMemcpyHostToDevice);
@@ -497,7 +702,7 @@ void argot_b200_surrogate_free(argot_b200_surrogate *s) {
   delete s;
 }
 
-// t_j predictions (n x 6) for raw inputs X (n x 4: log10 tau_HI, tau_HeI,
+// q_j predictions (n x 6) for raw inputs X (n x 4: log10 tau_HI, tau_HeI,
 // tau_HeII, log10 T) with the tensor-core inference numerics.
 int argot_b200_surrogate_eval(const argot_b200_surrogate *s, const float *X, int n, float *T, void *stream) {
   if (!s || (n && (!X || !T))) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
@@ -511,16 +716,20 @@ int argot_b200_surrogate_eval(const argot_b200_surrogate *s, const float *X, int
   return 0;
 }
 
+uint64_t argot_b200_surrogate_workspace(uint64_t nray_group) { return (uint64_t)kWorkPlanes * 4u * nray_group; }
+
 // Rates of blocks [b0, b1) with the surrogate (see argot_b200_photoion_rays;
+// work: device workspace of argot_b200_surrogate_workspace(nray) bytes;
 // counters, optional device uint64[2], receive the numbers of rays taken by
 // the surrogate and by the exact quadrature).
 int argot_b200_photoion_rays_surrogate(const argot_b200_grid *gp, const void *packed, const argot_b200_dev_tree *t,
                                        const argot_b200_surrogate *sur, uint64_t b0, uint64_t b1,
                                        const uint64_t *blk_off, uint64_t base, const uint32_t *rays, uint64_t nray,
-                                       const float *tau, float *rates6, unsigned long long *counters, void *stream) {
+                                       const float *tau, float *work, float *rates6, unsigned long long *counters,
+                                       void *stream) {
   uint64_t nb = 0;
-  if (!grid_valid(gp) || !packed || !t || !sur || !blk_off || !rates6 || (nray && (!rays || !tau)) ||
-      !t->emit_logT || !t->emit_i0 || argot_b200_num_blocks(gp, &nb) || b0 > b1 || b1 > nb) {
+  if (!grid_valid(gp) || !packed || !t || !sur || !blk_off || !rates6 || (nray && (!rays || !tau || !work)) ||
+      !t->emit_logT || !t->emit_i0 || !t->emit_m || argot_b200_num_blocks(gp, &nb) || b0 > b1 || b1 > nb) {
     set_status(ARGOT_B200_EINVAL);
     return ARGOT_B200_EINVAL;
   }
@@ -533,8 +742,12 @@ int argot_b200_photoion_rays_surrogate(const argot_b200_grid *gp, const void *pa
   static bool attr[64] = {false};
   {
     std::lock_guard<std::mutex> lock(mu);
+    if (dev < 0 || dev >= 64) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
     if (!attr[dev]) {
-      ARGOT_CUDA_TRY(cudaFuncSetAttribute(k_rate_sur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SurSmem)));
+      ARGOT_CUDA_TRY(cudaFuncSetAttribute(k_sur_predict, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)sizeof(PredSmem)));
+      ARGOT_CUDA_TRY(cudaFuncSetAttribute(k_sur_finish, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)sizeof(FinSmem)));
       attr[dev] = true;
     }
   }
@@ -542,9 +755,15 @@ int argot_b200_photoion_rays_surrogate(const argot_b200_grid *gp, const void *pa
   const uint64_t ncell = (uint64_t)gp->nx * gp->ny * gp->nz;
   const float4 *raw = (const float4 *)packed + ncell;
   const int threads = 32 * kSurWarps;
-  k_rate_sur<<<grid_blocks_for_rates((b1 - b0) * 32, threads), threads, sizeof(SurSmem), (cudaStream_t)stream>>>(
-      g, raw, t->emit_pos, t->emit_specn, t->emit_total, t->emit_logT, t->emit_i0, sur->dev, b0, b1, blk_off, base,
-      rays, nray, tau, rates6, counters);
+  const int blocks = grid_blocks_for_rates((b1 - b0) * 32, threads);
+  cudaStream_t st = (cudaStream_t)stream;
+  k_sur_predict<<<blocks, threads, sizeof(PredSmem), st>>>(g, raw, t->emit_pos, t->emit_total, t->emit_logT,
+                                                            t->emit_i0, t->emit_m, sur->dev, b0, b1, blk_off,
+                                                            base, rays, nray, tau, rates6, work);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  k_sur_finish<<<blocks, threads, sizeof(FinSmem), st>>>(g, raw, t->emit_pos, t->emit_specn, t->emit_total,
+                                                          sur->tol, b0, b1, blk_off, base, rays, nray, tau, work,
+                                                          rates6, counters);
   ARGOT_CUDA_TRY(cudaGetLastError());
   set_status(0);
   return 0;

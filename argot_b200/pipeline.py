@@ -182,11 +182,21 @@ class Problem:
         L.check(self.lib.argot_b200_dev_tree_set_blackbody(self._tree, self._dtree, T.ctypes.data,
                                                            self.sp), "dev_tree_set_blackbody")
 
-    def rates_surrogate(self, group: RayGroup, rays, tau, rates6, surrogate, counters=None):
+    def surrogate_work(self, nray: int | None = None):
+        """Device workspace of the surrogate rates for the largest group."""
+        n = max((g.nray for g in self.groups), default=0) if nray is None else nray
+        nbytes = int(self.lib.argot_b200_surrogate_workspace(max(n, 1)))
+        return torch.empty(nbytes // 4, dtype=torch.float32, device=self.device)
+
+    def rates_surrogate(self, group: RayGroup, rays, tau, rates6, surrogate, counters=None, work=None):
+        if work is None:
+            if getattr(self, "_sur_work", None) is None or self._sur_work.numel() < 7 * group.nray:
+                self._sur_work = self.surrogate_work()
+            work = self._sur_work
         L.check(self.lib.argot_b200_photoion_rays_surrogate(
             C.byref(self.grid), _p(self.packed), self._dtree, surrogate.handle, group.b0, group.b1,
-            _p(self.blk_off), group.base, _p(rays), group.nray, _p(tau), _p(rates6), _p(counters),
-            self.sp), "photoion_rays_surrogate")
+            _p(self.blk_off), group.base, _p(rays), group.nray, _p(tau), _p(work), _p(rates6),
+            _p(counters), self.sp), "photoion_rays_surrogate")
 
     def check_device_error(self):
         L.check(self.lib.argot_b200_check_device_error(self.sp), "device error flag")

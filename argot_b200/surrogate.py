@@ -1,15 +1,17 @@
 """Training and validation of the frequency-integral surrogate (driver of
 the hand-written CUDA kernels in csrc/mlp.cu; PyTorch only allocates).
 
-The network predicts t_j = ln(1 - ln(I_j / I_j0)) for the six integrals
-of the rate stage (Gamma and heating of HI, HeI, HeII) from
+The network predicts q_j = ln(y_j / ylin_j) for the six integrals of the
+rate stage (Gamma and heating of HI, HeI, HeII), y_j = ln(I_j / I_j0) and
+ylin_j = -sum_s tau_s m_js its exact thin limit (m_js: first moments of the
+normalised cross sections under the emitter's spectrum), from
 x = (log10 tau_HI, log10 tau_HeI, log10 tau_HeII, log10 T).  Training data:
 seeded samples of the exact 256-bin quadrature, generated on the device.
 
-`error_envelope` measures, on held-out samples, the largest error of
-ln(I/I0) in bins of the predicted t; the rate kernel uses that envelope
-as the per-ray error bound that decides between the surrogate and the
-exact quadrature.
+`error_envelope` measures, on held-out samples, the largest error of q in
+bins of the predicted q; the rate kernels turn it into a per-ray relative
+error bound |y| dq of each contribution and keep, per cell, the
+predictions whose bounds fit the cell's error budget.
 """
 from __future__ import annotations
 
@@ -25,8 +27,9 @@ from . import _lib as L
 
 NT = 256            # temperature grid of the training spectra
 NPARAM = 9030
-ENV_BINS = 64       # error-envelope bins over predicted t in [0, T_MAX]
-T_MAX = 6.0
+ENV_BINS = 64       # error-envelope bins over predicted q in [Q_LO, 0]
+Q_LO = -7.0
+OUT_SCALE, OUT_SHIFT = 3.5, -3.5  # q = 3.5 o - 3.5
 DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 WEIGHTS = os.path.join(DATA, "surrogate.npz")
 
@@ -41,6 +44,9 @@ class Surrogate:
     """Inference weights of a trained network on the current device."""
 
     def __init__(self, params, env, tol: float = 5e-4):
+        """tol: per-cell relative error budget of the surrogate's
+        contributions (the rest of a 1e-3 target is left to float rounding
+        and the exact rays)."""
         self.lib = _lib()
         p = np.ascontiguousarray(params, np.float32)
         e = np.ascontiguousarray(env, np.float32)
@@ -51,7 +57,7 @@ class Surrogate:
         self.tol = tol
 
     def eval(self, X):
-        """t_j predictions (n, 6) with the tensor-core inference numerics
+        """q_j predictions (n, 6) with the tensor-core inference numerics
         (X: device float32 tensor (n, 4) of raw inputs)."""
         n = X.shape[0]
         T = torch.empty((n, 6), dtype=torch.float32, device=X.device)
@@ -174,40 +180,62 @@ class Trainer:
         return hist
 
     def predict(self, X):
-        """t_j predictions (n, 6) with the training forward (CUDA cores)."""
+        """q_j predictions (n, 6) with the training forward (CUDA cores)."""
         n = X.shape[0]
         O = torch.empty((6, n), dtype=torch.float32, device=self.dev)
         L.check(self.lib.argot_b200_mlp_forward(self.params.data_ptr(), X.data_ptr(), n,
                                                 O.data_ptr(), self.sp), "mlp_forward")
-        return (O * 2.75 + 2.75).t()
+        return (O * OUT_SCALE + OUT_SHIFT).t()
+
+    def thin_limit(self, X):
+        """ylin_j = -sum_s tau_s m_js(T) of samples X (host arrays)."""
+        X = np.asarray(X, np.float64)
+        it = np.rint((X[:, 3] - 4.0) / 1.5 * (self.nT - 1)).astype(int)
+        m = moments_grid(self.spec_np, self.i0_np)
+        return -np.einsum("ns,njs->nj", 10.0 ** X[:, :3], m[it])
 
 
-def ln_ratio(t):
-    """ln(I/I0) from t = ln(1 - ln(I/I0))."""
-    return 1.0 - np.exp(np.asarray(t, np.float64))
+def rate_weights():
+    """w_j(nu) of the six integrals (256 x 6), the cross sections (256 x 3)
+    and sigma_s at each species' first absorbing bin."""
+    from .pipeline import tables
+    nu, cs = tables()
+    cs = cs.astype(np.float64)
+    nuf = nu.astype(np.float32).astype(np.float64)
+    thr = np.array([1.0, 1.8125, 4.0])
+    w6 = np.concatenate([cs, cs * np.maximum(nuf[:, None] - thr[None, :], 0.0)], 1)
+    sig0 = np.array([cs[cs[:, s] > 0, s][0] for s in range(3)])
+    return w6, cs, sig0
 
 
-def error_envelope(t_pred, t_true, bins: int = ENV_BINS, t_max: float = T_MAX, safety: float = 1.5):
-    """Largest |error of ln(I/I0)| per output and bin of predicted t, times
-    `safety`; empty bins inherit the largest error of their output."""
-    t_pred = np.asarray(t_pred, np.float64)
-    err = np.abs(ln_ratio(t_pred) - ln_ratio(t_true))
+def moments_grid(spec, i0):
+    """m[t, j, s] = sum_nu w_j s_nu(T_t) sigma_s / sigma_s0 / I_j0(T_t)."""
+    w6, cs, sig0 = rate_weights()
+    return np.einsum("tv,vj,vs->tjs", spec, w6, cs / sig0) / i0[:, :, None]
+
+
+def error_envelope(q_pred, q_true, bins: int = ENV_BINS, q_lo: float = Q_LO, safety: float = 1.5):
+    """Largest |error of q| per output and bin of predicted q (over the bin
+    and its two neighbours), times `safety`; empty bins take the largest
+    error of their output."""
+    q_pred = np.asarray(q_pred, np.float64)
+    err = np.abs(q_pred - np.asarray(q_true, np.float64))
     env = np.zeros((6, bins))
-    b = np.clip((t_pred / t_max * bins).astype(int), 0, bins - 1)
+    b = np.clip(((q_pred - q_lo) / -q_lo * bins).astype(int), 0, bins - 1)
     for j in range(6):
         mx = np.zeros(bins)
         np.maximum.at(mx, b[:, j], err[:, j])
         seen = np.bincount(b[:, j], minlength=bins) > 0
         mx[~seen] = err[:, j].max()
-        # monotone envelope: an error bound may only grow with t
-        env[j] = np.maximum.accumulate(mx) * safety
+        nb = np.maximum(mx, np.maximum(np.r_[mx[1:], mx[-1]], np.r_[mx[0], mx[:-1]]))
+        env[j] = nb * safety
     return env
 
 
 def save(params, env, path: str = WEIGHTS, meta=None):
     os.makedirs(os.path.dirname(path), exist_ok=True)
     np.savez(path, params=np.asarray(params, np.float32), envelope=np.asarray(env, np.float32),
-             t_max=T_MAX, **(meta or {}))
+             q_lo=Q_LO, **(meta or {}))
 
 
 def load(path: str = WEIGHTS):

@@ -35,7 +35,7 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-CONFIGS = ("largest", "plain", "precision", "learned", "tiny", "plain256")
+CONFIGS = ("largest", "plain", "precision", "learned", "tiny", "plain256", "batched", "batched_small")
 METRIC = "ray-cell crossings/s (march+stitch+rates, 1 B200)"
 UNIT = "crossings/s"
 
@@ -56,6 +56,10 @@ def make_workload(name: str, rank: int = 0):
     if name == "plain256":
         # profiling case: a field larger than L2 with few rays (~4 GB on the device)
         return W.plain(edge=256, nsrc=16, seed=1 + seed_shift)
+    if name == "batched":
+        return W.batched(48, seed=3 + seed_shift)
+    if name == "batched_small":
+        return W.batched(12, seed=3 + seed_shift, edges=(16, 24, 32))
     raise ValueError(name)
 
 
@@ -293,15 +297,26 @@ def run_ours(args):
     torch.cuda.set_device(local)
     init_dist(ws, "nccl")
     dev = torch.device("cuda", local)
-    wl = make_workload(args.config, rank)
+    sharded = args.shard and ws > 1
+    # sharded: every rank holds the same problem and takes its own target slabs
+    wl = make_workload(args.config, 0 if sharded else rank)
     prec = L.PRECISION_KAHAN if args.precision == "kahan" else L.PRECISION_REFERENCE
     mode = {"f32": L.RATE_EXACT_F32, "f64": L.RATE_EXACT_F64, "surrogate": L.RATE_SURROGATE}[args.rate]
 
     free, _ = torch.cuda.mem_get_info(dev)
     pb = Problem(wl, dev, max_group_rays=None)
-    need = pb.nray * 16 + (1 << 30)
-    if need > free * 0.9:
-        pb.groups = pb._make_groups(int(free * 0.8 / 16))
+    part, cell_ranges = (0, pb.nblocks), None
+    if sharded:
+        from argot_b200 import shard
+        parts = shard.partition(pb.blk_count.cpu().numpy(), ws, wl.edge)
+        cell_ranges = [shard.cells_of(b0, b1, wl.edge) for b0, b1 in parts]
+        part = parts[rank]
+    nray_mine = int(pb.blk_off_host[part[1]] - pb.blk_off_host[part[0]])
+    ncell_mine = (cell_ranges[rank][1] - cell_ranges[rank][0]) if sharded else pb.ncell
+    use_sur = mode == L.RATE_SURROGATE or not args.no_rate_modes
+    per_ray = 16 + (28 if use_sur else 0)  # rays + columns (+ surrogate workspace)
+    need = nray_mine * per_ray + (2 << 30)
+    pb.restrict(*part, max_rays=int(free * 0.8 / per_ray) if need > free * 0.9 else None)
     stream = pb.stream
     rays, tau = pb.alloc_group_buffers()
     rates6 = torch.zeros(6 * pb.ncell, dtype=torch.float32, device=dev)
@@ -309,7 +324,7 @@ def run_ours(args):
     if single:
         pb.emit(pb.groups[0], rays)
     crossings = torch.zeros(1, dtype=torch.int64, device=dev)
-    sur = load_surrogate(pb) if (mode == L.RATE_SURROGATE or not args.no_rate_modes) else None
+    sur = load_surrogate(pb) if use_sur else None
     if mode == L.RATE_SURROGATE and sur is None:
         raise SystemExit("--rate surrogate needs trained weights (python -m argot_b200.train_surrogate)")
 
@@ -325,6 +340,8 @@ def run_ours(args):
                 pb.emit(g, rays)
             pb.march(g, rays, tau, prec, count)
             rate_pass(g)
+        if sharded:  # the exchange step: every rank's rate slab to every rank
+            shard.gather_rates(rates6, cell_ranges)
 
     # warm-up (the first one also counts the crossings)
     for w in range(args.warmup):
@@ -365,31 +382,41 @@ def run_ours(args):
     t_local = e0.elapsed_time(e1) / 1e3
     t = allmax(ws, t_local, dev)
     total_cross = allsum(ws, float(n_cross) * args.steps, dev)
-    total_cells = allsum(ws, float(pb.ncell) * args.steps, dev)
+    total_cells = allsum(ws, float(ncell_mine) * args.steps, dev)
 
     hbm, bf16, peak_kind = measured_peaks()
-    alg_bytes = 16.0 * n_cross + 36.0 * pb.nray
+    alg_bytes = 16.0 * n_cross + 36.0 * nray_mine
     achieved = alg_bytes / t_march / 1e9
     launches_per_step = len(pb.groups) * (2 + (0 if single else 1))
 
-    # end to end through the C ABI from pinned host buffers
-    e2e = run_e2e(wl, dev, prec, mode, steps=max(1, min(args.steps, 3))) if not args.no_e2e else None
+    # end to end through the C ABI from pinned host buffers (the timed
+    # pass's buffers are released first: the e2e pass allocates its own)
+    del rays, tau
+    pb._sur_work = None
+    torch.cuda.empty_cache()
+    e2e = None if args.no_e2e else run_e2e(wl, dev, prec, mode, steps=max(1, min(args.steps, 3)),
+                                           part=part if sharded else None, cell_ranges=cell_ranges)
+    if e2e is not None and ws > 1:
+        e2e["value"] = allsum(ws, e2e.pop("_crossings"), dev) / allmax(ws, e2e["s_per_step"], dev)
+    elif e2e is not None:
+        e2e.pop("_crossings")
 
     line = {
         "metric": METRIC, "value": total_cross / t, "unit": UNIT, "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded lognormal mesh + clustered sources)",
+        "higher_is_better": True, "scaling": "strong" if sharded else "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded lognormal mesh + clustered sources)",
         "config": {"workload": wl.name, "mesh": f"{wl.edge}^3", "sources": wl.nsrc,
-                   "theta": wl.theta, "rays": pb.nray, "crossings": n_cross,
+                   "theta": wl.theta, "rays": nray_mine, "crossings": n_cross,
                    "march": args.precision, "rates": args.rate, "ray_groups": len(pb.groups),
                    "l2": "inputs larger than L2 (13 GB rays, 268 MB field); no flush",
-                   "parallelism": f"{ws} independent problems (one per GPU)"},
+                   "parallelism": (f"{ws} ranks, target x-slabs of one problem, rate slabs all-gathered"
+                                   if sharded else f"{ws} independent problems (one per GPU)")},
         "gamma_cells_per_s": total_cells / t,
         "split": {"march_s": t_march, "rates_s": t_rates,
                   "march_crossings_per_s": n_cross / t_march,
-                  "rates_gamma_cells_per_s": pb.ncell / t_rates,
-                  "rates_rays_per_s": pb.nray / t_rates},
+                  "rates_gamma_cells_per_s": ncell_mine / t_rates,
+                  "rates_rays_per_s": nray_mine / t_rates},
         "roofline": {"kernel": "k_march_rays", "bound": "hbm", "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": f"{peak_kind} hbm_gbs", "traffic": None,
@@ -418,11 +445,13 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def run_e2e(wl, dev, prec, mode, steps=2):
+def run_e2e(wl, dev, prec, mode, steps=2, part=None, cell_ranges=None):
     """Same metric through the public C ABI with host buffers: each step
     copies the mesh fields and the source table from pinned host memory,
     builds the tree, generates the rays on the device, marches, computes the
-    rates and copies the six rate fields back to pinned host memory."""
+    rates and copies the six rate fields back to pinned host memory.  With
+    `part` (sharded ranks) only that block range is computed and the rate
+    slabs are all-gathered before the copy back."""
     import torch
     from argot_b200 import _lib as L
     from argot_b200.pipeline import Problem
@@ -439,6 +468,8 @@ def run_e2e(wl, dev, prec, mode, steps=2):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         pb = Problem(wl, dev, host_fields=pin)
+        if part is not None:
+            pb.restrict(*part)
         if sur is not None:
             pb.set_blackbody()
         rays, tau = pb.alloc_group_buffers()
@@ -451,6 +482,9 @@ def run_e2e(wl, dev, prec, mode, steps=2):
                 pb.rates_surrogate(g, rays, tau, rates6, sur)
             else:
                 pb.rates(g, rays, tau, rates6, mode)
+        if part is not None:
+            from argot_b200 import shard
+            rates6 = shard.gather_rates(rates6, cell_ranges).view(-1)
         out.copy_(rates6, non_blocking=True)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
@@ -461,8 +495,134 @@ def run_e2e(wl, dev, prec, mode, steps=2):
             times.append(dt)
     t = statistics.median(times)
     return {"value": cross / t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(out.numel() * 4), "s_per_step": t,
+            "d2h_bytes_per_step": int(out.numel() * 4), "s_per_step": t, "_crossings": cross,
             "includes": "H2D fields, host tree, device ray generation, march, rates, D2H rates"}
+
+
+# ------------------------------------------------------------ batched arm
+def run_batched(args):
+    """48 problems of uneven size (mesh edge from {32,48,64,96,128}, 4-512
+    sources, sigma_ln in [0.5, 1.5]) per GPU; a step is one replay of the
+    CUDA graph of the persistent batch launch (march + EXACT_F32 rates of
+    every ray of every problem), configured by the autotuner first."""
+    import torch
+    from argot_b200.batch import Batch
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    init_dist(ws, "nccl")
+    dev = torch.device("cuda", local)
+    wls = make_workload(args.config, rank)
+    B = Batch(wls, dev)
+    stream = torch.cuda.current_stream(dev)
+    cfg, tune_ms = B.tune(reps=1)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    B.run(cnt)
+    torch.cuda.synchronize()
+    B.check_device_error()
+    n_cross = int(cnt.item())
+    for _ in range(args.warmup):
+        B.graph_launch()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        B.graph_launch()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    B.check_device_error()
+    t = allmax(ws, e0.elapsed_time(e1) / 1e3, dev)
+    total_cross = allsum(ws, float(n_cross) * args.steps, dev)
+    total_cells = allsum(ws, float(B.ncell) * args.steps, dev)
+    hbm, _, peak_kind = measured_peaks()
+    alg_bytes = 16.0 * n_cross + 24.0 * B.nray
+    achieved = alg_bytes / (t / args.steps) / 1e9 if ws == 1 else None
+    e2e = None if args.no_e2e else batched_e2e(B, wls, dev, steps=max(1, min(args.steps, 3)))
+    if e2e is not None:
+        cross = e2e.pop("_crossings")
+        e2e["value"] = allsum(ws, cross, dev) / allmax(ws, e2e["s_per_step"], dev)
+    line = {
+        "metric": METRIC, "value": total_cross / t, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded lognormal meshes + uniform sources)",
+        "config": {"workload": f"{args.config}: {len(wls)} problems, edges "
+                               f"{sorted(set(w.edge for w in wls))}, sources "
+                               f"{min(w.nsrc for w in wls)}-{max(w.nsrc for w in wls)}",
+                   "rays": B.nray, "crossings": n_cross, "cells": B.ncell,
+                   "launch": "one persistent kernel per step, replayed as a CUDA graph",
+                   "autotuned": cfg, "tune_best_ms": tune_ms,
+                   "l2": f"inputs larger than L2 ({B.nray * 4 / 1e9:.1f} GB rays); no flush",
+                   "parallelism": f"{ws} independent batches (one per GPU)"},
+        "gamma_cells_per_s": total_cells / t,
+        "roofline": {"kernel": "k_batch (march + rates fused)", "bound": "hbm", "achieved": achieved,
+                     "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if achieved else None,
+                     "peak_kind": f"{peak_kind} hbm_gbs", "traffic": None,
+                     "algorithmic_bytes": alg_bytes,
+                     "bytes_model": "16 B per crossing + 24 B per ray (end points; columns stay on chip)"},
+        "clocks": clk,
+        "gpu_launches": args.steps,
+    }
+    if e2e is not None:
+        line["e2e"] = e2e
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            big = max(wls, key=lambda w: (w.edge, w.nsrc))
+            cb = cpu_sample(big, target_seconds=args.cpu_seconds, R=reference_setup(big))
+            cb.pop("_probe_rays", None)
+            cb["sample"] = f"largest problem of the batch ({big.name}): " + cb["sample"]
+            line["cpu_baseline"] = cb
+        except Exception as exc:
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(),
+                                    "kind": "reference", "sample": f"failed: {exc}"}
+    B.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def batched_e2e(B, wls, dev, steps=2):
+    """The batch step through the public C ABI with host buffers: every
+    problem's four fields copied from pinned host memory and packed, the
+    batch graph replayed, every problem's six rate fields copied back to
+    pinned host memory.  The trees and rays are set up once (they depend
+    only on the source positions and the mesh geometry)."""
+    import torch
+    pins = [[torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in wl.fields()] for wl in wls]
+    outs = [torch.empty(6 * wl.ncell, dtype=torch.float32).pin_memory() for wl in wls]
+    h2d = sum(p.numel() * 4 for ps in pins for p in ps)
+    d2h = sum(o.numel() * 4 for o in outs)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    times = []
+    for s in range(steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for pb, ps in zip(B.problems, pins):
+            for dst, src in zip(pb.fields, ps):
+                dst.copy_(src, non_blocking=True)
+            pb.pack()
+        if s == 0:
+            B.run(cnt)
+        else:
+            B.graph_launch()
+        for o, r in zip(outs, B.rates):
+            o.copy_(r, non_blocking=True)
+        torch.cuda.synchronize()
+        if s > 0:
+            times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    cross = int(cnt.item())
+    return {"value": cross / t, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "s_per_step": t, "_crossings": cross,
+            "includes": "H2D fields + pack of every problem, batch graph replay, D2H rates"}
 
 
 # ------------------------------------------------------------ reference arm
@@ -471,6 +631,8 @@ def run_reference(args):
     if rank != 0:
         return
     wl = make_workload(args.config, 0)
+    if isinstance(wl, list):  # a batch: the largest problem stands for it
+        wl = max(wl, key=lambda w: (w.edge, w.nsrc))
     R = reference_setup(wl)
     vals = []
     info = None
@@ -506,6 +668,8 @@ def main(argv=None):
     p.add_argument("--rate", choices=("f32", "f64", "surrogate"), default="f32")
     p.add_argument("--no-rate-modes", action="store_true",
                    help="skip the one-pass comparison of the three rate kernels")
+    p.add_argument("--shard", action="store_true",
+                   help="N>1: one problem, target slabs sharded over the ranks (strong scaling)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -513,6 +677,8 @@ def main(argv=None):
     args = p.parse_args(argv)
     if args.impl == "reference":
         run_reference(args)
+    elif args.config.startswith("batched"):
+        run_batched(args)
     else:
         run_ours(args)
 

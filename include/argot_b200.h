@@ -268,14 +268,16 @@ ARGOT_B200_API int argot_b200_photoion_rays(const argot_b200_grid *g, const void
 /* No counterpart in the reference: its unimplemented Gamma(tau) table
  * (multi_freq_bin.h:11-17, prim_chem/calc_gamma_of_tau.c:5-17) is the
  * closest.  The network (4 -> 64 -> 64 -> 64 -> 6, SiLU, BF16 weights and
- * activations, FP32 accumulation) predicts t_j = ln(1 - ln(I_j/I_j0)) of the
- * six thin-cell integrals I_j (Gamma and heating of HI, HeI, HeII) from
- * (log10 tau_HI, log10 tau_HeI, log10 tau_HeII, log10 T). */
+ * activations, FP32 accumulation) predicts q_j = ln(y_j / ylin_j) of the six
+ * thin-cell integrals I_j (Gamma and heating of HI, HeI, HeII), where
+ * y_j = ln(I_j / I_j0) and ylin_j = -sum_s tau_s m_js is its exact thin
+ * limit, from (log10 tau_HI, log10 tau_HeI, log10 tau_HeII, log10 T). */
 typedef struct argot_b200_surrogate argot_b200_surrogate;
 
 /* Marks every emitter whose spectrum is a single-temperature blackbody
  * (src_T[i] > 0: the temperature of source i, <= 0: other spectrum) and
- * uploads each emitter's thin-cell integrals, which the surrogate needs. */
+ * uploads each emitter's thin-cell integrals I_j0 and first moments m_js,
+ * which the surrogate needs. */
 ARGOT_B200_API int argot_b200_dev_tree_set_blackbody(const argot_b200_tree *t, argot_b200_dev_tree *d,
                                                      const float *src_T, void *stream);
 ARGOT_B200_API int argot_b200_mlp_num_params(void);
@@ -283,13 +285,13 @@ ARGOT_B200_API int argot_b200_mlp_num_params(void);
  * their thin-cell integrals (nT x 6), host arrays */
 ARGOT_B200_API int argot_b200_mlp_spectra(int nT, double *spec, double *i0);
 /* n training samples of the exact quadrature on the device: X (n x 4),
- * Y (n x 6) = t_j; spec_dev / i0_dev as from argot_b200_mlp_spectra */
+ * Y (n x 6) = q_j; spec_dev / i0_dev as from argot_b200_mlp_spectra */
 ARGOT_B200_API int argot_b200_mlp_samples(const double *spec_dev, const double *i0_dev, int nT, uint64_t n,
                                           uint64_t seed, float *X, float *Y, void *stream);
 /* device floats of workspace a training step on nb samples needs */
 ARGOT_B200_API uint64_t argot_b200_mlp_workspace(int nb);
 /* forward pass (CUDA cores, the training numerics): normalised outputs O
- * (6 x n, output-major); t_j = 2.75 * O + 2.75 */
+ * (6 x n, output-major); q_j = 3.5 * O - 3.5 */
 ARGOT_B200_API int argot_b200_mlp_forward(const float *params, const float *X, int n, float *O, void *stream);
 /* one training step (forward, backward, deterministic gradient sums,
  * Adam on the FP32 master parameters); lr == 0 computes the gradient into
@@ -298,25 +300,75 @@ ARGOT_B200_API int argot_b200_mlp_train_step(float *params, float *m, float *v, 
                                              int nb, float lr, int step, float *work, float *grad_out,
                                              double *loss_out, void *stream);
 /* inference weights on the current device from the FP32 parameters (host),
- * the validated error envelope (6 x 64 bins of predicted t over [0, 6),
- * bound of |error of ln(I/I0)|) and the per-ray tolerance */
+ * the validated error envelope (6 x 64 bins of predicted q over [-7, 0],
+ * bound of |error of q|) and the per-cell relative error budget tol */
 ARGOT_B200_API int argot_b200_surrogate_create(const float *params, const float *env, float tol,
                                                argot_b200_surrogate **out);
 ARGOT_B200_API void argot_b200_surrogate_free(argot_b200_surrogate *s);
 /* the network on raw inputs X (n x 4) with the tensor-core inference
- * numerics: t_j predictions T (n x 6) */
+ * numerics: q_j predictions T (n x 6) */
 ARGOT_B200_API int argot_b200_surrogate_eval(const argot_b200_surrogate *s, const float *X, int n, float *T,
                                              void *stream);
-/* argot_b200_photoion_rays with the surrogate and exact FP32 fallback;
- * counters (device uint64[2], optional) receive the numbers of rays taken
- * by the surrogate and by the exact quadrature */
+/* bytes of device workspace argot_b200_photoion_rays_surrogate needs for a
+ * ray group of nray_group rays (7 floats per ray) */
+ARGOT_B200_API uint64_t argot_b200_surrogate_workspace(uint64_t nray_group);
+/* argot_b200_photoion_rays with the surrogate and exact FP32 fallback: per
+ * cell and output, the rays whose validated error bounds fit within tol of
+ * the cell's total keep the network's prediction, the others take the
+ * exact quadrature.  Deterministic.  counters (device uint64[2], optional)
+ * receive the numbers of rays taken by the surrogate and by the exact
+ * quadrature. */
 ARGOT_B200_API int argot_b200_photoion_rays_surrogate(const argot_b200_grid *g, const void *packed_dev,
                                                       const argot_b200_dev_tree *t,
                                                       const argot_b200_surrogate *sur, uint64_t b0, uint64_t b1,
                                                       const uint64_t *blk_offsets_dev, uint64_t base,
                                                       const uint32_t *rays_dev, uint64_t nray_group,
-                                                      const float *tau_dev, float *rates6_dev,
+                                                      const float *tau_dev, float *work_dev, float *rates6_dev,
                                                       unsigned long long *counters_dev, void *stream);
+
+/* ---- batching: many problems in one persistent launch -------------------- */
+/* No counterpart in the reference, which runs one mesh per process.  Each
+ * problem is prepared by the calls above (pack_fields, tree_build +
+ * dev_tree_upload, count_rays + scan_blocks, emit_rays over all its blocks
+ * with base 0); one launch then marches and integrates every ray of every
+ * problem (Kahan march + EXACT_F32 rates, the same arithmetic as
+ * argot_b200_march_rays + argot_b200_photoion_rays, so each problem's rates
+ * equal those of the problem run alone, bit for bit). */
+typedef struct argot_b200_batch argot_b200_batch;
+typedef struct {
+  argot_b200_grid grid;
+  const void *packed_dev;                /* argot_b200_pack_fields output */
+  const argot_b200_dev_tree *tree;
+  const uint64_t *blk_offsets_dev;       /* nblocks + 1, argot_b200_scan_blocks */
+  const uint64_t *blk_offsets_host;      /* host copy of the same */
+  const uint32_t *rays_dev;              /* every ray of the problem, base 0 */
+  float *rates6_dev;                     /* 6 x ncell, overwritten */
+} argot_b200_batch_problem;
+typedef struct {
+  int warps_per_cta;     /* 4 or 8 */
+  int ctas_per_sm;       /* 1..16, 0 = the occupancy limit */
+  int blocks_per_item;   /* target blocks per tile of the work queue */
+  int order;             /* 0: tiles by estimated cost, largest first; 1: problem order */
+} argot_b200_batch_config;
+/* the problems' device buffers stay owned by the caller and must outlive
+ * the batch */
+ARGOT_B200_API int argot_b200_batch_create(const argot_b200_batch_problem *problems, int n,
+                                           argot_b200_batch **out);
+ARGOT_B200_API void argot_b200_batch_free(argot_b200_batch *b);
+ARGOT_B200_API int argot_b200_batch_configure(argot_b200_batch *b, const argot_b200_batch_config *cfg);
+ARGOT_B200_API int argot_b200_batch_get_config(const argot_b200_batch *b, argot_b200_batch_config *cfg);
+ARGOT_B200_API int argot_b200_batch_num_items(const argot_b200_batch *b);
+/* one persistent launch over every problem (crossings_dev: optional device
+ * counter of ray-cell crossings, added to) */
+ARGOT_B200_API int argot_b200_batch_run(argot_b200_batch *b, unsigned long long *crossings_dev, void *stream);
+/* the same launch as a CUDA graph, captured on first use (and after every
+ * configuration change), replayed on `stream` */
+ARGOT_B200_API int argot_b200_batch_graph_launch(argot_b200_batch *b, void *stream);
+/* the autotuner: coordinate search over the configuration, each candidate
+ * timed with CUDA events over `reps` launches on the batch itself; leaves
+ * the fastest configuration set */
+ARGOT_B200_API int argot_b200_batch_tune(argot_b200_batch *b, int reps, argot_b200_batch_config *best,
+                                         float *best_ms, void *stream);
 
 /* Reads and clears the device-side error flag of the current device (set
  * when a march exceeded its step bound, which only non-finite input can

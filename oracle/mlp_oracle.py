@@ -4,9 +4,10 @@ forward / backward kernels in argot_b200/csrc/mlp.cu.
 
 Same architecture and numerics contract as the device code:
 4 -> 64 -> 64 -> 64 -> 6, SiLU; weights rounded to BF16 (biases not);
-first two hidden activations rounded to BF16 after SiLU; last hidden layer
-and inputs unrounded; loss = mean over samples and outputs of the squared
-error of the normalised output, gradients straight through the rounding.
+inputs and activations unrounded (the tensor-core inference carries each
+as a BF16 pair hi + lo, 16 mantissa bits); loss = mean over samples and
+outputs of the squared error of the normalised output, gradients straight
+through the weight rounding.
 """
 from __future__ import annotations
 
@@ -24,7 +25,7 @@ OFF_B4 = OFF_W4 + NOUT * H
 NPARAM = OFF_B4 + NOUT
 
 TAU_LO, TAU_HI, T_LO, T_HI = -6.0, 3.0, 4.0, 5.5
-OUT_SHIFT = OUT_SCALE = 2.75
+OUT_SHIFT, OUT_SCALE = -3.5, 3.5
 
 
 def bf16(x):
@@ -63,9 +64,9 @@ def forward(p, X):
     W1, W2, W3, W4 = (bf16(w.astype(np.float32)) for w in (W1, W2, W3, W4))
     x = norm_in(X)
     z1 = x @ W1.T + b1
-    a1 = bf16(silu(z1).astype(np.float32))
+    a1 = silu(z1)
     z2 = a1 @ W2.T + b2
-    a2 = bf16(silu(z2).astype(np.float32))
+    a2 = silu(z2)
     z3 = a2 @ W3.T + b3
     a3 = silu(z3)
     o = a3 @ W4.T + b4
@@ -95,9 +96,17 @@ def loss_and_grad(p, X, Y):
     return loss, g
 
 
-def exact_targets(X, spec, i0, cs, sig0, w6):
-    """t_j = ln(1 - ln(I_j / I_j0)) by the exact 256-bin sum (FP64); spec
-    rows indexed by the temperature grid position encoded in X[:, 3]."""
+def moments(spec, i0, cs, sig0, w6):
+    """m[t, j, s]: first moment of sigma_s / sigma_s0 under the weight
+    w_j(nu) s_nu(T_t), normalised by I_j0."""
+    shat = cs / sig0
+    return np.einsum("tv,vj,vs->tjs", spec, w6, shat) / i0[:, :, None]
+
+
+def exact_targets(X, spec, i0, cs, sig0, w6, with_y=False):
+    """q_j = ln(y_j / ylin_j), y_j = ln(I_j / I_j0), ylin_j = -sum_s tau_s m_js,
+    by the exact 256-bin sums (FP64); spec rows indexed by the temperature
+    grid position encoded in X[:, 3]."""
     nT = len(spec)
     it = np.rint((X[:, 3] - T_LO) / (T_HI - T_LO) * (nT - 1)).astype(int)
     tau = 10.0 ** np.asarray(X[:, :3], np.float64)
@@ -105,4 +114,6 @@ def exact_targets(X, spec, i0, cs, sig0, w6):
     att = np.exp(-(tau @ shat.T)) * spec[it]
     I = att @ w6
     y = np.log(I / i0[it])
-    return np.log1p(-y)
+    ylin = -np.einsum("ns,njs->nj", tau, moments(spec, i0, cs, sig0, w6)[it])
+    q = np.log(y / ylin)
+    return (q, y) if with_y else q

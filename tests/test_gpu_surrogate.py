@@ -30,10 +30,11 @@ def test_samples_match_exact_quadrature(trainer):
     X, Y = X.cpu().numpy(), Y.cpu().numpy()
     cs, sig0, w6 = _tables()
     want = MO.exact_targets(X, trainer.spec_np, trainer.i0_np, cs, sig0, w6)
-    # float32 storage of t and of the inputs
+    # float32 storage of q and of the inputs
     assert np.allclose(Y, want, rtol=2e-5, atol=2e-5)
     assert X[:, :3].min() >= -6 and X[:, :3].max() <= 3
-    assert Y.min() >= 0
+    # Jensen: the thin limit bounds y from below, so q <= 0
+    assert Y.max() <= 1e-6 and Y.min() > -12
 
 
 def test_gradient_matches_fp64_oracle(trainer):
@@ -62,9 +63,11 @@ def test_gradient_matches_fp64_oracle(trainer):
 
 
 def test_training_reduces_loss(trainer):
-    X, Y = trainer.samples(200_000, seed=7)
-    hist = trainer.train(X, Y, epochs=3, batch=8192, lr=3e-3)
-    assert hist[-1] < 0.3 * hist[0] or hist[-1] < 1e-3
+    X, Y = trainer.samples(1_000_000, seed=7)
+    _, loss0 = trainer.gradient(X[:8192].contiguous(), Y[:8192].contiguous())
+    hist = trainer.train(X, Y, epochs=4, batch=8192, lr=3e-3)
+    assert hist[-1] < 0.1 * loss0, (loss0, hist)
+    assert hist[-1] < hist[0]
 
 
 def test_tensor_core_inference_matches_training_forward(trainer):
