@@ -16,7 +16,7 @@
 // Error control per cell.  Kernel 1 predicts every ray's six contributions
 // c_j with a relative error bound eps (from the validated envelope of the
 // network's error, measured on held-out samples) and a lower bound S_j of
-// each cell's total, sum c_j (1 - eps).  Kernel 2 keeps the predictions of the rays with the smallest
+// each cell's total (each ray's true sum is at least I^ e^-x per node).  Kernel 2 keeps the predictions of the rays with the smallest
 // shares beta = eps max_j c_j / S_j while their sum stays within the cell's
 // budget tol, so that the surrogate's error is at most tol S_j per cell and
 // output; the other rays take the exact FP32 quadrature.  A ray always
@@ -224,9 +224,9 @@ __device__ __forceinline__ RayTask ray_task(const GridDev &g, const float4 *__re
 // Kernel 1 of the surrogate rates: for every ray of blocks [b0, b1) the
 // network's prediction of its six contributions c_j and a relative error
 // bound eps (work planes 0..5 and 6; eps = +inf for a ray that must take
-// the exact quadrature), and per cell a lower bound S_j = sum c_j (1 - eps)
-// of the true total of its surrogate-capable rays (written to rates6,
-// which kernel 2 overwrites).
+// the exact quadrature), and per cell a lower bound S_j of the true total
+// of its surrogate-capable rays (written to rates6, which kernel 2
+// overwrites).
 //
 // Error bound of one ray: at quadrature node i the network's q has the
 // validated error bound dq = env_j(q^) (largest error on held-out samples in
@@ -321,12 +321,15 @@ __global__ void __launch_bounds__(32 * kSurWarps)
       // ---- phase C: predicted contributions and their error bound
       if (tl >= 0) {
         float cj[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float low[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // lower-bound factor of each c_j
         float eps = kInf;
         if (nq > 0) {
           float mj[18];
 #pragma unroll
           for (int k = 0; k < 18; k++) mj[k] = __ldg(emit_m + 18 * (size_t)e + k);
-          float G[6] = {0, 0, 0, 0, 0, 0}, dG[6] = {0, 0, 0, 0, 0, 0};
+          // G: predicted node sum; dG: bound of its error; Gl: lower bound
+          // of the true sum (I >= I^ e^-x at every node)
+          float G[6] = {0, 0, 0, 0, 0, 0}, dG[6] = {0, 0, 0, 0, 0, 0}, Gl[6] = {0, 0, 0, 0, 0, 0};
           for (int i = 0; i < nq; i++) {
             float u, wq;
             gl_node(nq, i, &u, &wq);
@@ -343,11 +346,15 @@ __global__ void __launch_bounds__(32 * kSurWarps)
               const float a = wq * __expf(yh);
               G[j] += a;
               dG[j] = fmaf(a, x * __expf(x), dG[j]);
+              Gl[j] = fmaf(a, __expf(-x), Gl[j]);
             }
           }
           eps = 0.f;
 #pragma unroll
-          for (int j = 0; j < 6; j++) eps = fmaxf(eps, G[j] > 0.f ? dG[j] / G[j] : (dG[j] > 0.f ? kInf : 0.f));
+          for (int j = 0; j < 6; j++) {
+            eps = fmaxf(eps, G[j] > 0.f ? dG[j] / G[j] : (dG[j] > 0.f ? kInf : 0.f));
+            low[j] = G[j] > 0.f ? (Gl[j] / G[j]) * (1.f - kGLErr) : 0.f;
+          }
           // plus the Gauss-Legendre quadrature error of the cell factor
           eps += kGLErr;
 #pragma unroll
@@ -357,12 +364,11 @@ __global__ void __launch_bounds__(32 * kSurWarps)
           }
         }
         // the cell budget is taken from a lower bound of the true total:
-        // c_true >= c (1 - eps)
-        const float lowf = fmaxf(0.f, 1.f - eps);
+        // c_true >= c (Gl / G) (1 - GL error)
 #pragma unroll
         for (int j = 0; j < 6; j++) {
           work[j * nray + r] = cj[j];
-          S.c[wib][lane][j] = cj[j] * lowf;
+          S.c[wib][lane][j] = cj[j] * low[j];
         }
         work[6 * nray + r] = eps;
       }

@@ -216,6 +216,25 @@ def batched(nprob: int = 48, seed: int = 3, edges=(32, 48, 64, 96, 128)):
     return out
 
 
+def ionized(edge: int = 64, nsrc: int = 64, seed: int = 9, sigma_ln: float = 1.0,
+            neutral: float = 1e-4):
+    """A fully ionised volume (H II and He III, as inside a merged ionised
+    region late in reionisation): lognormal density, residual fractions
+    fHI, fHeI, fHeII log-uniform within a factor 10 around `neutral`, so
+    that most rays are optically thin."""
+    rng = np.random.default_rng(seed)
+    dens = lognormal_density(edge, sigma_ln, rng)
+    pos = rng.uniform(0.0, 1.0, (nsrc, 3)).astype(np.float32)
+    rate = _rates_loguniform(rng, nsrc, 1e49, 1e51)
+    n = edge ** 3
+    frac = lambda: (neutral * 10.0 ** rng.uniform(-0.5, 0.5, n)).astype(np.float32)
+    w = _finish(f"ionized{edge}_src{nsrc}", edge, dens, 1.0 - frac(), np.zeros(n), pos, rate, 0.5,
+                f"lognormal sigma_ln={sigma_ln}; H II + He III, neutral fractions ~{neutral}")
+    w.fHeI = frac()
+    w.fHeII = frac()
+    return w
+
+
 def tiny(edge: int = 16, nsrc: int = 4, seed: int = 7, sigma_ln: float = 1.0):
     """Small lognormal problem for unit tests."""
     return _lognormal_ionized(f"tiny{edge}_src{nsrc}", edge, nsrc, sigma_ln, 1e49, 1e51, seed)

@@ -35,7 +35,8 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-CONFIGS = ("largest", "plain", "precision", "learned", "tiny", "plain256", "batched", "batched_small")
+CONFIGS = ("largest", "plain", "precision", "learned", "tiny", "plain256", "batched", "batched_small",
+           "ionized")
 METRIC = "ray-cell crossings/s (march+stitch+rates, 1 B200)"
 # DRAM bytes per ray-cell crossing of k_march_rays<Kahan> measured by ncu on
 # the 256^3 / 16-source case (82.38 GB over 6.030e10 crossings); the
@@ -60,6 +61,9 @@ def make_workload(name: str, rank: int = 0):
     if name == "plain256":
         # profiling case: a field larger than L2 with few rays (~4 GB on the device)
         return W.plain(edge=256, nsrc=16, seed=1 + seed_shift)
+    if name == "ionized":
+        # fully ionised 128^3 (thin rays): where the surrogate can serve rays
+        return W.ionized(128, 256, seed=9 + seed_shift)
     if name == "batched":
         return W.batched(48, seed=3 + seed_shift)
     if name == "batched_small":
