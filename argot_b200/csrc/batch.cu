@@ -51,21 +51,16 @@ template <int kWarps>
 __global__ void __launch_bounds__(32 * kWarps)
     k_batch(const BatchProb *__restrict__ probs, const BatchItem *__restrict__ items, uint32_t nitems,
             uint32_t *__restrict__ next, unsigned long long *__restrict__ crossings, int *__restrict__ err) {
-  __shared__ float4 s_tab[3 * kNu];
+  __shared__ BinPair s_pairs[kBinPairs];
   __shared__ float s_nd[kWarps][32][6];
   __shared__ double s_p[kWarps][32][3];
   __shared__ double s_out[kWarps][32][6];
   __shared__ int s_e[kWarps][32], s_t[kWarps][32];
-  for (int k = threadIdx.x; k < kNu; k += blockDim.x) {
-    s_tab[3 * k + 0] = make_float4(c_tab.cs_l2e[0][k], c_tab.cs_l2e[1][k], c_tab.cs_l2e[2][k], c_tab.cs[0][k]);
-    s_tab[3 * k + 1] = make_float4(c_tab.cs[1][k], c_tab.cs[2][k], c_tab.hw[0][k], c_tab.hw[1][k]);
-    s_tab[3 * k + 2] = make_float4(c_tab.hw[2][k], 0.f, 0.f, 0.f);
-  }
+  load_bin_pairs(s_pairs);
   __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int grp = lane >> 3, j = lane & 7;
   const unsigned gmask = 0xffu << (8 * grp);
-  const float ln2 = 0.69314718055994531f;
   unsigned long long steps_total = 0;
   bool bad = false;
   for (;;) {
@@ -130,23 +125,9 @@ __global__ void __launch_bounds__(32 * kWarps)
           const float N0 = s_nd[wib][q][0], N1 = s_nd[wib][q][1], N2 = s_nd[wib][q][2];
           const float D0 = s_nd[wib][q][3], D1 = s_nd[wib][q][4], D2 = s_nd[wib][q][5];
           const float *sp = specn + (size_t)s_e[wib][q] * kNu;
-          float g0 = 0.f, g1 = 0.f, g2 = 0.f, h0 = 0.f, h1 = 0.f, h2 = 0.f;
-#pragma unroll 4
-          for (int m = 0; m < kNu / 8; m++) {
-            const int k = j + 8 * m;
-            const float4 A = s_tab[3 * k + 0], B = s_tab[3 * k + 1], Cq = s_tab[3 * k + 2];
-            const float tl2 = fmaf(N0, A.x, fmaf(N1, A.y, N2 * A.z));
-            const float dl2 = fmaf(D0, A.x, fmaf(D1, A.y, D2 * A.z));
-            const float ee = ex2_approx(-tl2);
-            const float ed = ex2_approx(-dl2);
-            const float wv = __ldg(sp + k) * ee * phi_pc(dl2 * ln2, ed);
-            g0 = fmaf(A.w, wv, g0);
-            g1 = fmaf(B.x, wv, g1);
-            g2 = fmaf(B.y, wv, g2);
-            h0 = fmaf(B.z, wv, h0);
-            h1 = fmaf(B.w, wv, h1);
-            h2 = fmaf(Cq.x, wv, h2);
-          }
+          float part[6];
+          ray_bins_packed(s_pairs, sp, j, N0, N1, N2, D0, D1, D2, part);
+          float g0 = part[0], g1 = part[1], g2 = part[2], h0 = part[3], h1 = part[4], h2 = part[5];
 #pragma unroll
           for (int o = 1; o < 8; o <<= 1) {
             g0 += __shfl_xor_sync(gmask, g0, o);

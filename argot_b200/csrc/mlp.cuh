@@ -20,10 +20,10 @@
 // Architecture: 4 -> 64 -> 64 -> 64 -> 6, SiLU, BF16 weights and activations
 // with FP32 accumulation.  Every activation (and the normalised input)
 // enters the tensor cores as a BF16 pair hi + lo, the FP32 value split to
-// 16 mantissa bits, so that the output is not limited by the 8-bit BF16
-// rounding of the activations: single-BF16 activations left a floor of
-// ~5e-3 in q, which no training removes.  The weights are single BF16
-// values (the network is trained with them rounded).
+// 16 mantissa bits, so that the 8-bit BF16 rounding of the activations
+// does not add to the error.  The weights are single BF16 values (the
+// network is trained with them rounded); they set the network's error
+// floor, a median |dq| of ~5e-3 after 40 epochs of 2e7 samples.
 #pragma once
 #include <cuda_bf16.h>
 
@@ -53,9 +53,18 @@ __device__ __forceinline__ float bf16_round(float x) {
   return __bfloat162float(__float2bfloat16_rn(x));
 }
 
-// SiLU as the inference kernel evaluates it: z / (1 + e^-z) with the fast
-// exponential and division (relative error a few 1e-7, far below the
-// network's own; the hardware tanh, 2^-11, would set a floor of its own).
-__device__ __forceinline__ float silu_acc(float z) { return __fdividef(z, 1.f + __expf(-z)); }
+// SiLU as the inference kernel evaluates it: z sigmoid(z) with
+// sigmoid(z) = (1 + tanh(z/2)) / 2 and the hardware tanh (one MUFU
+// operation; its 2^-11 error is well below that of the BF16 weights, and
+// the error envelope is measured with these numerics).
+__device__ __forceinline__ float tanh_approx(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float silu_acc(float z) {
+  const float h = 0.5f * z;
+  return fmaf(h, tanh_approx(h), h);
+}
 
 }  // namespace argot

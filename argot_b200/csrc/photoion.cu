@@ -94,7 +94,8 @@ __global__ void __launch_bounds__(32 * kRateWarps)
 // the FP64 per-ray parameters of ray i of the chunk (geometry, columns,
 // prefactors).  Phase B: the warp splits into four groups of eight lanes;
 // a group takes one ray at a time and its lanes share the 256 frequency
-// bins (lane j: bins j, j+8, ...), reading the frequency tables from shared
+// bins (lane j: bins j, j+8, ..., two at a time with the packed f32x2
+// arithmetic, ray_bins_packed), reading the frequency tables from shared
 // memory; three butterfly steps sum the eight partial sums.  Phase C: lane
 // j adds the rays that end in cell j of the block, in ray order.
 constexpr int kF32Warps = 4;
@@ -104,21 +105,16 @@ __global__ void __launch_bounds__(32 * kF32Warps)
                const float *__restrict__ specn, const double *__restrict__ total, uint64_t b0, uint64_t b1,
                const uint64_t *__restrict__ blk_off, uint64_t base, const uint32_t *__restrict__ rays,
                uint64_t nray, const float *__restrict__ tau, float *__restrict__ rates6) {
-  __shared__ float4 s_tab[3 * kNu];
+  __shared__ BinPair s_pairs[kBinPairs];
   __shared__ float s_nd[kF32Warps][32][6];
   __shared__ double s_p[kF32Warps][32][3];
   __shared__ double s_out[kF32Warps][32][6];
   __shared__ int s_e[kF32Warps][32], s_t[kF32Warps][32];
-  for (int k = threadIdx.x; k < kNu; k += blockDim.x) {
-    s_tab[3 * k + 0] = make_float4(c_tab.cs_l2e[0][k], c_tab.cs_l2e[1][k], c_tab.cs_l2e[2][k], c_tab.cs[0][k]);
-    s_tab[3 * k + 1] = make_float4(c_tab.cs[1][k], c_tab.cs[2][k], c_tab.hw[0][k], c_tab.hw[1][k]);
-    s_tab[3 * k + 2] = make_float4(c_tab.hw[2][k], 0.f, 0.f, 0.f);
-  }
+  load_bin_pairs(s_pairs);
   __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int grp = lane >> 3, j = lane & 7;
   const unsigned gmask = 0xffu << (8 * grp);
-  const float ln2 = 0.69314718055994531f;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
@@ -160,23 +156,9 @@ __global__ void __launch_bounds__(32 * kF32Warps)
         const float N0 = s_nd[wib][q][0], N1 = s_nd[wib][q][1], N2 = s_nd[wib][q][2];
         const float D0 = s_nd[wib][q][3], D1 = s_nd[wib][q][4], D2 = s_nd[wib][q][5];
         const float *sp = specn + (size_t)s_e[wib][q] * kNu;
-        float g0 = 0.f, g1 = 0.f, g2 = 0.f, h0 = 0.f, h1 = 0.f, h2 = 0.f;
-#pragma unroll 4
-        for (int m = 0; m < kNu / 8; m++) {
-          const int k = j + 8 * m;
-          const float4 A = s_tab[3 * k + 0], B = s_tab[3 * k + 1], Cq = s_tab[3 * k + 2];
-          const float tl2 = fmaf(N0, A.x, fmaf(N1, A.y, N2 * A.z));
-          const float dl2 = fmaf(D0, A.x, fmaf(D1, A.y, D2 * A.z));
-          const float e = ex2_approx(-tl2);
-          const float ed = ex2_approx(-dl2);
-          const float wv = __ldg(sp + k) * e * phi_pc(dl2 * ln2, ed);
-          g0 = fmaf(A.w, wv, g0);
-          g1 = fmaf(B.x, wv, g1);
-          g2 = fmaf(B.y, wv, g2);
-          h0 = fmaf(B.z, wv, h0);
-          h1 = fmaf(B.w, wv, h1);
-          h2 = fmaf(Cq.x, wv, h2);
-        }
+        float part[6];
+        ray_bins_packed(s_pairs, sp, j, N0, N1, N2, D0, D1, D2, part);
+        float g0 = part[0], g1 = part[1], g2 = part[2], h0 = part[3], h1 = part[4], h2 = part[5];
 #pragma unroll
         for (int o = 1; o < 8; o <<= 1) {
           g0 += __shfl_xor_sync(gmask, g0, o);

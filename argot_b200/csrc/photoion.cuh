@@ -212,4 +212,75 @@ static __device__ __noinline__ void rate_bins_f32(const RayCols &c, const float 
   }
 }
 
+// ---- packed FP32 bin loop: two bins per instruction with the f32x2 FMA
+// and multiply of sm_100.  An 8-lane group integrates one ray; lane j owns
+// the bin pairs (j + 16 i, j + 16 i + 8), i = 0..15 (the bins j + 8 m), and
+// keeps one partial sum per output and pair member.
+struct BinPair {
+  float2 l2e[3];  // sigma_s log2(e) of the two bins
+  float2 cs[3];   // sigma_s
+  float2 hw[3];   // sigma_s ((float) nu - nu_s)^+
+  float2 pad;     // 80 B: the eight lanes of a group hit distinct banks
+};
+constexpr int kBinPairs = kNu / 2;
+
+// Fills the pair table from the constant tables (all threads of the block
+// take part; the caller synchronises).
+__device__ __forceinline__ void load_bin_pairs(BinPair *tab) {
+  for (int p = threadIdx.x; p < kBinPairs; p += blockDim.x) {
+    const int j = p & 7, i = p >> 3;
+    const int k0 = j + 16 * i, k1 = k0 + 8;
+    BinPair b;
+#pragma unroll
+    for (int s = 0; s < 3; s++) {
+      b.l2e[s] = make_float2(c_tab.cs_l2e[s][k0], c_tab.cs_l2e[s][k1]);
+      b.cs[s] = make_float2(c_tab.cs[s][k0], c_tab.cs[s][k1]);
+      b.hw[s] = make_float2(c_tab.hw[s][k0], c_tab.hw[s][k1]);
+    }
+    b.pad = make_float2(0.f, 0.f);
+    tab[p] = b;
+  }
+}
+
+// phi_pc of dl2 = dtau log2(e), with e^-dtau evaluated only where it is
+// used (dtau >= 0.1): same values as phi_pc, one exponential fewer in the
+// thin bins.
+__device__ __forceinline__ float phi_pc_lazy(float dl2) {
+  const float x = dl2 * 0.69314718055994531f;
+  if (x < 0.1f) return phi_pc(x, 0.f);
+  return phi_pc(x, ex2_approx(-dl2));
+}
+
+// The lane's six partial sums (Gamma then heating of HI, HeI, HeII) of one
+// ray with columns N (to the cell) and D (of the cell) in cm^-2; sp: the
+// emitter's normalised spectrum.  The caller adds the eight lanes.
+__device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab, const float *__restrict__ sp,
+                                                int j, float N0, float N1, float N2, float D0, float D1, float D2,
+                                                float (&out)[6]) {
+  const float2 n0 = make_float2(N0, N0), n1 = make_float2(N1, N1), n2 = make_float2(N2, N2);
+  const float2 d0 = make_float2(D0, D0), d1 = make_float2(D1, D1), d2 = make_float2(D2, D2);
+  float2 acc[6];
+#pragma unroll
+  for (int q = 0; q < 6; q++) acc[q] = make_float2(0.f, 0.f);
+#pragma unroll 4
+  for (int i = 0; i < kBinPairs / 8; i++) {
+    const BinPair &b = tab[j + 8 * i];
+    const int k0 = j + 16 * i;
+    const float2 tl = __ffma2_rn(n0, b.l2e[0], __ffma2_rn(n1, b.l2e[1], __fmul2_rn(n2, b.l2e[2])));
+    const float2 dl = __ffma2_rn(d0, b.l2e[0], __ffma2_rn(d1, b.l2e[1], __fmul2_rn(d2, b.l2e[2])));
+    const float2 s = make_float2(__ldg(sp + k0), __ldg(sp + k0 + 8));
+    const float2 e = make_float2(ex2_approx(-tl.x), ex2_approx(-tl.y));
+    const float2 ph = make_float2(phi_pc_lazy(dl.x), phi_pc_lazy(dl.y));
+    const float2 w = __fmul2_rn(__fmul2_rn(s, e), ph);
+    acc[0] = __ffma2_rn(b.cs[0], w, acc[0]);
+    acc[1] = __ffma2_rn(b.cs[1], w, acc[1]);
+    acc[2] = __ffma2_rn(b.cs[2], w, acc[2]);
+    acc[3] = __ffma2_rn(b.hw[0], w, acc[3]);
+    acc[4] = __ffma2_rn(b.hw[1], w, acc[4]);
+    acc[5] = __ffma2_rn(b.hw[2], w, acc[5]);
+  }
+#pragma unroll
+  for (int q = 0; q < 6; q++) out[q] = acc[q].x + acc[q].y;
+}
+
 }  // namespace argot

@@ -68,7 +68,7 @@ struct PredSmem {
 };
 
 struct FinSmem {
-  float4 tab[3 * kNu];
+  BinPair pairs[kBinPairs];
   // per warp
   float Sc[kSurWarps][32][6];                // lower bounds of the cell totals
   unsigned hist[kSurWarps][32][kHistBins];   // budget-share histogram per cell
@@ -233,7 +233,7 @@ __device__ __forceinline__ RayTask ray_task(const GridDev &g, const float4 *__re
 // bins of predicted q, times a safety factor), so with y^ = ylin e^q^,
 // |y - y^| <= |y^| (e^dq - 1) = x and |I - I^| <= I^ (e^x - 1) <= I^ x e^x;
 // the node bounds add up over the nodes.
-__global__ void __launch_bounds__(32 * kSurWarps)
+__global__ void __launch_bounds__(32 * kSurWarps, 4)
     k_sur_predict(GridDev g, const float4 *__restrict__ raw, const float4 *__restrict__ emit_pos,
                   const double *__restrict__ total, const float *__restrict__ emit_logT,
                   const double *__restrict__ emit_i0, const float *__restrict__ emit_m,
@@ -429,16 +429,11 @@ __global__ void __launch_bounds__(32 * kSurWarps)
                  float *__restrict__ rates6, unsigned long long *__restrict__ counters) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   FinSmem &S = *reinterpret_cast<FinSmem *>(smem_raw);
-  for (int k = threadIdx.x; k < kNu; k += blockDim.x) {
-    S.tab[3 * k + 0] = make_float4(c_tab.cs_l2e[0][k], c_tab.cs_l2e[1][k], c_tab.cs_l2e[2][k], c_tab.cs[0][k]);
-    S.tab[3 * k + 1] = make_float4(c_tab.cs[1][k], c_tab.cs[2][k], c_tab.hw[0][k], c_tab.hw[1][k]);
-    S.tab[3 * k + 2] = make_float4(c_tab.hw[2][k], 0.f, 0.f, 0.f);
-  }
+  load_bin_pairs(S.pairs);
   __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int grp = lane >> 3, jj = lane & 7;
   const unsigned gmask = 0xffu << (8 * grp);
-  const float ln2 = 0.69314718055994531f;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
@@ -523,18 +518,9 @@ __global__ void __launch_bounds__(32 * kSurWarps)
           const float N0 = S.nd[wib][qq][0], N1 = S.nd[wib][qq][1], N2 = S.nd[wib][qq][2];
           const float D0 = S.nd[wib][qq][3], D1 = S.nd[wib][qq][4], D2 = S.nd[wib][qq][5];
           const float *sp = specn + (size_t)S.e[wib][qq] * kNu;
-          float g0 = 0.f, g1 = 0.f, g2 = 0.f, h0 = 0.f, h1 = 0.f, h2 = 0.f;
-#pragma unroll 4
-          for (int m = 0; m < kNu / 8; m++) {
-            const int k = jj + 8 * m;
-            const float4 A4 = S.tab[3 * k + 0], B4 = S.tab[3 * k + 1], C4 = S.tab[3 * k + 2];
-            const float tl2 = fmaf(N0, A4.x, fmaf(N1, A4.y, N2 * A4.z));
-            const float dl2 = fmaf(D0, A4.x, fmaf(D1, A4.y, D2 * A4.z));
-            const float ee = ex2_approx(-tl2), ed = ex2_approx(-dl2);
-            const float wv = __ldg(sp + k) * ee * phi_pc(dl2 * ln2, ed);
-            g0 = fmaf(A4.w, wv, g0); g1 = fmaf(B4.x, wv, g1); g2 = fmaf(B4.y, wv, g2);
-            h0 = fmaf(B4.z, wv, h0); h1 = fmaf(B4.w, wv, h1); h2 = fmaf(C4.x, wv, h2);
-          }
+          float part[6];
+          ray_bins_packed(S.pairs, sp, jj, N0, N1, N2, D0, D1, D2, part);
+          float g0 = part[0], g1 = part[1], g2 = part[2], h0 = part[3], h1 = part[4], h2 = part[5];
 #pragma unroll
           for (int o = 1; o < 8; o <<= 1) {
             g0 += __shfl_xor_sync(gmask, g0, o); g1 += __shfl_xor_sync(gmask, g1, o);
