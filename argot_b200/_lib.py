@@ -1,7 +1,8 @@
 """ctypes binding of libargot_b200.so (the C ABI in include/argot_b200.h).
 
-The library is built in-tree (``argot_b200/build.py``).  Loading fails
-loudly when it is missing: there is no CPU fallback for any entry point.
+The library is built in-tree (``argot_b200/build.py``); the environment
+variable ARGOT_B200_LIB may name another build of it.  Loading fails loudly
+when it is missing: there is no CPU fallback for any entry point.
 """
 from __future__ import annotations
 
@@ -127,7 +128,7 @@ def load(path: str | None = None):
     with _lock:
         if _lib is not None:
             return _lib
-        path = path or LIB_PATH
+        path = path or os.environ.get("ARGOT_B200_LIB") or LIB_PATH
         if not os.path.exists(path):
             raise FileNotFoundError(
                 f"{path} is not built; run `python -m argot_b200.build` (no CPU fallback exists)")

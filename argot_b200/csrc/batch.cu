@@ -47,8 +47,13 @@ struct BatchItem {
   uint32_t prob, b0, b1, pad;
 };
 
+// Launch shape: kWarps warps per CTA and at least ARGOT_BATCH_MIN_WARPS / kWarps
+// CTAs resident per SM (which caps the registers per thread).
+#ifndef ARGOT_BATCH_MIN_WARPS
+#define ARGOT_BATCH_MIN_WARPS 16
+#endif
 template <int kWarps>
-__global__ void __launch_bounds__(32 * kWarps)
+__global__ void __launch_bounds__(32 * kWarps, ARGOT_BATCH_MIN_WARPS / kWarps)
     k_batch(const BatchProb *__restrict__ probs, const BatchItem *__restrict__ items, uint32_t nitems,
             uint32_t *__restrict__ next, unsigned long long *__restrict__ crossings, int *__restrict__ err) {
   __shared__ BinPair s_pairs[kBinPairs];

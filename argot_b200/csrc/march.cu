@@ -127,8 +127,13 @@ __global__ void __launch_bounds__(256) k_walk(GridDev g, const DevNode *__restri
 // Consecutive rays of a block come from the same emitter and end in
 // neighbouring cells, so the 32 lanes march nearly parallel paths of nearly
 // equal length and their gathers hit the same cache lines.
+// Launch shape: 256 threads, at least ARGOT_MARCH_MIN_CTAS CTAs resident per
+// SM (which caps the registers per thread).
+#ifndef ARGOT_MARCH_MIN_CTAS
+#define ARGOT_MARCH_MIN_CTAS 4
+#endif
 template <int kPrec>
-__global__ void __launch_bounds__(256, 4) k_march_rays(GridDev g, const float4 *__restrict__ cells,
+__global__ void __launch_bounds__(256, ARGOT_MARCH_MIN_CTAS) k_march_rays(GridDev g, const float4 *__restrict__ cells,
                                                     const float4 *__restrict__ emit_pos, uint64_t b0,
                                                     uint64_t b1, const uint64_t *__restrict__ blk_off,
                                                     uint64_t base, const uint32_t *__restrict__ rays,

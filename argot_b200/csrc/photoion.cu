@@ -98,9 +98,17 @@ __global__ void __launch_bounds__(32 * kRateWarps)
 // arithmetic, ray_bins_packed), reading the frequency tables from shared
 // memory; three butterfly steps sum the eight partial sums.  Phase C: lane
 // j adds the rays that end in cell j of the block, in ray order.
-constexpr int kF32Warps = 4;
+// Launch shape: ARGOT_RATE_WARPS warps per CTA, at least ARGOT_RATE_MIN_CTAS
+// CTAs resident per SM (which caps the registers per thread).
+#ifndef ARGOT_RATE_WARPS
+#define ARGOT_RATE_WARPS 4
+#endif
+#ifndef ARGOT_RATE_MIN_CTAS
+#define ARGOT_RATE_MIN_CTAS 1
+#endif
+constexpr int kF32Warps = ARGOT_RATE_WARPS;
 
-__global__ void __launch_bounds__(32 * kF32Warps)
+__global__ void __launch_bounds__(32 * kF32Warps, ARGOT_RATE_MIN_CTAS)
     k_rate_f32(GridDev g, const float4 *__restrict__ raw, const float4 *__restrict__ emit_pos,
                const float *__restrict__ specn, const double *__restrict__ total, uint64_t b0, uint64_t b1,
                const uint64_t *__restrict__ blk_off, uint64_t base, const uint32_t *__restrict__ rays,
