@@ -99,12 +99,14 @@ __global__ void __launch_bounds__(32 * kRateWarps)
 // memory; three butterfly steps sum the eight partial sums.  Phase C: lane
 // j adds the rays that end in cell j of the block, in ray order.
 // Launch shape: ARGOT_RATE_WARPS warps per CTA, at least ARGOT_RATE_MIN_CTAS
-// CTAs resident per SM (which caps the registers per thread).
+// CTAs resident per SM (which caps the registers per thread).  Measured on
+// B200 (192^3, 1024 sources): 8 warps x 4 CTAs (64 registers) is 19% faster
+// than 4 warps at 72 registers.
 #ifndef ARGOT_RATE_WARPS
-#define ARGOT_RATE_WARPS 4
+#define ARGOT_RATE_WARPS 8
 #endif
 #ifndef ARGOT_RATE_MIN_CTAS
-#define ARGOT_RATE_MIN_CTAS 1
+#define ARGOT_RATE_MIN_CTAS 4
 #endif
 constexpr int kF32Warps = ARGOT_RATE_WARPS;
 

@@ -36,7 +36,7 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 CONFIGS = ("largest", "plain", "precision", "learned", "tiny", "plain256", "batched", "batched_small",
-           "ionized")
+           "ionized", "ionized64")
 METRIC = "ray-cell crossings/s (march+stitch+rates, 1 B200)"
 # DRAM bytes per ray-cell crossing of k_march_rays<Kahan> measured by ncu on
 # the 256^3 / 16-source case (82.38 GB over 6.030e10 crossings); the
@@ -64,6 +64,9 @@ def make_workload(name: str, rank: int = 0):
     if name == "ionized":
         # fully ionised 128^3 (thin rays): where the surrogate can serve rays
         return W.ionized(128, 256, seed=9 + seed_shift)
+    if name == "ionized64":
+        # profiling case for the surrogate kernels (fills the GPU, ~1 GB on the device)
+        return W.ionized(64, 64, seed=9 + seed_shift)
     if name == "batched":
         return W.batched(48, seed=3 + seed_shift)
     if name == "batched_small":
