@@ -24,6 +24,7 @@
 // blackbody in [1e4, 10^5.5] K, when dtau_max > 2, or when a node's
 // log10 tau lies above 3.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <cmath>
 #include <cstring>
@@ -100,13 +101,25 @@ __device__ __forceinline__ void split_bf16x2(float x0, float x1, uint32_t *hi, u
   *lo = pack_bf16x2(x0 - h0, x1 - h1);
 }
 
+// SiLU of two values, z sigmoid(z) = h + h tanh(h) with h = z/2, the two
+// tanh in one packed half-precision MUFU operation (its error, ~2^-11, is
+// that of the single-precision tanh.approx and well below the BF16 weights').
+__device__ __forceinline__ void silu2(float z0, float z1, float *s0, float *s1) {
+  const float h0 = 0.5f * z0, h1 = 0.5f * z1;
+  const __half2 hh = __floats2half2_rn(h0, h1);
+  uint32_t t;
+  asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(*reinterpret_cast<const uint32_t *>(&hh)));
+  const float2 tf = __half22float2(*reinterpret_cast<const __half2 *>(&t));
+  *s0 = fmaf(h0, tf.x, h0);
+  *s1 = fmaf(h1, tf.y, h1);
+}
+
 // SiLU of the 8 accumulator values of two N-tiles, in fragment order.
 __device__ __forceinline__ void silu8(const float (&a)[4], const float (&b)[4], float (&s)[8]) {
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-    s[i] = silu_acc(a[i]);
-    s[4 + i] = silu_acc(b[i]);
-  }
+  silu2(a[0], a[1], &s[0], &s[1]);
+  silu2(a[2], a[3], &s[2], &s[3]);
+  silu2(b[0], b[1], &s[4], &s[5]);
+  silu2(b[2], b[3], &s[6], &s[7]);
 }
 
 // The network on 16 evaluations (rows r0..r0+15 of the warp's list).  The
@@ -233,7 +246,15 @@ __device__ __forceinline__ RayTask ray_task(const GridDev &g, const float4 *__re
 // bins of predicted q, times a safety factor), so with y^ = ylin e^q^,
 // |y - y^| <= |y^| (e^dq - 1) = x and |I - I^| <= I^ (e^x - 1) <= I^ x e^x;
 // the node bounds add up over the nodes.
-__global__ void __launch_bounds__(32 * kSurWarps, 4)
+// Launch shapes: kSurWarps warps per CTA, at least ARGOT_SUR_PREDICT_MIN_CTAS
+// and ARGOT_SUR_FINISH_MIN_CTAS CTAs resident per SM (register caps).
+#ifndef ARGOT_SUR_PREDICT_MIN_CTAS
+#define ARGOT_SUR_PREDICT_MIN_CTAS 4
+#endif
+#ifndef ARGOT_SUR_FINISH_MIN_CTAS
+#define ARGOT_SUR_FINISH_MIN_CTAS 1
+#endif
+__global__ void __launch_bounds__(32 * kSurWarps, ARGOT_SUR_PREDICT_MIN_CTAS)
     k_sur_predict(GridDev g, const float4 *__restrict__ raw, const float4 *__restrict__ emit_pos,
                   const double *__restrict__ total, const float *__restrict__ emit_logT,
                   const double *__restrict__ emit_i0, const float *__restrict__ emit_m,
@@ -328,7 +349,7 @@ __global__ void __launch_bounds__(32 * kSurWarps, 4)
 #pragma unroll
           for (int k = 0; k < 18; k++) mj[k] = __ldg(emit_m + 18 * (size_t)e + k);
           // G: predicted node sum; dG: bound of its error; Gl: lower bound
-          // of the true sum (I >= I^ e^-x at every node)
+          // of the true sum (I >= I^ e^-x >= I^ (1 - x) at every node)
           float G[6] = {0, 0, 0, 0, 0, 0}, dG[6] = {0, 0, 0, 0, 0, 0}, Gl[6] = {0, 0, 0, 0, 0, 0};
           for (int i = 0; i < nq; i++) {
             float u, wq;
@@ -345,8 +366,10 @@ __global__ void __launch_bounds__(32 * kSurWarps, 4)
               const float x = -yh * S.w.env[j][bin];
               const float a = wq * __expf(yh);
               G[j] += a;
-              dG[j] = fmaf(a, x * __expf(x), dG[j]);
-              Gl[j] = fmaf(a, __expf(-x), Gl[j]);
+              // e^x <= 1 + x + x^2 (0 <= x <= 1) and e^-x >= 1 - x
+              const float ex = x <= 1.f ? fmaf(x, x + 1.f, 1.f) : __expf(x);
+              dG[j] = fmaf(a, x * ex, dG[j]);
+              Gl[j] = fmaf(a, fmaxf(0.f, 1.f - x), Gl[j]);
             }
           }
           eps = 0.f;
@@ -421,7 +444,7 @@ __device__ __forceinline__ double beta_edge(int b) { return exp2(0.5 * (double)(
 // of a bin is bounded by its count times its upper edge) keep the
 // network's contributions; every other ray takes the exact FP32
 // quadrature.  Per-cell sums in ray order, as the exact kernels.
-__global__ void __launch_bounds__(32 * kSurWarps)
+__global__ void __launch_bounds__(32 * kSurWarps, ARGOT_SUR_FINISH_MIN_CTAS)
     k_sur_finish(GridDev g, const float4 *__restrict__ raw, const float4 *__restrict__ emit_pos,
                  const float *__restrict__ specn, const double *__restrict__ total, float tol, uint64_t b0,
                  uint64_t b1, const uint64_t *__restrict__ blk_off, uint64_t base, const uint32_t *__restrict__ rays,

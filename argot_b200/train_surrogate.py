@@ -30,18 +30,30 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--out", default=S.WEIGHTS)
+    ap.add_argument("--revalidate", action="store_true",
+                    help="keep the parameters of --out and only re-measure the error envelope "
+                         "with the current inference kernel")
     a = ap.parse_args(argv)
     torch.cuda.set_device(0)
     t0 = time.time()
     tr = S.Trainer("cuda", seed=a.seed)
-    X, Y = tr.samples(a.samples, a.seed)
     Xv, Yv = tr.samples(a.val, a.seed + 1)
-    torch.cuda.synchronize()
-    t_gen = time.time() - t0
-    hist = tr.train(X, Y, a.epochs, a.batch, a.lr, seed=a.seed, log=print)
-    torch.cuda.synchronize()
-    t_train = time.time() - t0 - t_gen
-    params = tr.params.cpu().numpy()
+    prev = {}
+    if a.revalidate:
+        params, _ = S.load(a.out)
+        with np.load(a.out) as f:
+            prev = json.loads(str(f["meta"])) if "meta" in f.files else {}
+        hist = [prev.get("final_loss")]
+        t_gen, t_train = prev.get("gen_s", 0.0), prev.get("train_s", 0.0)
+        a.samples, a.epochs, a.batch, a.lr = (prev.get(k, getattr(a, k)) for k in ("samples", "epochs", "batch", "lr"))
+    else:
+        X, Y = tr.samples(a.samples, a.seed)
+        torch.cuda.synchronize()
+        t_gen = time.time() - t0
+        hist = tr.train(X, Y, a.epochs, a.batch, a.lr, seed=a.seed, log=print)
+        torch.cuda.synchronize()
+        t_train = time.time() - t0 - t_gen
+        params = tr.params.cpu().numpy()
     sur = S.Surrogate(params, np.zeros((6, S.ENV_BINS), np.float32), tol=1.0)
     qv = sur.eval(Xv).cpu().numpy().astype(np.float64)
     qt = Yv.cpu().numpy().astype(np.float64)
@@ -53,7 +65,8 @@ def main(argv=None):
             "final_loss": hist[-1], "gen_s": t_gen, "train_s": t_train,
             "val_max_err_q": dq.max(0).tolist(), "val_median_err_q": np.median(dq, 0).tolist(),
             "val_frac_rel_I_within_5e-4": np.mean(rel <= 5e-4, 0).tolist(),
-            "val_frac_rel_I_within_5e-4_thin": float(np.mean(rel[np.abs(y[:, 0]) < 1, 0] <= 5e-4))}
+            "val_frac_rel_I_within_5e-4_thin": float(np.mean(rel[np.abs(y[:, 0]) < 1, 0] <= 5e-4)),
+            "envelope_revalidated": bool(a.revalidate)}
     S.save(params, env, a.out, {"meta": json.dumps(meta)})
     print(json.dumps(meta))
 
