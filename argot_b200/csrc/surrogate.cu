@@ -24,7 +24,6 @@
 // blackbody in [1e4, 10^5.5] K, when dtau_max > 2, or when a node's
 // log10 tau lies above 3.
 #include <cuda_bf16.h>
-#include <cuda_fp16.h>
 
 #include <cmath>
 #include <cstring>
@@ -101,25 +100,15 @@ __device__ __forceinline__ void split_bf16x2(float x0, float x1, uint32_t *hi, u
   *lo = pack_bf16x2(x0 - h0, x1 - h1);
 }
 
-// SiLU of two values, z sigmoid(z) = h + h tanh(h) with h = z/2, the two
-// tanh in one packed half-precision MUFU operation (its error, ~2^-11, is
-// that of the single-precision tanh.approx and well below the BF16 weights').
-__device__ __forceinline__ void silu2(float z0, float z1, float *s0, float *s1) {
-  const float h0 = 0.5f * z0, h1 = 0.5f * z1;
-  const __half2 hh = __floats2half2_rn(h0, h1);
-  uint32_t t;
-  asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(*reinterpret_cast<const uint32_t *>(&hh)));
-  const float2 tf = __half22float2(*reinterpret_cast<const __half2 *>(&t));
-  *s0 = fmaf(h0, tf.x, h0);
-  *s1 = fmaf(h1, tf.y, h1);
-}
-
-// SiLU of the 8 accumulator values of two N-tiles, in fragment order.
+// SiLU of the 8 accumulator values of two N-tiles, in fragment order (the
+// single-precision hardware tanh: a packed half-precision tanh was measured
+// no faster here and less accurate).
 __device__ __forceinline__ void silu8(const float (&a)[4], const float (&b)[4], float (&s)[8]) {
-  silu2(a[0], a[1], &s[0], &s[1]);
-  silu2(a[2], a[3], &s[2], &s[3]);
-  silu2(b[0], b[1], &s[4], &s[5]);
-  silu2(b[2], b[3], &s[6], &s[7]);
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    s[i] = silu_acc(a[i]);
+    s[4 + i] = silu_acc(b[i]);
+  }
 }
 
 // The network on 16 evaluations (rows r0..r0+15 of the warp's list).  The
