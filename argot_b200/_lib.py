@@ -85,6 +85,7 @@ SIGNATURES = {
     "argot_b200_stitch": (i32, [u64, vp, vp, u64, vp, vp]),
     "argot_b200_photoion_rays": (i32, [GP, vp, vp, u64, u64, vp, u64, vp, u64, vp, i32, vp, vp]),
     "argot_b200_check_device_error": (i32, [vp]),
+    "argot_b200_smooth_rates": (i32, [GP, vp, vp, i32, vp]),
     "argot_b200_tables": (None, [vp, vp]),
     "argot_b200_photon_rate": (None, [i32, f32, f64, vp]),
     "argot_b200_photon_counts": (None, [i32, f32, vp, vp]),

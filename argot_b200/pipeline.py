@@ -198,6 +198,14 @@ class Problem:
             _p(self.blk_off), group.base, _p(rays), group.nray, _p(tau), _p(work), _p(rates6),
             _p(counters), self.sp), "photoion_rays_surrogate")
 
+    def smooth(self, rates6, out=None, isolated: bool = True):
+        """The 27-point smoothing of smooth_photoion_rate.c on the device;
+        returns `out` (a new tensor unless given)."""
+        out = torch.empty_like(rates6) if out is None else out
+        L.check(self.lib.argot_b200_smooth_rates(C.byref(self.grid), _p(rates6), _p(out), int(isolated),
+                                                 self.sp), "smooth_rates")
+        return out
+
     def check_device_error(self):
         L.check(self.lib.argot_b200_check_device_error(self.sp), "device error flag")
 

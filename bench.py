@@ -377,6 +377,17 @@ def run_ours(args):
     t_march = ev[0].elapsed_time(ev[1]) / 1e3
     t_rates = ev[1].elapsed_time(ev[2]) / 1e3
     rate_modes = None if args.no_rate_modes else compare_rate_modes(pb, rays, tau, prec, sur)
+    # the next stage of an iteration: the 27-point smoothing of the rates
+    # (smooth_photoion_rate.c), on the device
+    smoothed = torch.empty_like(rates6)
+    pb.smooth(rates6, smoothed)
+    es0, es1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    es0.record(stream)
+    pb.smooth(rates6, smoothed)
+    es1.record(stream)
+    torch.cuda.synchronize()
+    t_smooth = es0.elapsed_time(es1) / 1e3
+    del smoothed
 
     clocks = ClockSampler(local)
     barrier(ws)
@@ -428,7 +439,8 @@ def run_ours(args):
         "split": {"march_s": t_march, "rates_s": t_rates,
                   "march_crossings_per_s": n_cross / t_march,
                   "rates_gamma_cells_per_s": ncell_mine / t_rates,
-                  "rates_rays_per_s": nray_mine / t_rates},
+                  "rates_rays_per_s": nray_mine / t_rates,
+                  "smooth_s": t_smooth, "smooth_gb_per_s": 2 * 24 * pb.ncell / t_smooth / 1e9},
         "roofline": {"kernel": "k_march_rays", "bound": "hbm", "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": f"{peak_kind} hbm_gbs",

@@ -264,6 +264,15 @@ ARGOT_B200_API int argot_b200_photoion_rays(const argot_b200_grid *g, const void
                              const float *tau_dev, int mode, float *rates6_dev,
                              void *stream);
 
+/* smooth_photoion_rate (src/smooth_photoion_rate.c:27-1588, single rank):
+ * the 27-point smoothing of the six rate planes (layout of rates6 above),
+ * centre weighted by 30, normalised by 1/56, in the reference's order and
+ * precision (bit-identical); at the mesh faces a copy of the nearest cell
+ * (isolated = 1, the reference's default build) or the periodic image
+ * (isolated = 0).  out6 must not alias in6. */
+ARGOT_B200_API int argot_b200_smooth_rates(const argot_b200_grid *g, const float *in6, float *out6, int isolated,
+                                           void *stream);
+
 /* ---- surrogate of the frequency integral (BF16 MLP, tensor cores) ------- */
 /* No counterpart in the reference: its unimplemented Gamma(tau) table
  * (multi_freq_bin.h:11-17, prim_chem/calc_gamma_of_tau.c:5-17) is the

@@ -60,6 +60,7 @@ SOURCES = [
     "prim_chem/cross_section.c",
     "mpi_rank.c",
     "timing.c",
+    "smooth_photoion_rate.c",
 ]
 
 EDGES = (16, 32, 48, 64, 96, 128, 192, 256)
@@ -81,8 +82,8 @@ def patched_run_param(src_text: str, edge: int) -> str:
     return t
 
 
-def ref_lib_path(edge: int, fast_math: bool = False) -> str:
-    tag = "_fm" if fast_math else ""
+def ref_lib_path(edge: int, fast_math: bool = False, isolated: bool = False) -> str:
+    tag = ("_fm" if fast_math else "") + ("_iso" if isolated else "")
     return os.path.join(REF_OUT, f"libargot_ref_n{edge}{tag}.so")
 
 
@@ -95,7 +96,10 @@ def reference_available(ref: str = DEFAULT_REF) -> bool:
 
 
 def build_ref(edge: int, ref: str = DEFAULT_REF, fast_math: bool = False,
-              verbose: bool = False) -> str:
+              verbose: bool = False, isolated: bool = False) -> str:
+    """isolated: the reference Makefile's default `isolated = yes`
+    (-D__ISOLATED__), which only changes mpi_rank.c on this path: a missing
+    neighbour rank instead of the periodic image."""
     src_dir = os.path.join(ref, "src")
     if not os.path.isdir(src_dir):
         raise FileNotFoundError(f"reference sources not found at {src_dir}")
@@ -105,12 +109,14 @@ def build_ref(edge: int, ref: str = DEFAULT_REF, fast_math: bool = False,
         text = patched_run_param(f.read(), edge)
     with open(os.path.join(inc, "run_param.h"), "w") as f:
         f.write(text)
-    out = ref_lib_path(edge, fast_math)
+    out = ref_lib_path(edge, fast_math, isolated)
     cmd = [_cc(), "-O2", "-std=gnu99", "-fopenmp", "-fPIC", "-shared", "-w",
            "-fno-strict-aliasing", "-ffp-contract=off"]
     if fast_math:
         cmd.append("-ffast-math")
     cmd += FLAGS
+    if isolated:
+        cmd.append("-D__ISOLATED__")
     cmd += ["-I" + inc, "-I-", "-I" + os.path.join(HERE, "shim"),
             "-I" + src_dir, "-I" + os.path.join(src_dir, "prim_chem")]
     cmd += [os.path.join(src_dir, s) for s in SOURCES]
@@ -144,6 +150,8 @@ def build_all(edges=EDGES, ref: str = DEFAULT_REF, verbose: bool = False):
         for e in edges:
             built.append(build_ref(e, ref, False, verbose))
         built.append(build_ref(64, ref, True, verbose))
+        built.append(build_ref(16, ref, False, verbose, isolated=True))
+        built.append(build_ref(32, ref, False, verbose, isolated=True))
     return built
 
 

@@ -154,12 +154,12 @@ class RefLib:
 
     _cache: dict = {}
 
-    def __init__(self, edge: int, fast_math: bool = False):
-        path = _build.ref_lib_path(edge, fast_math)
+    def __init__(self, edge: int, fast_math: bool = False, isolated: bool = False):
+        path = _build.ref_lib_path(edge, fast_math, isolated)
         if not os.path.exists(path):
             if not _build.reference_available():
                 raise FileNotFoundError(f"{path} missing and the reference is absent")
-            _build.build_ref(edge, fast_math=fast_math)
+            _build.build_ref(edge, fast_math=fast_math, isolated=isolated)
         # each edge is a distinct library with its own static state
         self.lib = L = C.CDLL(path, mode=C.RTLD_LOCAL)
         self.edge = edge
@@ -183,7 +183,9 @@ class RefLib:
         L.ref_march_segments.argtypes = [C.c_uint64, _f32p, _f32p, C.c_void_p]
         L.ref_accum_segments.argtypes = [C.c_uint64, C.c_uint64, _u64p, _f32p, _f32p]
         L.ref_photoion_rays.argtypes = [C.c_uint64, _i32p, _f32p, _f64p, _f32p, C.c_void_p]
+        L.ref_smooth_rates.argtypes = [_f32p]
         assert L.ref_mesh_edge() == edge
+        self.isolated = isolated
 
     def struct_sizes(self):
         out = np.zeros(10, np.uint64)
@@ -194,6 +196,13 @@ class RefLib:
         out = np.zeros(40, np.uint64)
         self.lib.ref_struct_offsets(out)
         return out[:32]
+
+    def smooth_rates(self, rates6):
+        """smooth_photoion_rate.c on six rate planes (6, ncell) float32;
+        returns the smoothed planes (needs init() first)."""
+        r = np.ascontiguousarray(rates6, np.float32).reshape(6, -1).copy()
+        self.lib.ref_smooth_rates(r)
+        return r
 
     def init(self, lunit, denstonh, theta=0.5, nthreads=1):
         assert self.lib.ref_init(lunit, denstonh, theta, nthreads) == 0

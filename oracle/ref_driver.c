@@ -143,6 +143,8 @@ int ref_init(double lunit, double denstonh, float theta_crit, int nthreads)
   g_run.nmesh_per_loop = NMESH_LOCAL;
   setup_freq_param(&g_run.freq);
   setup_cross_section(g_run.csect, &g_run.freq);
+  g_run.rank_x = g_run.rank_y = g_run.rank_z = 0;
+  g_mpi.photoion_rate_type = ARGOT_SHIM_SIZED_TYPE(sizeof(struct photoion_rate));
   omp_init_nest_lock(&g_omp.omp_lock);
   if (nthreads > 0) omp_set_num_threads(nthreads);
   if (!g_mesh) g_mesh = (struct fluid_mesh *)calloc(NMESH_LOCAL, sizeof(struct fluid_mesh));
@@ -449,4 +451,31 @@ int ref_photoion_rays(uint64_t nray, const int32_t *tgt3, const float *src3,
   free(ray);
   if (wall) *wall = t;
   return 0;
+}
+
+/* The reference's smooth_photoion_rate (27-point stencil, central weight 30,
+ * halo by MPI one-sided puts; on one rank: a copy of the nearest cell when
+ * built with __ISOLATED__, the periodic image otherwise) applied to six rate
+ * planes rates6 (Gamma HI, HeI, HeII, Heat HI, HeI, HeII; ncell floats
+ * each), in place. */
+void ref_smooth_rates(float *rates6)
+{
+  const size_t n = NMESH_LOCAL;
+  for (size_t i = 0; i < n; i++) {
+    g_mesh[i].prev_chem.GammaHI = rates6[0 * n + i];
+    g_mesh[i].prev_chem.GammaHeI = rates6[1 * n + i];
+    g_mesh[i].prev_chem.GammaHeII = rates6[2 * n + i];
+    g_mesh[i].prev_chem.HeatHI = rates6[3 * n + i];
+    g_mesh[i].prev_chem.HeatHeI = rates6[4 * n + i];
+    g_mesh[i].prev_chem.HeatHeII = rates6[5 * n + i];
+  }
+  smooth_photoion_rate(g_mesh, &g_run, &g_mpi);
+  for (size_t i = 0; i < n; i++) {
+    rates6[0 * n + i] = g_mesh[i].prev_chem.GammaHI;
+    rates6[1 * n + i] = g_mesh[i].prev_chem.GammaHeI;
+    rates6[2 * n + i] = g_mesh[i].prev_chem.GammaHeII;
+    rates6[3 * n + i] = g_mesh[i].prev_chem.HeatHI;
+    rates6[4 * n + i] = g_mesh[i].prev_chem.HeatHeI;
+    rates6[5 * n + i] = g_mesh[i].prev_chem.HeatHeII;
+  }
 }

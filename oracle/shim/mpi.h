@@ -2,8 +2,8 @@
  * Single-rank stand-in for the subset of MPI that ARGOT's ray-tracing hot
  * path calls (test infrastructure only: it lets the reference's own
  * calc_optical_depth.c / accum_optical_depth.c / assign_ray_segment.c /
- * calc_photoion_rate.c be compiled and run on one host without an MPI
- * library).
+ * calc_photoion_rate.c / smooth_photoion_rate.c be compiled and run on one
+ * host without an MPI library).
  *
  * Semantics with one rank (rank 0 of a world of size 1):
  *  - MPI_Win_create records the window base and displacement unit, so that
@@ -39,8 +39,13 @@ typedef struct argot_shim_win { char *base; size_t size; int disp_unit; } *MPI_W
 #define MPI_MODE_NOSUCCEED 2
 #define MPI_MODE_NOSTORE 4
 
+/* a derived datatype of n bytes (the reference builds its struct types with
+ * MPI_Type_struct; here the driver sets them to their byte size) */
+#define ARGOT_SHIM_SIZED_TYPE(n) (0x10000 + (int)(n))
+
 static inline size_t argot_shim_type_size(MPI_Datatype t)
 {
+  if (t >= 0x10000) return (size_t)(t - 0x10000);
   switch (t) {
   case MPI_BYTE: return 1;
   case MPI_FLOAT: return 4;
