@@ -211,16 +211,65 @@ class Problem:
 
     # ------------------------------------------------------------- whole pass
     def run(self, precision=L.PRECISION_KAHAN, mode=L.RATE_EXACT_F32, rates6=None,
-            buffers=None, crossings=None, keep_rays=False):
-        """march + rates over every group; returns rates6 (6, ncell)."""
+            buffers=None, crossings=None, keep_rays=False, overlap: int = 0):
+        """march + rates over every group; returns rates6 (6, ncell).
+
+        overlap = P > 1 (one group whose buffers hold all rays): the group
+        is cut into P parts along its blocks; the march of part p+1 runs on
+        one stream while the rates of part p run on another, so the
+        latency-bound march and the MUFU-bound rate kernel share the GPU at
+        each hand-over.  Same arithmetic: the result equals overlap = 0 bit
+        for bit.  The caller's current stream is ordered after all of it."""
         if rates6 is None:
             rates6 = torch.zeros(6 * self.ncell, dtype=torch.float32, device=self.device)
         rays, tau = buffers if buffers is not None else self.alloc_group_buffers()
+        if overlap > 1 and len(self.groups) == 1 and self.groups[0].nray > 0:
+            return self._run_overlapped(precision, mode, rates6, rays, tau, crossings, keep_rays, overlap)
         for g in self.groups:
             if len(self.groups) > 1 or not keep_rays:
                 self.emit(g, rays)
             self.march(g, rays, tau, precision, crossings)
             self.rates(g, rays, tau, rates6, mode)
+        return rates6
+
+    def parts(self, rays, tau, n: int):
+        """The single group cut into about n parts along its blocks, each with
+        its views of the ray buffer (offset base) and of the column buffer
+        (three planes of the part's rays at 3 * base)."""
+        g0 = self.groups[0]
+        sub = self._make_groups(max(1, -(-g0.nray // n)), g0.b0, g0.b1)
+        out = []
+        for g in sub:
+            lo = g.base - g0.base
+            out.append((RayGroup(g.b0, g.b1, g.base, g.nray), rays[lo:lo + max(g.nray, 1)],
+                        tau[3 * lo:3 * (lo + max(g.nray, 1))]))
+        return out
+
+    def _run_overlapped(self, precision, mode, rates6, rays, tau, crossings, keep_rays, n):
+        if getattr(self, "_ovl", None) is None or self._ovl[0] != (n, rays.data_ptr(), tau.data_ptr()):
+            self._ovl = ((n, rays.data_ptr(), tau.data_ptr()), self.parts(rays, tau, n),
+                         torch.cuda.Stream(self.device), torch.cuda.Stream(self.device))
+        _, views, s_march, s_rates = self._ovl
+        main = self.stream
+        s_march.wait_stream(main)
+        s_rates.wait_stream(main)
+        try:
+            self.stream = s_march
+            events = []
+            for g, r, t in views:
+                if not keep_rays:
+                    self.emit(g, r)
+                self.march(g, r, t, precision, crossings)
+                e = torch.cuda.Event()
+                e.record(s_march)
+                events.append(e)
+            self.stream = s_rates
+            for (g, r, t), e in zip(views, events):
+                s_rates.wait_event(e)
+                self.rates(g, r, t, rates6, mode)
+        finally:
+            self.stream = main
+        main.wait_stream(s_rates)
         return rates6
 
     def close(self):

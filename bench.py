@@ -346,12 +346,18 @@ def run_ours(args):
         else:
             pb.rates(g, rays, tau, rates6, mode)
 
+    overlap = args.overlap if (single and mode != L.RATE_SURROGATE) else 0
+
     def step(count=None):
-        for g in pb.groups:
-            if not single:
-                pb.emit(g, rays)
-            pb.march(g, rays, tau, prec, count)
-            rate_pass(g)
+        if overlap > 1:
+            # march of part p+1 on one stream, rates of part p on another
+            pb.run(prec, mode, rates6, (rays, tau), count, keep_rays=True, overlap=overlap)
+        else:
+            for g in pb.groups:
+                if not single:
+                    pb.emit(g, rays)
+                pb.march(g, rays, tau, prec, count)
+                rate_pass(g)
         if sharded:  # the exchange step: every rank's rate slab to every rank
             shard.gather_rates(rates6, cell_ranges)
 
@@ -410,7 +416,8 @@ def run_ours(args):
     hbm, bf16, peak_kind = measured_peaks()
     alg_bytes = 16.0 * n_cross + 36.0 * nray_mine
     achieved = alg_bytes / t_march / 1e9
-    launches_per_step = len(pb.groups) * (2 + (0 if single else 1))
+    launches_per_step = (2 * len(pb.parts(rays, tau, overlap)) if overlap > 1
+                         else len(pb.groups) * (2 + (0 if single else 1)))
 
     # end to end through the C ABI from pinned host buffers (the timed
     # pass's buffers are released first: the e2e pass allocates its own)
@@ -418,6 +425,7 @@ def run_ours(args):
     pb._sur_work = None
     torch.cuda.empty_cache()
     e2e = None if args.no_e2e else run_e2e(wl, dev, prec, mode, steps=max(1, min(args.steps, 3)),
+                                           overlap=args.overlap,
                                            part=part if sharded else None, cell_ranges=cell_ranges)
     if e2e is not None and ws > 1:
         e2e["value"] = allsum(ws, e2e.pop("_crossings"), dev) / allmax(ws, e2e["s_per_step"], dev)
@@ -432,6 +440,7 @@ def run_ours(args):
         "config": {"workload": wl.name, "mesh": f"{wl.edge}^3", "sources": wl.nsrc,
                    "theta": wl.theta, "rays": nray_mine, "crossings": n_cross,
                    "march": args.precision, "rates": args.rate, "ray_groups": len(pb.groups),
+                   "overlap_parts": overlap,
                    "l2": "inputs larger than L2 (13 GB rays, 268 MB field); no flush",
                    "parallelism": (f"{ws} ranks, target x-slabs of one problem, rate slabs all-gathered"
                                    if sharded else f"{ws} independent problems (one per GPU)")},
@@ -472,7 +481,7 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def run_e2e(wl, dev, prec, mode, steps=2, part=None, cell_ranges=None):
+def run_e2e(wl, dev, prec, mode, steps=2, part=None, cell_ranges=None, overlap=0):
     """Same metric through the public C ABI with host buffers: each step
     copies the mesh fields and the source table from pinned host memory,
     builds the tree, generates the rays on the device, marches, computes the
@@ -502,13 +511,16 @@ def run_e2e(wl, dev, prec, mode, steps=2, part=None, cell_ranges=None):
         rays, tau = pb.alloc_group_buffers()
         rates6 = torch.zeros(6 * pb.ncell, dtype=torch.float32, device=dev)
         cnt = torch.zeros(1, dtype=torch.int64, device=dev)
-        for g in pb.groups:
-            pb.emit(g, rays)
-            pb.march(g, rays, tau, prec, cnt)
-            if sur is not None:
-                pb.rates_surrogate(g, rays, tau, rates6, sur)
-            else:
-                pb.rates(g, rays, tau, rates6, mode)
+        if sur is None and overlap > 1 and len(pb.groups) == 1:
+            pb.run(prec, mode, rates6, (rays, tau), cnt, overlap=overlap)
+        else:
+            for g in pb.groups:
+                pb.emit(g, rays)
+                pb.march(g, rays, tau, prec, cnt)
+                if sur is not None:
+                    pb.rates_surrogate(g, rays, tau, rates6, sur)
+                else:
+                    pb.rates(g, rays, tau, rates6, mode)
         if part is not None:
             from argot_b200 import shard
             rates6 = shard.gather_rates(rates6, cell_ranges).view(-1)
@@ -697,6 +709,9 @@ def main(argv=None):
                    help="skip the one-pass comparison of the three rate kernels")
     p.add_argument("--shard", action="store_true",
                    help="N>1: one problem, target slabs sharded over the ranks (strong scaling)")
+    p.add_argument("--overlap", type=int, default=16,
+                   help="cut the ray group into N parts and overlap the march of one part with the "
+                        "rates of the previous one on two streams (0: one stream, kernels in sequence)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
