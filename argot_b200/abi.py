@@ -31,6 +31,12 @@ class FluidMesh(C.Structure):
                                   ("high_mach", C.c_short)]
 
 
+class FluidMeshIO(C.Structure):
+    """struct fluid_mesh_io (fluid.h:118-125): one cell of a mesh dump"""
+    _fields_ = [(n, C.c_float) for n in ("dens", "eneg", "momx", "momy", "momz", "uene", "pot")] + \
+               [("chem", PrimChem)]
+
+
 class RadiationSrc(C.Structure):
     _fields_ = [("type", C.c_int), ("param", C.c_float), ("xpos", C.c_float),
                 ("ypos", C.c_float), ("zpos", C.c_float),

@@ -68,7 +68,8 @@ class Problem:
         self.device = torch.device(device)
         self.grid = unit_box_grid(wl.edge, wl.lunit, wl.denstonh)
         self.ncell = wl.edge ** 3
-        self.spectra = photon_rates(photon_counts, wl.src_type, wl.src_param, wl.src_rate)
+        self.spectra = (np.ascontiguousarray(wl.src_spectra, np.float64) if wl.src_spectra is not None
+                        else photon_rates(photon_counts, wl.src_type, wl.src_param, wl.src_rate))
         with torch.cuda.device(self.device):
             self.stream = torch.cuda.current_stream(self.device)
             if host_fields is not None:

@@ -47,6 +47,9 @@ class Workload:
     lunit: float = 0.0
     denstonh: float = 0.0
     notes: str = ""
+    # optional explicit photon rates per bin (nsrc, 256), e.g. read from a
+    # source file; otherwise formed from type, param and rate
+    src_spectra: np.ndarray | None = None
 
     @property
     def nsrc(self) -> int:

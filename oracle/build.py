@@ -61,6 +61,9 @@ SOURCES = [
     "mpi_rank.c",
     "timing.c",
     "smooth_photoion_rate.c",
+    "output_data.c",
+    "input_data.c",
+    "make_directory.c",
 ]
 
 EDGES = (16, 32, 48, 64, 96, 128, 192, 256)

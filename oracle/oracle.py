@@ -184,6 +184,10 @@ class RefLib:
         L.ref_accum_segments.argtypes = [C.c_uint64, C.c_uint64, _u64p, _f32p, _f32p]
         L.ref_photoion_rays.argtypes = [C.c_uint64, _i32p, _f32p, _f64p, _f32p, C.c_void_p]
         L.ref_smooth_rates.argtypes = [_f32p]
+        L.ref_write_files.argtypes = [C.c_char_p, C.c_char_p]
+        L.ref_read_files.argtypes = [C.c_char_p, C.c_char_p, _f32p, _f32p, _f32p, _f32p, _i32p, _f32p,
+                                     _f32p, _f64p, C.c_int64]
+        L.ref_read_files.restype = C.c_int64
         assert L.ref_mesh_edge() == edge
         self.isolated = isolated
 
@@ -196,6 +200,24 @@ class RefLib:
         out = np.zeros(40, np.uint64)
         self.lib.ref_struct_offsets(out)
         return out[:32]
+
+    def write_files(self, mesh_file: str, src_prefix: str):
+        """The reference's output_mesh_single / output_src on the loaded
+        mesh and sources."""
+        self.lib.ref_write_files(mesh_file.encode(), src_prefix.encode())
+
+    def read_files(self, mesh_file: str, src_file: str, max_src: int = 1 << 16):
+        """The reference's input_mesh_single / input_src_file: (dens, fHI,
+        fHeI, fHeII), (type, param, xyz, photon rates)."""
+        n = self.edge ** 3
+        f = [np.zeros(n, np.float32) for _ in range(4)]
+        typ = np.zeros(max_src, np.int32)
+        par = np.zeros(max_src, np.float32)
+        xyz = np.zeros((max_src, 3), np.float32)
+        spec = np.zeros((max_src, NGRID_NU), np.float64)
+        k = self.lib.ref_read_files(mesh_file.encode(), src_file.encode(), *f, typ, par, xyz, spec, max_src)
+        assert k >= 0
+        return f, (typ[:k], par[:k], xyz[:k], spec[:k])
 
     def smooth_rates(self, rates6):
         """smooth_photoion_rate.c on six rate planes (6, ncell) float32;

@@ -479,3 +479,48 @@ void ref_smooth_rates(float *rates6)
     rates6[5 * n + i] = g_mesh[i].prev_chem.HeatHeII;
   }
 }
+
+/* The reference's own writers on the loaded mesh and sources:
+ * output_mesh_single (output_data.c:14-44) to mesh_file and output_src
+ * (output_data.c:59-73) to <src_prefix>_src.dat. */
+void ref_write_files(const char *mesh_file, const char *src_prefix)
+{
+  output_mesh_single(g_mesh, &g_run, (char *)mesh_file);
+  output_src(g_src, &g_run, (char *)src_prefix);
+}
+
+/* The reference's own readers (input_data.c:112-150, 196-223) into scratch
+ * state: the mesh's dens, fHI, fHeI, fHeII and the sources' type, param,
+ * position and photon rates (up to max_src).  Returns nsrc, or -1 when the
+ * file holds more than max_src.  The mesh header must match this build
+ * (the reader exits otherwise). */
+int64_t ref_read_files(const char *mesh_file, const char *src_file, float *dens, float *fHI, float *fHeI,
+                       float *fHeII, int *type, float *param, float *xyz, double *spectra, int64_t max_src)
+{
+  static struct run_param tmp_run;
+  struct fluid_mesh *m = (struct fluid_mesh *)calloc(NMESH_LOCAL, sizeof(struct fluid_mesh));
+  if (!m) return -1;
+  input_mesh_single(m, &tmp_run, (char *)mesh_file);
+  for (size_t i = 0; i < NMESH_LOCAL; i++) {
+    dens[i] = m[i].dens;
+    fHI[i] = m[i].chem.fHI;
+    fHeI[i] = m[i].chem.fHeI;
+    fHeII[i] = m[i].chem.fHeII;
+  }
+  free(m);
+  struct radiation_src *s = (struct radiation_src *)calloc(NSOURCE_MAX, sizeof(struct radiation_src));
+  if (!s) return -1;
+  input_src_file(s, &tmp_run, (char *)src_file);
+  int64_t n = (int64_t)tmp_run.nsrc;
+  if (n > max_src) { free(s); return -1; }
+  for (int64_t i = 0; i < n; i++) {
+    type[i] = s[i].type;
+    param[i] = s[i].param;
+    xyz[3 * i + 0] = s[i].xpos;
+    xyz[3 * i + 1] = s[i].ypos;
+    xyz[3 * i + 2] = s[i].zpos;
+    memcpy(spectra + i * NGRID_NU, s[i].photon_rate, sizeof(double) * NGRID_NU);
+  }
+  free(s);
+  return n;
+}
