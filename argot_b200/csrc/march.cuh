@@ -161,21 +161,29 @@ static __device__ __forceinline__ Tau3 march_kahan(const GridDev &g, const float
   float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
   const int cap = cx + cy + cz;  // every finite step crosses at least one face
   int it = 0, lastmask = 0;
+  // blocks of 16 steps (unrolled; the Kahan fold and the step bound are
+  // checked once per block, so only "faces left" is tested per step)
   while ((cx | cy | cz) && it < cap) {
-    const float r = fminf(rx, fminf(ry, rz));
-    const bool hx = rx == r, hy = ry == r, hz = rz == r;
-    idx += (hx ? dsx : 0) + (hy ? dsy : 0) + (hz ? dsz : 0);
-    const float4 nn = __ldg(cells + idx);
-    p0 = fmaf(r, n.x, p0);
-    p1 = fmaf(r, n.y, p1);
-    p2 = fmaf(r, n.z, p2);
-    cx -= hx; cy -= hy; cz -= hz;
-    rx = hx ? (cx ? tdx : kInf) : rx - r;
-    ry = hy ? (cy ? tdy : kInf) : ry - r;
-    rz = hz ? (cz ? tdz : kInf) : rz - r;
-    lastmask = (hx ? 1 : 0) | (hy ? 2 : 0) | (hz ? 4 : 0);
-    n = nn;
-    if ((++it & 15) == 0) {
+    int k = 0;
+#pragma unroll
+    for (; k < 16; k++) {
+      if (!(cx | cy | cz)) break;
+      const float r = fminf(rx, fminf(ry, rz));
+      const bool hx = rx == r, hy = ry == r, hz = rz == r;
+      idx += (hx ? dsx : 0) + (hy ? dsy : 0) + (hz ? dsz : 0);
+      const float4 nn = __ldg(cells + idx);
+      p0 = fmaf(r, n.x, p0);
+      p1 = fmaf(r, n.y, p1);
+      p2 = fmaf(r, n.z, p2);
+      cx -= hx; cy -= hy; cz -= hz;
+      rx = hx ? (cx ? tdx : kInf) : rx - r;
+      ry = hy ? (cy ? tdy : kInf) : ry - r;
+      rz = hz ? (cz ? tdz : kInf) : rz - r;
+      lastmask = (hx ? 1 : 0) | (hy ? 2 : 0) | (hz ? 4 : 0);
+      n = nn;
+    }
+    it += k;
+    if (k == 16) {
       kahan_add(s0, c0, p0);
       kahan_add(s1, c1, p1);
       kahan_add(s2, c2, p2);
