@@ -128,8 +128,7 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float v) {
 // cell is issued before the current one is accumulated.  Chords are summed
 // with FMA into per-species partial sums that are folded into Kahan sums
 // every 16 steps (compensated summation over blocks of 16 terms).  The last
-// chord runs from the end cell's entry face -- on the crossed axis with the
-// largest |u| -- to the end point.
+// chord runs from the end cell's entry face to the end point.
 static __device__ __forceinline__ Tau3 march_kahan(const GridDev &g, const float4 *__restrict__ cells,
                                                    float xs, float ys, float zs, float xe, float ye,
                                                    float ze, int *steps, bool *bad) {
@@ -160,7 +159,8 @@ static __device__ __forceinline__ Tau3 march_kahan(const GridDev &g, const float
   float p0 = 0.f, p1 = 0.f, p2 = 0.f;
   float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
   const int cap = cx + cy + cz;  // every finite step crosses at least one face
-  int it = 0, lastmask = 0;
+  const bool crx = cx != 0, cry = cy != 0, crz = cz != 0;  // axes with faces to cross
+  int it = 0;
   // blocks of 16 steps (unrolled; the Kahan fold and the step bound are
   // checked once per block, so only "faces left" is tested per step)
   while ((cx | cy | cz) && it < cap) {
@@ -179,7 +179,6 @@ static __device__ __forceinline__ Tau3 march_kahan(const GridDev &g, const float
       rx = hx ? (cx ? tdx : kInf) : rx - r;
       ry = hy ? (cy ? tdy : kInf) : ry - r;
       rz = hz ? (cz ? tdz : kInf) : rz - r;
-      lastmask = (hx ? 1 : 0) | (hy ? 2 : 0) | (hz ? 4 : 0);
       n = nn;
     }
     it += k;
@@ -191,20 +190,15 @@ static __device__ __forceinline__ Tau3 march_kahan(const GridDev &g, const float
     }
   }
   if (cx | cy | cz) *bad = true;  // only non-finite input leaves faces uncrossed
+  // the ray enters the end cell at its latest face crossing, so the last
+  // chord is the shortest distance from an axis's entry face of the end
+  // cell to the end point, over the axes that had faces to cross
   float depth = len;
-  if (lastmask) {
-    // among the axes crossed last, the one with the largest |u|
-    int a = -1;
-    float best = -1.f;
-    if ((lastmask & 1) && ax > best) { best = ax; a = 0; }
-    if ((lastmask & 2) && ay > best) { best = ay; a = 1; }
-    if ((lastmask & 4) && az > best) { best = az; a = 2; }
-    if (a == 0)
-      depth = fabsf((xe - g.xminl) - g.dx * (float)(ixe + (stx < 0))) * iax;
-    else if (a == 1)
-      depth = fabsf((ye - g.yminl) - g.dy * (float)(iye + (sty < 0))) * iay;
-    else
-      depth = fabsf((ze - g.zminl) - g.dz * (float)(ize + (stz < 0))) * iaz;
+  if (crx | cry | crz) {
+    depth = kInf;
+    if (crx) depth = fminf(depth, fabsf((xe - g.xminl) - g.dx * (float)(ixe + (stx < 0))) * iax);
+    if (cry) depth = fminf(depth, fabsf((ye - g.yminl) - g.dy * (float)(iye + (sty < 0))) * iay);
+    if (crz) depth = fminf(depth, fabsf((ze - g.zminl) - g.dz * (float)(ize + (stz < 0))) * iaz);
   }
   p0 = fmaf(depth, n.x, p0);
   p1 = fmaf(depth, n.y, p1);
