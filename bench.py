@@ -39,10 +39,10 @@ CONFIGS = ("largest", "plain", "precision", "learned", "tiny", "plain256", "batc
            "ionized", "ionized64")
 METRIC = "ray-cell crossings/s (march+stitch+rates, 1 B200)"
 # DRAM bytes per ray-cell crossing of k_march_rays<Kahan> measured by ncu on
-# the 256^3 / 16-source case (1.008 TB/s over a 149.1 ms launch = 150.4 GB
+# the 256^3 / 16-source case (1.0045 TB/s over a 128.5 ms launch = 129.1 GB
 # for 6.030e10 crossings); the workloads here are too large to capture, so
 # `traffic` scales this figure.
-MARCH_DRAM_BYTES_PER_CROSSING = 2.494
+MARCH_DRAM_BYTES_PER_CROSSING = 2.141
 UNIT = "crossings/s"
 
 
@@ -455,7 +455,7 @@ def run_ours(args):
                      "peak_kind": f"{peak_kind} hbm_gbs",
                      "traffic": MARCH_DRAM_BYTES_PER_CROSSING * n_cross,
                      "traffic_source": "ncu DRAM bytes per crossing on 256^3 / 16 sources "
-                                       "(2.494 B), scaled by this launch's crossings",
+                                       "(2.141 B), scaled by this launch's crossings",
                      "algorithmic_bytes": alg_bytes,
                      "bytes_model": "16 B per crossing + 36 B per ray"},
         "clocks": clk,
