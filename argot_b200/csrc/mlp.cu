@@ -378,7 +378,7 @@ int argot_b200_mlp_forward(const float *params, const float *X, int n, float *O,
   return 0;
 }
 
-// One training step on the batch (X: nb x 4, Y: nb x 6 targets t_j):
+// One training step on the batch (X: nb x 4, Y: nb x 6 targets q_j):
 // forward, backward, deterministic gradient reduction, Adam (lr > 0) or
 // gradient only (lr == 0; grad_out receives the gradient if non-NULL).
 // m, v: Adam moments (kMlpParams each); step: 1-based Adam step;

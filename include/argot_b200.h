@@ -249,7 +249,11 @@ ARGOT_B200_API int argot_b200_stitch(uint64_t nseg, const uint64_t *ray_indx_dev
 
 #define ARGOT_B200_RATE_EXACT_F64 0   /* reference algorithm in FP64        */
 #define ARGOT_B200_RATE_EXACT_F32 1   /* FP32, FP64 only for small-dtau phi */
-#define ARGOT_B200_RATE_SURROGATE 2   /* BF16 MLP with exact fallback       */
+#define ARGOT_B200_RATE_SURROGATE 2   /* BF16 MLP with exact fallback: needs
+                                         its weights and workspace, so it runs
+                                         through argot_b200_photoion_rays_surrogate;
+                                         argot_b200_photoion_rays returns
+                                         ARGOT_B200_ENOTSUP for it */
 
 /* Per-cell rates for the target cells of blocks [b0, b1) from their rays'
  * columns.  rates6_dev: 6 planes of ncell floats (Gamma HI, HeI, HeII,
