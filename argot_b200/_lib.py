@@ -50,7 +50,7 @@ class BatchProblem(C.Structure):
 class BatchConfig(C.Structure):
     """argot_b200_batch_config"""
     _fields_ = [("warps_per_cta", C.c_int), ("ctas_per_sm", C.c_int), ("blocks_per_item", C.c_int),
-                ("order", C.c_int)]
+                ("order", C.c_int), ("mode", C.c_int), ("parts", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -57,8 +57,11 @@ class Batch:
         L.check(self.lib.argot_b200_batch_get_config(self.handle, C.byref(c)), "batch_get_config")
         return c.as_dict()
 
-    def configure(self, warps_per_cta=8, ctas_per_sm=0, blocks_per_item=4, order=0):
-        c = L.BatchConfig(warps_per_cta, ctas_per_sm, blocks_per_item, order)
+    def configure(self, warps_per_cta=8, ctas_per_sm=0, blocks_per_item=4, order=0, mode=0, parts=8):
+        """mode 0: fused march + rates in one persistent kernel; 1: split into
+        a persistent march kernel and a persistent rate kernel overlapped
+        over `parts` parts of the tile list."""
+        c = L.BatchConfig(warps_per_cta, ctas_per_sm, blocks_per_item, order, mode, parts)
         L.check(self.lib.argot_b200_batch_configure(self.handle, C.byref(c)), "batch_configure")
 
     def tune(self, reps: int = 1):

@@ -13,8 +13,15 @@
 //
 // Tiles are queued largest first (estimated cost: rays x (mesh edge + a
 // constant for the quadrature)), so the long tiles of the big meshes start
-// early and the short ones fill the tail.  The tile length, warps per CTA
-// and CTAs per SM are chosen by argot_b200_batch_tune, which times
+// early and the short ones fill the tail.
+//
+// Split mode runs the same tiles through two persistent kernels instead --
+// the march (writing the columns of every ray to HBM) and the rates --
+// each with its own launch shape, the tile list cut into parts so that
+// the rates of one part overlap the march of the next on a second stream.
+// The arithmetic is again that of the single-problem kernels.  The mode,
+// the tile length, the fused kernel's warps per CTA and CTAs per SM and the
+// number of parts are chosen by argot_b200_batch_tune, which times
 // candidate configurations on the batch itself.
 #include <algorithm>
 #include <cmath>
@@ -41,6 +48,7 @@ struct BatchProb {
   const uint32_t *rays;  // every ray of the problem, base 0
   float *rates6;
   uint64_t nray;
+  float *tau;  // split mode: three column planes of nray (batch-owned)
 };
 
 struct BatchItem {
@@ -176,6 +184,86 @@ __global__ void __launch_bounds__(32 * kWarps, ARGOT_BATCH_MIN_WARPS / kWarps)
   if (bad) atomicExch(err, 1);
 }
 
+// ---- split mode: the march and the rates as two persistent kernels over
+// the same tiles, their columns through HBM, so that each runs with its own
+// launch shape; a part of the tile list is integrated while the next part
+// is marched (two streams, one graph).
+
+// Launch shapes of the split kernels (as the single-problem kernels).
+#ifndef ARGOT_SPLIT_MARCH_MIN_CTAS
+#define ARGOT_SPLIT_MARCH_MIN_CTAS 6
+#endif
+#ifndef ARGOT_SPLIT_RATE_MIN_CTAS
+#define ARGOT_SPLIT_RATE_MIN_CTAS 4
+#endif
+constexpr int kSplitRateWarps = 8;
+
+__global__ void __launch_bounds__(256, ARGOT_SPLIT_MARCH_MIN_CTAS)
+    k_batch_march(const BatchProb *__restrict__ probs, const BatchItem *__restrict__ items, uint32_t i0,
+                  uint32_t i1, uint32_t *__restrict__ next, unsigned long long *__restrict__ crossings,
+                  int *__restrict__ err) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long steps_total = 0;
+  bool bad = false;
+  for (;;) {
+    uint32_t it = 0;
+    if (lane == 0) it = i0 + atomicAdd(next, 1u);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it >= i1) break;
+    const BatchItem wi = items[it];
+    const BatchProb &P = probs[wi.prob];
+    const GridDev g = P.g;
+    for (uint64_t b = wi.b0; b < wi.b1; b++) {
+      const uint64_t r0 = P.blk_off[b], r1 = P.blk_off[b + 1];
+      int bix, biy, biz;
+      block_cell(g, b, 0, &bix, &biy, &biz);
+      for (uint64_t r = r0 + lane; r < r1; r += 32) {
+        const uint32_t w = __ldg(P.rays + r);
+        const int l = (int)(w & 31u);
+        const float xe = cell_centre(g.xmin, g.ix0 + bix + (l >> 4), g.dx);
+        const float ye = cell_centre(g.ymin, g.iy0 + biy + ((l >> 2) & 3), g.dy);
+        const float ze = cell_centre(g.zmin, g.iz0 + biz + (l & 3), g.dz);
+        const float4 ep = __ldg(P.emit_pos + (w >> 5));
+        float xs, ys, zs;
+        ray_start(g, ep.x, ep.y, ep.z, xe, ye, ze, &xs, &ys, &zs);
+        int steps = 0;
+        const Tau3 t = march_kahan(g, P.cells, xs, ys, zs, xe, ye, ze, &steps, &bad);
+        P.tau[r] = t.hi;
+        P.tau[P.nray + r] = t.hei;
+        P.tau[2 * P.nray + r] = t.heii;
+        steps_total += (unsigned long long)steps;
+      }
+    }
+  }
+  if (crossings) {
+    for (int o = 16; o; o >>= 1) steps_total += __shfl_xor_sync(0xffffffffu, steps_total, o);
+    if (lane == 0 && steps_total) atomicAdd(crossings, steps_total);
+  }
+  if (bad) atomicExch(err, 1);
+}
+
+__global__ void __launch_bounds__(32 * kSplitRateWarps, ARGOT_SPLIT_RATE_MIN_CTAS)
+    k_batch_rates(const BatchProb *__restrict__ probs, const BatchItem *__restrict__ items, uint32_t i0,
+                  uint32_t i1, uint32_t *__restrict__ next) {
+  __shared__ BinPair s_pairs[kBinPairs];
+  __shared__ RateWarpSmem s_w[kSplitRateWarps];
+  load_bin_pairs(s_pairs);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  for (;;) {
+    uint32_t it = 0;
+    if (lane == 0) it = i0 + atomicAdd(next, 1u);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it >= i1) break;
+    const BatchItem wi = items[it];
+    const BatchProb &P = probs[wi.prob];
+    const GridDev g = P.g;
+    for (uint64_t b = wi.b0; b < wi.b1; b++)
+      rate_block_f32(g, P.raw, P.emit_pos, P.specn, P.total, s_pairs, b, P.blk_off[b], P.blk_off[b + 1], P.rays,
+                     P.nray, P.tau, P.rates6, s_w[wib], lane);
+  }
+}
+
 }  // namespace argot
 
 using namespace argot;
@@ -191,11 +279,19 @@ struct argot_b200_batch {
   uint32_t nitems = 0;
   uint32_t *next_dev = nullptr;
   int *err = nullptr;
-  argot_b200_batch_config cfg{8, 0, 4, 0};
+  argot_b200_batch_config cfg{8, 0, 4, 0, 0, 8};
   int grid = 0;
   cudaStream_t cap = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // split mode
+  float *tau = nullptr;             // column planes of every problem
+  uint64_t total_rays = 0;
+  cudaStream_t side = nullptr;      // the rates' stream
+  cudaStream_t side_cap = nullptr;  // the rates' stream while capturing
+  std::vector<cudaEvent_t> ev;      // fork, one per part, join
+  uint32_t *counters = nullptr;     // two per part
+  int grid_march = 0, grid_rates = 0;
 };
 
 namespace {
@@ -214,9 +310,45 @@ int max_ctas_per_sm(int warps) {
   return e == cudaSuccess ? n : 0;
 }
 
+constexpr int kMaxParts = 64;
+
 bool config_valid(const argot_b200_batch_config &c) {
   return (c.warps_per_cta == 4 || c.warps_per_cta == 8) && c.ctas_per_sm >= 0 && c.ctas_per_sm <= 16 &&
-         c.blocks_per_item >= 1 && c.blocks_per_item <= 4096 && (c.order == 0 || c.order == 1);
+         c.blocks_per_item >= 1 && c.blocks_per_item <= 4096 && (c.order == 0 || c.order == 1) &&
+         (c.mode == 0 || c.mode == 1) && c.parts >= 1 && c.parts <= kMaxParts;
+}
+
+// The split mode's buffers (columns of every ray, counters, second stream
+// and events), made on first use.
+int ensure_split(argot_b200_batch *b) {
+  if (b->tau) return 0;
+  if (b->total_rays) {
+    if (cudaMalloc(&b->tau, sizeof(float) * 3 * b->total_rays) != cudaSuccess) {
+      cudaGetLastError();
+      b->tau = nullptr;
+      return ARGOT_B200_ENOMEM;
+    }
+  } else {
+    ARGOT_CUDA_TRY(cudaMalloc(&b->tau, 16));
+  }
+  ARGOT_CUDA_TRY(cudaMalloc(&b->counters, sizeof(uint32_t) * 2 * kMaxParts));
+  ARGOT_CUDA_TRY(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
+  ARGOT_CUDA_TRY(cudaStreamCreateWithFlags(&b->side_cap, cudaStreamNonBlocking));
+  b->ev.resize(kMaxParts + 2);
+  for (auto &e : b->ev) ARGOT_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  uint64_t off = 0;
+  for (auto &q : b->probs) {
+    q.tau = b->tau + 3 * off;
+    off += q.nray;
+  }
+  ARGOT_CUDA_TRY(cudaMemcpy(b->probs_dev, b->probs.data(), sizeof(BatchProb) * b->probs.size(),
+                            cudaMemcpyHostToDevice));
+  int n = 0;
+  ARGOT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_march, 256, 0));
+  b->grid_march = b->sms * (n > 0 ? n : 1);
+  ARGOT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_rates, 32 * kSplitRateWarps, 0));
+  b->grid_rates = b->sms * (n > 0 ? n : 1);
+  return 0;
 }
 
 // Work list of the configuration: tiles of blocks_per_item consecutive
@@ -265,7 +397,37 @@ int build_items(argot_b200_batch *b) {
   return 0;
 }
 
-int launch(argot_b200_batch *b, unsigned long long *crossings, cudaStream_t st) {
+// Split mode: the tile list cut into parts; part p is marched on `st`,
+// then integrated on the side stream once its march is done, while `st`
+// marches part p + 1.  The side stream joins `st` at the end.
+int launch_split(argot_b200_batch *b, unsigned long long *crossings, cudaStream_t st, cudaStream_t side) {
+  const int parts = b->cfg.parts;
+  ARGOT_CUDA_TRY(cudaMemsetAsync(b->counters, 0, sizeof(uint32_t) * 2 * parts, st));
+  ARGOT_CUDA_TRY(cudaEventRecord(b->ev[0], st));
+  ARGOT_CUDA_TRY(cudaStreamWaitEvent(side, b->ev[0], 0));
+  for (int p = 0; p < parts; p++) {
+    const uint32_t i0 = (uint32_t)((uint64_t)b->nitems * p / parts);
+    const uint32_t i1 = (uint32_t)((uint64_t)b->nitems * (p + 1) / parts);
+    k_batch_march<<<b->grid_march, 256, 0, st>>>(b->probs_dev, b->items_dev, i0, i1, b->counters + 2 * p,
+                                                  crossings, b->err);
+    ARGOT_CUDA_TRY(cudaGetLastError());
+    ARGOT_CUDA_TRY(cudaEventRecord(b->ev[1 + p], st));
+    ARGOT_CUDA_TRY(cudaStreamWaitEvent(side, b->ev[1 + p], 0));
+    k_batch_rates<<<b->grid_rates, 32 * kSplitRateWarps, 0, side>>>(b->probs_dev, b->items_dev, i0, i1,
+                                                                      b->counters + 2 * p + 1);
+    ARGOT_CUDA_TRY(cudaGetLastError());
+  }
+  ARGOT_CUDA_TRY(cudaEventRecord(b->ev[1 + parts], side));
+  ARGOT_CUDA_TRY(cudaStreamWaitEvent(st, b->ev[1 + parts], 0));
+  return 0;
+}
+
+int launch(argot_b200_batch *b, unsigned long long *crossings, cudaStream_t st, bool capturing = false) {
+  if (b->cfg.mode == 1) {
+    int rc = ensure_split(b);
+    if (rc) return rc;
+    return launch_split(b, crossings, st, capturing ? b->side_cap : b->side);
+  }
   ARGOT_CUDA_TRY(cudaMemsetAsync(b->next_dev, 0, sizeof(uint32_t), st));
   if (b->cfg.warps_per_cta == 4)
     k_batch<4><<<b->grid, 128, 0, st>>>(b->probs_dev, b->items_dev, b->nitems, b->next_dev, crossings, b->err);
@@ -319,6 +481,8 @@ int argot_b200_batch_create(const argot_b200_batch_problem *p, int n, argot_b200
     q.rays = p[i].rays_dev;
     q.rates6 = p[i].rates6_dev;
     q.nray = p[i].blk_offsets_host[nb];
+    q.tau = nullptr;
+    b->total_rays += q.nray;
     b->probs.push_back(q);
     b->blk_off.emplace_back(p[i].blk_offsets_host, p[i].blk_offsets_host + nb + 1);
   }
@@ -338,6 +502,11 @@ void argot_b200_batch_free(argot_b200_batch *b) {
   if (!b) return;
   drop_graph(b);
   if (b->cap) cudaStreamDestroy(b->cap);
+  if (b->side) cudaStreamDestroy(b->side);
+  if (b->side_cap) cudaStreamDestroy(b->side_cap);
+  for (auto e : b->ev) cudaEventDestroy(e);
+  cudaFree(b->tau);
+  cudaFree(b->counters);
   cudaFree(b->probs_dev);
   cudaFree(b->items_dev);
   cudaFree(b->next_dev);
@@ -371,8 +540,12 @@ int argot_b200_batch_run(argot_b200_batch *b, unsigned long long *crossings_dev,
 int argot_b200_batch_graph_launch(argot_b200_batch *b, void *stream) {
   if (!b) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
   if (!b->exec) {
+    if (b->cfg.mode == 1) {
+      const int r = ensure_split(b);  // allocates: must precede the capture
+      if (r) { set_status(r); return r; }
+    }
     ARGOT_CUDA_TRY(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
-    const int rc = launch(b, nullptr, b->cap);
+    const int rc = launch(b, nullptr, b->cap, true);
     cudaGraph_t gr = nullptr;
     const cudaError_t e = cudaStreamEndCapture(b->cap, &gr);
     if (rc || e != cudaSuccess) {
@@ -389,8 +562,10 @@ int argot_b200_batch_graph_launch(argot_b200_batch *b, void *stream) {
   return 0;
 }
 
-// Coordinate search over the configuration: starting from the current one,
-// each parameter in turn takes every candidate value with the others held;
+// Coordinate search over the configuration (the fused kernel's warps per
+// CTA and CTAs per SM, tile length, queue order, fused or split mode, the
+// split mode's number of parts): starting from the current one, each
+// parameter in turn takes every candidate value with the others held;
 // a candidate is timed by CUDA events around `reps` launches after one
 // warm-up launch.  Leaves the best configuration set.
 int argot_b200_batch_tune(argot_b200_batch *b, int reps, argot_b200_batch_config *best_out, float *best_ms,
@@ -421,16 +596,24 @@ int argot_b200_batch_tune(argot_b200_batch *b, int reps, argot_b200_batch_config
   const int per_sm[] = {1, 2, 3, 4, 6, 8};
   const int tiles[] = {1, 2, 4, 8, 16, 64};
   const int orders[] = {0, 1};
+  const int modes[] = {0, 1};
+  const int nparts[] = {2, 4, 8, 16};
   for (int pass = 0; pass < 2 && !rc; pass++) {
-    for (int dim = 0; dim < 4 && !rc; dim++) {
-      const int *vals = dim == 0 ? warps : dim == 1 ? per_sm : dim == 2 ? tiles : orders;
-      const int nv = dim == 0 ? 2 : dim == 1 ? 6 : dim == 2 ? 6 : 2;
+    for (int dim = 0; dim < 6 && !rc; dim++) {
+      // the fused kernel's launch shape only matters in fused mode, the
+      // number of parts only in split mode
+      if ((dim <= 1 && best.mode == 1) || (dim == 5 && best.mode == 0)) continue;
+      const int *vals = dim == 0 ? warps : dim == 1 ? per_sm : dim == 2 ? tiles : dim == 3 ? orders
+                      : dim == 4 ? modes : nparts;
+      const int nv = dim == 0 ? 2 : dim == 1 ? 6 : dim == 2 ? 6 : dim == 3 ? 2 : dim == 4 ? 2 : 4;
       for (int k = 0; k < nv && !rc; k++) {
         argot_b200_batch_config c = best;
-        int *field = dim == 0 ? &c.warps_per_cta : dim == 1 ? &c.ctas_per_sm : dim == 2 ? &c.blocks_per_item : &c.order;
+        int *field = dim == 0 ? &c.warps_per_cta : dim == 1 ? &c.ctas_per_sm : dim == 2 ? &c.blocks_per_item
+                   : dim == 3 ? &c.order : dim == 4 ? &c.mode : &c.parts;
         if (*field == vals[k]) continue;
         *field = vals[k];
         if (dim == 1 && vals[k] > max_ctas_per_sm(c.warps_per_cta)) continue;
+        if (c.mode == 1 && ensure_split(b) != 0) continue;  // no room for the columns: fused only
         float t = 0.f;
         rc = time_cfg(c, &t);
         if (!rc && t < t_best) {

@@ -116,93 +116,15 @@ __global__ void __launch_bounds__(32 * kF32Warps, ARGOT_RATE_MIN_CTAS)
                const uint64_t *__restrict__ blk_off, uint64_t base, const uint32_t *__restrict__ rays,
                uint64_t nray, const float *__restrict__ tau, float *__restrict__ rates6) {
   __shared__ BinPair s_pairs[kBinPairs];
-  __shared__ float s_nd[kF32Warps][32][6];
-  __shared__ double s_p[kF32Warps][32][3];
-  __shared__ double s_out[kF32Warps][32][6];
-  __shared__ int s_e[kF32Warps][32], s_t[kF32Warps][32];
+  __shared__ RateWarpSmem s_w[kF32Warps];
   load_bin_pairs(s_pairs);
   __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int grp = lane >> 3, j = lane & 7;
-  const unsigned gmask = 0xffu << (8 * grp);
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
-  for (uint64_t b = b0 + warp; b < b1; b += nwarp) {
-    int ix, iy, iz;
-    const bool own_valid = block_cell(g, b, lane, &ix, &iy, &iz);
-    const uint64_t own = own_valid ? cell_index(g, ix, iy, iz) : 0;
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    int bix, biy, biz;
-    block_cell(g, b, 0, &bix, &biy, &biz);
-    const uint64_t r0 = blk_off[b] - base, r1 = blk_off[b + 1] - base;
-    for (uint64_t rc = r0; rc < r1; rc += 32) {
-      // phase A
-      const uint64_t r = rc + lane;
-      int t = -1;
-      if (r < r1) {
-        const uint32_t w = __ldg(rays + r);
-        const uint32_t e = w >> 5;
-        t = (int)(w & 31u);
-        const int lx = bix + (t >> 4), ly = biy + ((t >> 2) & 3), lz = biz + (t & 3);
-        const float4 ep = __ldg(emit_pos + e);
-        const RayGeom geo = ray_geometry(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z);
-        const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
-        const RayCols cols = ray_columns(g, __ldg(tau + r), __ldg(tau + nray + r), __ldg(tau + 2 * nray + r), rw, geo);
-        const RayParams p = ray_params(cols, __ldg(total + e));
-#pragma unroll
-        for (int s = 0; s < 3; s++) {
-          s_nd[wib][lane][s] = p.N[s];
-          s_nd[wib][lane][3 + s] = p.D[s];
-          s_p[wib][lane][s] = p.P[s];
-        }
-        s_e[wib][lane] = (int)e;
-      }
-      s_t[wib][lane] = t;
-      __syncwarp();
-      const int nk = (int)min((uint64_t)32, r1 - rc);
-      // phase B
-      for (int q = grp; q < nk; q += 4) {
-        const float N0 = s_nd[wib][q][0], N1 = s_nd[wib][q][1], N2 = s_nd[wib][q][2];
-        const float D0 = s_nd[wib][q][3], D1 = s_nd[wib][q][4], D2 = s_nd[wib][q][5];
-        const float *sp = specn + (size_t)s_e[wib][q] * kNu;
-        float part[6];
-        ray_bins_packed(s_pairs, sp, j, N0, N1, N2, D0, D1, D2, part);
-        float g0 = part[0], g1 = part[1], g2 = part[2], h0 = part[3], h1 = part[4], h2 = part[5];
-#pragma unroll
-        for (int o = 1; o < 8; o <<= 1) {
-          g0 += __shfl_xor_sync(gmask, g0, o);
-          g1 += __shfl_xor_sync(gmask, g1, o);
-          g2 += __shfl_xor_sync(gmask, g2, o);
-          h0 += __shfl_xor_sync(gmask, h0, o);
-          h1 += __shfl_xor_sync(gmask, h1, o);
-          h2 += __shfl_xor_sync(gmask, h2, o);
-        }
-        if (j == 0) {
-          const double p0 = s_p[wib][q][0], p1 = s_p[wib][q][1], p2 = s_p[wib][q][2];
-          s_out[wib][q][0] = p0 * g0;
-          s_out[wib][q][1] = p1 * g1;
-          s_out[wib][q][2] = p2 * g2;
-          s_out[wib][q][3] = p0 * h0 * kHNuL;
-          s_out[wib][q][4] = p1 * h1 * kHNuL;
-          s_out[wib][q][5] = p2 * h2 * kHNuL;
-        }
-      }
-      __syncwarp();
-      // phase C
-      for (int k = 0; k < nk; k++) {
-        if (s_t[wib][k] == lane) {
-#pragma unroll
-          for (int s = 0; s < 6; s++) acc[s] += s_out[wib][k][s];
-        }
-      }
-      __syncwarp();
-    }
-    if (own_valid) {
-#pragma unroll
-      for (int s = 0; s < 6; s++) rates6[s * ncell + own] = (float)acc[s];
-    }
-  }
+  for (uint64_t b = b0 + warp; b < b1; b += nwarp)
+    rate_block_f32(g, raw, emit_pos, specn, total, s_pairs, b, blk_off[b] - base, blk_off[b + 1] - base, rays,
+                   nray, tau, rates6, s_w[wib], lane);
 }
 
 // ------------------------------------------------------------- drop-in rays

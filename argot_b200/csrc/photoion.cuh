@@ -283,4 +283,97 @@ __device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab,
   for (int q = 0; q < 6; q++) out[q] = acc[q].x + acc[q].y;
 }
 
+// Per-warp scratch of rate_block_f32.
+struct RateWarpSmem {
+  float nd[32][6];    // N_s, dN_s of the chunk's rays (cm^-2)
+  double p[32][3];    // prefactors
+  double out[32][6];  // per-ray rates
+  int e[32], t[32];   // emitter, target lane
+};
+
+// The FP32 rates of one target block b whose rays are [r0, r1) of `rays`
+// (columns in three planes of nray), written to its cells in rates6; one
+// warp.  Phase A: per-ray parameters, one lane per ray, 32 rays at a time.
+// Phase B: four 8-lane groups, one ray each, over the bin pairs
+// (ray_bins_packed), three butterfly steps.  Phase C: lane j adds the rays
+// of cell j of the block in ray order.
+__device__ __forceinline__ void rate_block_f32(const GridDev &g, const float4 *__restrict__ raw,
+                                               const float4 *__restrict__ emit_pos, const float *__restrict__ specn,
+                                               const double *__restrict__ total, const BinPair *__restrict__ pairs,
+                                               uint64_t b, uint64_t r0, uint64_t r1,
+                                               const uint32_t *__restrict__ rays, uint64_t nray,
+                                               const float *__restrict__ tau, float *__restrict__ rates6,
+                                               RateWarpSmem &S, int lane) {
+  const int grp = lane >> 3, j = lane & 7;
+  const unsigned gmask = 0xffu << (8 * grp);
+  const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
+  int ix, iy, iz;
+  const bool own_valid = block_cell(g, b, lane, &ix, &iy, &iz);
+  const uint64_t own = own_valid ? cell_index(g, ix, iy, iz) : 0;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  int bix, biy, biz;
+  block_cell(g, b, 0, &bix, &biy, &biz);
+  for (uint64_t rc = r0; rc < r1; rc += 32) {
+    const uint64_t r = rc + lane;
+    int t = -1;
+    if (r < r1) {
+      const uint32_t w = __ldg(rays + r);
+      const uint32_t e = w >> 5;
+      t = (int)(w & 31u);
+      const int lx = bix + (t >> 4), ly = biy + ((t >> 2) & 3), lz = biz + (t & 3);
+      const float4 ep = __ldg(emit_pos + e);
+      const RayGeom geo = ray_geometry(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z);
+      const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
+      const RayCols cols = ray_columns(g, __ldg(tau + r), __ldg(tau + nray + r), __ldg(tau + 2 * nray + r), rw, geo);
+      const RayParams p = ray_params(cols, __ldg(total + e));
+#pragma unroll
+      for (int s = 0; s < 3; s++) {
+        S.nd[lane][s] = p.N[s];
+        S.nd[lane][3 + s] = p.D[s];
+        S.p[lane][s] = p.P[s];
+      }
+      S.e[lane] = (int)e;
+    }
+    S.t[lane] = t;
+    __syncwarp();
+    const int nk = (int)min((uint64_t)32, r1 - rc);
+    for (int q = grp; q < nk; q += 4) {
+      float part[6];
+      ray_bins_packed(pairs, specn + (size_t)S.e[q] * kNu, j, S.nd[q][0], S.nd[q][1], S.nd[q][2], S.nd[q][3],
+                      S.nd[q][4], S.nd[q][5], part);
+      float g0 = part[0], g1 = part[1], g2 = part[2], h0 = part[3], h1 = part[4], h2 = part[5];
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) {
+        g0 += __shfl_xor_sync(gmask, g0, o);
+        g1 += __shfl_xor_sync(gmask, g1, o);
+        g2 += __shfl_xor_sync(gmask, g2, o);
+        h0 += __shfl_xor_sync(gmask, h0, o);
+        h1 += __shfl_xor_sync(gmask, h1, o);
+        h2 += __shfl_xor_sync(gmask, h2, o);
+      }
+      if (j == 0) {
+        const double p0 = S.p[q][0], p1 = S.p[q][1], p2 = S.p[q][2];
+        S.out[q][0] = p0 * g0;
+        S.out[q][1] = p1 * g1;
+        S.out[q][2] = p2 * g2;
+        S.out[q][3] = p0 * h0 * kHNuL;
+        S.out[q][4] = p1 * h1 * kHNuL;
+        S.out[q][5] = p2 * h2 * kHNuL;
+      }
+    }
+    __syncwarp();
+    for (int k = 0; k < nk; k++) {
+      if (S.t[k] == lane) {
+#pragma unroll
+        for (int s = 0; s < 6; s++) acc[s] += S.out[k][s];
+      }
+    }
+    __syncwarp();
+  }
+  if (own_valid) {
+#pragma unroll
+    for (int s = 0; s < 6; s++) rates6[s * ncell + own] = (float)acc[s];
+  }
+}
+
 }  // namespace argot

@@ -343,7 +343,8 @@ ARGOT_B200_API int argot_b200_photoion_rays_surrogate(const argot_b200_grid *g, 
 /* No counterpart in the reference, which runs one mesh per process.  Each
  * problem is prepared by the calls above (pack_fields, tree_build +
  * dev_tree_upload, count_rays + scan_blocks, emit_rays over all its blocks
- * with base 0); one launch then marches and integrates every ray of every
+ * with base 0); one launch (fused mode) or one graph of two persistent
+ * kernels (split mode) then marches and integrates every ray of every
  * problem (Kahan march + EXACT_F32 rates, the same arithmetic as
  * argot_b200_march_rays + argot_b200_photoion_rays, so each problem's rates
  * equal those of the problem run alone, bit for bit). */
@@ -358,10 +359,17 @@ typedef struct {
   float *rates6_dev;                     /* 6 x ncell, overwritten */
 } argot_b200_batch_problem;
 typedef struct {
-  int warps_per_cta;     /* 4 or 8 */
-  int ctas_per_sm;       /* 1..16, 0 = the occupancy limit */
+  int warps_per_cta;     /* fused mode: 4 or 8 */
+  int ctas_per_sm;       /* fused mode: 1..16, 0 = the occupancy limit */
   int blocks_per_item;   /* target blocks per tile of the work queue */
   int order;             /* 0: tiles by estimated cost, largest first; 1: problem order */
+  int mode;              /* 0: fused march + rates in one persistent kernel;
+                          * 1: split -- a persistent march kernel and a
+                          *    persistent rate kernel, columns through HBM
+                          *    (12 bytes per ray, allocated on first use), the
+                          *    rates of one part overlapping the march of the
+                          *    next on a second stream */
+  int parts;             /* split mode: 1..64 parts of the tile list */
 } argot_b200_batch_config;
 /* the problems' device buffers stay owned by the caller and must outlive
  * the batch */

@@ -65,19 +65,29 @@ def test_batch_matches_solo_runs(batch, solo):
     assert int(cnt.item()) == sum(c for _, c in solo)
 
 
-@pytest.mark.parametrize("cfg", [dict(warps_per_cta=4, ctas_per_sm=1, blocks_per_item=1, order=1),
-                                 dict(warps_per_cta=8, ctas_per_sm=2, blocks_per_item=16, order=0),
-                                 dict(warps_per_cta=4, ctas_per_sm=0, blocks_per_item=64, order=0)])
+_CFGS = [dict(warps_per_cta=4, ctas_per_sm=1, blocks_per_item=1, order=1, mode=0, parts=8),
+         dict(warps_per_cta=8, ctas_per_sm=2, blocks_per_item=16, order=0, mode=0, parts=8),
+         dict(warps_per_cta=4, ctas_per_sm=0, blocks_per_item=64, order=0, mode=0, parts=8),
+         dict(warps_per_cta=8, ctas_per_sm=0, blocks_per_item=1, order=0, mode=1, parts=1),
+         dict(warps_per_cta=8, ctas_per_sm=0, blocks_per_item=4, order=1, mode=1, parts=5),
+         dict(warps_per_cta=8, ctas_per_sm=0, blocks_per_item=2, order=0, mode=1, parts=64)]
+
+
+@pytest.mark.parametrize("cfg", _CFGS)
 def test_batch_every_configuration(batch, solo, cfg):
+    import torch
     batch.configure(**cfg)
     assert batch.config() == cfg
     _clear(batch)
-    batch.run()
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    batch.run(cnt)
     _check(batch, solo)
+    assert int(cnt.item()) == sum(c for _, c in solo)
 
 
-def test_batch_graph_replay(batch, solo):
-    batch.configure(warps_per_cta=8, ctas_per_sm=0, blocks_per_item=4, order=0)
+@pytest.mark.parametrize("mode", [0, 1])
+def test_batch_graph_replay(batch, solo, mode):
+    batch.configure(warps_per_cta=8, ctas_per_sm=0, blocks_per_item=4, order=0, mode=mode, parts=4)
     for _ in range(3):
         _clear(batch)
         batch.graph_launch()
