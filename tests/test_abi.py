@@ -86,3 +86,27 @@ def test_invalid_arguments_rejected_without_gpu():
     nb = C.c_uint64()
     assert lib.argot_b200_num_blocks(None, C.byref(nb)) == _lib.EINVAL
     assert lib.argot_b200_last_error() == _lib.EINVAL
+
+
+def test_batch_and_surrogate_reject_bad_arguments():
+    """Argument checks of the batch and surrogate entry points run before any
+    CUDA call, so they answer on a host without a GPU."""
+    import ctypes as C
+    from argot_b200 import _lib as L
+    from argot_b200.pipeline import unit_box_grid
+    lib = L.load()
+    h = C.c_void_p()
+    assert lib.argot_b200_batch_create(None, 0, C.byref(h)) == L.EINVAL
+    probs = (L.BatchProblem * 1)()
+    probs[0] = L.BatchProblem(unit_box_grid(8, 1.0, 1.0), None, None, None, None, None, None)
+    assert lib.argot_b200_batch_create(probs, 1, C.byref(h)) == L.EINVAL   # no buffers
+    assert lib.argot_b200_batch_configure(None, None) == L.EINVAL
+    assert lib.argot_b200_batch_run(None, None, None) == L.EINVAL
+    assert lib.argot_b200_batch_graph_launch(None, None) == L.EINVAL
+    assert lib.argot_b200_batch_tune(None, 1, None, None, None) == L.EINVAL
+    assert lib.argot_b200_batch_num_items(None) == -1
+    assert lib.argot_b200_surrogate_workspace(10) == 7 * 4 * 10
+    assert lib.argot_b200_surrogate_create(None, None, 5e-4, C.byref(h)) == L.EINVAL
+    g = unit_box_grid(8, 1.0, 1.0)
+    assert lib.argot_b200_photoion_rays_surrogate(C.byref(g), None, None, None, 0, 1, None, 0, None, 0, None,
+                                                  None, None, None, None) == L.EINVAL
