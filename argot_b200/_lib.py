@@ -66,6 +66,8 @@ SIGNATURES = {
     "zero_out_photoion_rate_cuda": (None, [vp, vp, vp]),
     "accum_optical_depth": (None, [vp, vp, vp, vp]),
     "argot_b200_set_dropin_march_mode": (i32, [i32]),
+    "smooth_photoion_rate": (None, [vp, vp, vp, vp, vp]),
+    "argot_b200_set_dropin_smooth_faces": (i32, [i32]),
     "argot_b200_pack_fields": (i32, [GP, vp, vp, vp, vp, vp, vp]),
     "argot_b200_pack_fluid_mesh": (i32, [GP, vp, vp, vp]),
     "argot_b200_tree_build": (i32, [GP, i32, vp, vp, f32, C.POINTER(vp)]),

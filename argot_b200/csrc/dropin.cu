@@ -1,7 +1,7 @@
-// dropin.cu -- the reference's own entry points (src/prototype.h:75,121,
+// dropin.cu -- the reference's own entry points (src/prototype.h:75,89,121,
 // 152-153) on one GPU, for argot_mpi / argot_hydro_mpi to link in place of
-// calc_optical_depth_cuda.o, calc_photoion_rate_cuda.o and
-// accum_optical_depth.o on a single rank.
+// calc_optical_depth_cuda.o, calc_photoion_rate_cuda.o,
+// accum_optical_depth.o and smooth_photoion_rate.o on a single rank.
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
@@ -22,6 +22,7 @@ int launch_rate_rayio(const GridDev &g, const float4 *raw, const void *rays_io, 
 int launch_accum_runs(const GridDev &g, const void *rays_io, uint64_t nray, int rx, int ry, int rz,
                       const double *per6, void *mesh, cudaStream_t st);
 int launch_zero_rates(uint64_t n, void *mesh, cudaStream_t st);
+int launch_smooth_mesh(int nx, int ny, int nz, void *mesh, float *work, int isolated, cudaStream_t st);
 int *err_flag(int dev);
 int check_err_flag(int *flag, cudaStream_t st);
 
@@ -47,6 +48,7 @@ struct DropinState {
   Pool cells;   // packed fields: cells + raw, 32 B per cell
   Pool work[2]; // double-buffered segment / ray chunks
   Pool per6;    // per-ray rates
+  Pool smooth;  // rate planes of the smoothing: 12 floats per cell
   cudaStream_t lane[2] = {nullptr, nullptr};
   cudaEvent_t ev = nullptr;
   cudaEvent_t rate_done[2] = {nullptr, nullptr};
@@ -57,6 +59,7 @@ struct DropinState {
 std::mutex g_mu;
 DropinState g_state;
 int g_march_mode = -1;
+int g_smooth_isolated = 1;
 
 int march_mode() {
   if (g_march_mode < 0) {
@@ -229,6 +232,62 @@ int do_rates(cuda_mem_space *cm, light_ray *ray, light_ray_IO *ray_io, cuda_para
   return 0;
 }
 
+// smooth_photoion_rate with __USE_GPU__ on one rank
+// (src/smooth_photoion_rate.c:27-1588): the reference copies the rates of
+// mesh_dev to the host (recv_photoion_data), smooths them there, copies the
+// result back into mesh_dev (send_photoion_data) and into the host mesh.
+// Here the smoothing runs on mesh_dev in place; only the host copy of the
+// result crosses PCIe.
+int do_smooth(fluid_mesh *mesh, run_param *run, cuda_mem_space *cm, cuda_param *cp) {
+  if (!cm || !run || !cm[0].mesh_dev) return ARGOT_B200_EINVAL;
+  const int nx = run->nmesh_x_local, ny = run->nmesh_y_local, nz = run->nmesh_z_local;
+  if (nx <= 0 || ny <= 0 || nz <= 0) return ARGOT_B200_EINVAL;
+  const uint64_t ncell = (uint64_t)nx * ny * nz;
+  if (ncell >= (1ull << 32)) return ARGOT_B200_EINVAL;
+  DeviceScope dscope;
+  if (!dscope.ok) return ARGOT_B200_ECUDA;
+  std::lock_guard<std::mutex> lock(g_mu);
+  DropinState &s = g_state;
+  int rc = ensure_state(s);
+  if (rc) return rc;
+  ARGOT_CUDA_TRY(s.smooth.ensure(12 * sizeof(float) * ncell));
+  cudaStream_t caller = caller_stream(cp);
+  float *work = (float *)s.smooth.ptr;
+  if ((rc = launch_smooth_mesh(nx, ny, nz, cm[0].mesh_dev, work, g_smooth_isolated, caller))) return rc;
+  if (mesh) {
+    std::vector<float> host(6 * ncell);
+    ARGOT_CUDA_TRY(cudaMemcpyAsync(host.data(), work + 6 * ncell, 6 * sizeof(float) * ncell,
+                                   cudaMemcpyDeviceToHost, caller));
+    ARGOT_CUDA_TRY(cudaStreamSynchronize(caller));
+    auto scatter = [&](uint64_t a, uint64_t b) {
+      for (uint64_t i = a; i < b; i++) {
+        prim_chem &pc = mesh[i].prev_chem;
+        pc.GammaHI = host[0 * ncell + i];
+        pc.GammaHeI = host[1 * ncell + i];
+        pc.GammaHeII = host[2 * ncell + i];
+        pc.HeatHI = host[3 * ncell + i];
+        pc.HeatHeI = host[4 * ncell + i];
+        pc.HeatHeII = host[5 * ncell + i];
+      }
+    };
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (ncell < 65536 || hw == 1) {
+      scatter(0, ncell);
+      return 0;
+    }
+    std::vector<std::thread> th;
+    const uint64_t per = (ncell + hw - 1) / hw;
+    for (unsigned t = 0; t < hw; t++) {
+      const uint64_t a = t * per, b = std::min(ncell, a + per);
+      if (a < b) th.emplace_back(scatter, a, b);
+    }
+    for (auto &x : th) x.join();
+    return 0;
+  }
+  ARGOT_CUDA_TRY(cudaStreamSynchronize(caller));
+  return 0;
+}
+
 }  // namespace dropin_detail
 using namespace dropin_detail;
 }  // namespace argot
@@ -246,6 +305,23 @@ int argot_b200_set_dropin_march_mode(int mode) {
       mode == ARGOT_B200_MARCH_KAHAN ? ARGOT_B200_PRECISION_KAHAN : ARGOT_B200_PRECISION_REFERENCE;
   set_status(0);
   return 0;
+}
+
+int argot_b200_set_dropin_smooth_faces(int faces) {
+  if (faces != ARGOT_B200_FACES_PERIODIC && faces != ARGOT_B200_FACES_ISOLATED) {
+    set_status(ARGOT_B200_EINVAL);
+    return ARGOT_B200_EINVAL;
+  }
+  argot::g_smooth_isolated = faces == ARGOT_B200_FACES_ISOLATED;
+  set_status(0);
+  return 0;
+}
+
+void smooth_photoion_rate(::fluid_mesh *mesh, ::run_param *this_run, ::cuda_mem_space *cuda_mem,
+                          ::cuda_param *this_cuda, struct mpi_param *this_mpi) {
+  (void)this_mpi;
+  set_status(argot::do_smooth((argot::fluid_mesh *)mesh, (argot::run_param *)this_run,
+                              (argot::cuda_mem_space *)cuda_mem, (argot::cuda_param *)this_cuda));
 }
 
 void calc_optical_depth_cuda(::ray_segment *seg, ::cuda_mem_space *cuda_mem,

@@ -76,6 +76,7 @@ struct run_param;
 struct cuda_mem_space;
 struct cuda_param;
 struct omp_param;
+struct mpi_param;
 
 /* Replaces src/calc_optical_depth_cuda.cu:29-144 (declared at
  * src/prototype.h:152).  Overwrites seg[0..run->nseg).optical_depth_* in
@@ -112,6 +113,27 @@ ARGOT_B200_API void accum_optical_depth(struct light_ray *ray, struct ray_segmen
 #define ARGOT_B200_MARCH_REFERENCE 0
 #define ARGOT_B200_MARCH_KAHAN 1
 ARGOT_B200_API int argot_b200_set_dropin_march_mode(int mode);
+
+/* Replaces src/smooth_photoion_rate.c:27-1588 as built with __USE_GPU__
+ * (src/prototype.h:89) on a single rank.  Smooths
+ * cuda_mem[0].mesh_dev[].prev_chem.{Gamma,Heat}{HI,HeI,HeII} in place on the
+ * device, bit-identical to the reference's host smoothing (27 cells, centre
+ * weighted by 30, times 1/56), so the rates stay in HBM for the GPU
+ * chemistry (src/chemistry.cu) that reads mesh_dev next; then, when mesh is
+ * not NULL, writes the smoothed values into mesh[].prev_chem as the
+ * reference does.  this_mpi is not used (no neighbour ranks).  The mesh
+ * faces follow argot_b200_set_dropin_smooth_faces. */
+ARGOT_B200_API void smooth_photoion_rate(struct fluid_mesh *mesh, struct run_param *this_run,
+                                         struct cuda_mem_space *cuda_mem, struct cuda_param *this_cuda,
+                                         struct mpi_param *this_mpi);
+
+/* Faces of the drop-in smoothing: ARGOT_B200_FACES_ISOLATED (default; ARGOT
+ * built with -D__ISOLATED__, its Makefile's default: a face cell stands in
+ * for its missing neighbour) or ARGOT_B200_FACES_PERIODIC (the periodic
+ * image). */
+#define ARGOT_B200_FACES_PERIODIC 0
+#define ARGOT_B200_FACES_ISOLATED 1
+ARGOT_B200_API int argot_b200_set_dropin_smooth_faces(int faces);
 
 /* ================================================= 2. device-resident API */
 
