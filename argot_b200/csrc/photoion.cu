@@ -110,11 +110,13 @@ __global__ void __launch_bounds__(32 * kRateWarps)
 #endif
 constexpr int kF32Warps = ARGOT_RATE_WARPS;
 
+template <bool kServed>
 __global__ void __launch_bounds__(32 * kF32Warps, ARGOT_RATE_MIN_CTAS)
     k_rate_f32(GridDev g, const float4 *__restrict__ raw, const float4 *__restrict__ emit_pos,
                const float *__restrict__ specn, const double *__restrict__ total, uint64_t b0, uint64_t b1,
                const uint64_t *__restrict__ blk_off, uint64_t base, const uint32_t *__restrict__ rays,
-               uint64_t nray, const float *__restrict__ tau, float *__restrict__ rates6) {
+               uint64_t nray, const float *__restrict__ tau, float *__restrict__ rates6,
+               const float *__restrict__ pred) {
   __shared__ BinPair s_pairs[kBinPairs];
   __shared__ RateWarpSmem s_w[kF32Warps];
   load_bin_pairs(s_pairs);
@@ -123,8 +125,22 @@ __global__ void __launch_bounds__(32 * kF32Warps, ARGOT_RATE_MIN_CTAS)
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t b = b0 + warp; b < b1; b += nwarp)
-    rate_block_f32(g, raw, emit_pos, specn, total, s_pairs, b, blk_off[b] - base, blk_off[b + 1] - base, rays,
-                   nray, tau, rates6, s_w[wib], lane);
+    rate_block_f32<kServed>(g, raw, emit_pos, specn, total, s_pairs, b, blk_off[b] - base, blk_off[b + 1] - base,
+                            rays, nray, tau, rates6, s_w[wib], lane, pred);
+}
+
+// The FP32 rates of blocks [b0, b1) where the rays flagged in pred (7
+// planes: six contributions and a flag, see rate_block_f32) keep their
+// given contributions: the surrogate's second stage.
+int launch_rate_f32_served(const GridDev &g, const float4 *raw, const float4 *emit_pos, const float *specn,
+                           const double *total, uint64_t b0, uint64_t b1, const uint64_t *blk_off, uint64_t base,
+                           const uint32_t *rays, uint64_t nray, const float *tau, float *rates6, const float *pred,
+                           cudaStream_t st) {
+  if (b0 >= b1) return 0;
+  k_rate_f32<true><<<grid_blocks_for_rates((b1 - b0) * 32, 32 * kF32Warps), 32 * kF32Warps, 0, st>>>(
+      g, raw, emit_pos, specn, total, b0, b1, blk_off, base, rays, nray, tau, rates6, pred);
+  ARGOT_CUDA_TRY(cudaGetLastError());
+  return 0;
 }
 
 // ------------------------------------------------------------- drop-in rays
@@ -262,8 +278,9 @@ extern "C" int argot_b200_photoion_rays(const argot_b200_grid *gp, const void *p
         g, raw, t->emit_pos, t->emit_spec64, t->emit_specn, t->emit_total, b0, b1, blk_off, base, rays, nray, tau,
         rates6);
   else
-    k_rate_f32<<<grid_blocks_for_rates((b1 - b0) * 32, 32 * kF32Warps), 32 * kF32Warps, 0, st>>>(
-        g, raw, t->emit_pos, t->emit_specn, t->emit_total, b0, b1, blk_off, base, rays, nray, tau, rates6);
+    k_rate_f32<false><<<grid_blocks_for_rates((b1 - b0) * 32, 32 * kF32Warps), 32 * kF32Warps, 0, st>>>(
+        g, raw, t->emit_pos, t->emit_specn, t->emit_total, b0, b1, blk_off, base, rays, nray, tau, rates6,
+        nullptr);
   ARGOT_CUDA_TRY(cudaGetLastError());
   set_status(0);
   return 0;

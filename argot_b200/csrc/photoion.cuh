@@ -289,6 +289,7 @@ struct RateWarpSmem {
   double p[32][3];    // prefactors
   double out[32][6];  // per-ray rates
   int e[32], t[32];   // emitter, target lane
+  int q[32];          // lanes of the chunk's rays that take the quadrature
 };
 
 // The FP32 rates of one target block b whose rays are [r0, r1) of `rays`
@@ -297,13 +298,18 @@ struct RateWarpSmem {
 // Phase B: four 8-lane groups, one ray each, over the bin pairs
 // (ray_bins_packed), three butterfly steps.  Phase C: lane j adds the rays
 // of cell j of the block in ray order.
+// kServed: `pred` holds 7 planes of nray floats, six per-ray contributions
+// and a flag; a ray whose flag is non-zero contributes those six values
+// and skips the quadrature, which runs over the remaining rays of the
+// chunk only (the surrogate's fallback).
+template <bool kServed = false>
 __device__ __forceinline__ void rate_block_f32(const GridDev &g, const float4 *__restrict__ raw,
                                                const float4 *__restrict__ emit_pos, const float *__restrict__ specn,
                                                const double *__restrict__ total, const BinPair *__restrict__ pairs,
                                                uint64_t b, uint64_t r0, uint64_t r1,
                                                const uint32_t *__restrict__ rays, uint64_t nray,
                                                const float *__restrict__ tau, float *__restrict__ rates6,
-                                               RateWarpSmem &S, int lane) {
+                                               RateWarpSmem &S, int lane, const float *__restrict__ pred = nullptr) {
   const int grp = lane >> 3, j = lane & 7;
   const unsigned gmask = 0xffu << (8 * grp);
   const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
@@ -316,28 +322,42 @@ __device__ __forceinline__ void rate_block_f32(const GridDev &g, const float4 *_
   for (uint64_t rc = r0; rc < r1; rc += 32) {
     const uint64_t r = rc + lane;
     int t = -1;
+    bool quad = false;
     if (r < r1) {
       const uint32_t w = __ldg(rays + r);
       const uint32_t e = w >> 5;
       t = (int)(w & 31u);
-      const int lx = bix + (t >> 4), ly = biy + ((t >> 2) & 3), lz = biz + (t & 3);
-      const float4 ep = __ldg(emit_pos + e);
-      const RayGeom geo = ray_geometry(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z);
-      const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
-      const RayCols cols = ray_columns(g, __ldg(tau + r), __ldg(tau + nray + r), __ldg(tau + 2 * nray + r), rw, geo);
-      const RayParams p = ray_params(cols, __ldg(total + e));
+      if (kServed && __ldg(pred + 6 * nray + r) != 0.f) {
 #pragma unroll
-      for (int s = 0; s < 3; s++) {
-        S.nd[lane][s] = p.N[s];
-        S.nd[lane][3 + s] = p.D[s];
-        S.p[lane][s] = p.P[s];
+        for (int s = 0; s < 6; s++) S.out[lane][s] = (double)__ldg(pred + s * nray + r);
+      } else {
+        quad = true;
+        const int lx = bix + (t >> 4), ly = biy + ((t >> 2) & 3), lz = biz + (t & 3);
+        const float4 ep = __ldg(emit_pos + e);
+        const RayGeom geo = ray_geometry(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z);
+        const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
+        const RayCols cols = ray_columns(g, __ldg(tau + r), __ldg(tau + nray + r), __ldg(tau + 2 * nray + r), rw, geo);
+        const RayParams p = ray_params(cols, __ldg(total + e));
+#pragma unroll
+        for (int s = 0; s < 3; s++) {
+          S.nd[lane][s] = p.N[s];
+          S.nd[lane][3 + s] = p.D[s];
+          S.p[lane][s] = p.P[s];
+        }
+        S.e[lane] = (int)e;
       }
-      S.e[lane] = (int)e;
     }
     S.t[lane] = t;
-    __syncwarp();
     const int nk = (int)min((uint64_t)32, r1 - rc);
-    for (int q = grp; q < nk; q += 4) {
+    int nq = nk;
+    if (kServed) {
+      const unsigned m = __ballot_sync(0xffffffffu, quad);
+      if (quad) S.q[__popc(m & ((1u << lane) - 1u))] = lane;
+      nq = __popc(m);
+    }
+    __syncwarp();
+    for (int i = grp; i < nq; i += 4) {
+      const int q = kServed ? S.q[i] : i;
       float part[6];
       ray_bins_packed(pairs, specn + (size_t)S.e[q] * kNu, j, S.nd[q][0], S.nd[q][1], S.nd[q][2], S.nd[q][3],
                       S.nd[q][4], S.nd[q][5], part);

@@ -16,10 +16,12 @@
 // Error control per cell.  Kernel 1 predicts every ray's six contributions
 // c_j with a relative error bound eps (from the validated envelope of the
 // network's error, measured on held-out samples) and a lower bound S_j of
-// each cell's total (each ray's true sum is at least I^ e^-x per node).  Kernel 2 keeps the predictions of the rays with the smallest
-// shares beta = eps max_j c_j / S_j while their sum stays within the cell's
-// budget tol, so that the surrogate's error is at most tol S_j per cell and
-// output; the other rays take the exact FP32 quadrature.  A ray always
+// each cell's total (each ray's true sum is at least I^ e^-x per node).
+// Kernel 2 keeps the predictions of the rays with the smallest shares
+// beta = eps max_j c_j / S_j while their sum stays within the cell's budget
+// tol, so that the surrogate's error is at most tol S_j per cell and
+// output; kernel 3 (the FP32 rate kernel) runs the exact quadrature for the
+// other rays and sums the cells.  A ray always
 // takes the exact quadrature when its emitter is not a single-temperature
 // blackbody in [1e4, 10^5.5] K, when dtau_max > 2, or when a node's
 // log10 tau lies above 3.
@@ -37,6 +39,10 @@
 namespace argot {
 
 int grid_blocks_for_rates(uint64_t n, int threads);
+int launch_rate_f32_served(const GridDev &g, const float4 *raw, const float4 *emit_pos, const float *specn,
+                           const double *total, uint64_t b0, uint64_t b1, const uint64_t *blk_off, uint64_t base,
+                           const uint32_t *rays, uint64_t nray, const float *tau, float *rates6, const float *pred,
+                           cudaStream_t st);
 
 constexpr int kEnvBins = 64;        // error envelope bins over predicted q
 constexpr float kEnvQLo = -7.0f;     // ... in [-7, 0]
@@ -67,16 +73,11 @@ struct PredSmem {
   int t[kSurWarps][32];
 };
 
-struct FinSmem {
-  BinPair pairs[kBinPairs];
+struct SelSmem {
   // per warp
   float Sc[kSurWarps][32][6];                // lower bounds of the cell totals
   unsigned hist[kSurWarps][32][kHistBins];   // budget-share histogram per cell
   int thr[kSurWarps][32];                    // last accepted bin per cell
-  float nd[kSurWarps][32][6];                // N_s, dN_s (cm^-2, float)
-  double p[kSurWarps][32][3];                // prefactors
-  double out[kSurWarps][32][6];              // per-ray rates
-  int e[kSurWarps][32], t[kSurWarps][32];
 };
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
@@ -431,21 +432,16 @@ __device__ __forceinline__ double beta_edge(int b) { return exp2(0.5 * (double)(
 // Kernel 2: per cell, the rays whose error bounds fit the budget
 // tol * S_j (the smallest bounds first, by the histogram of beta; the sum
 // of a bin is bounded by its count times its upper edge) keep the
-// network's contributions; every other ray takes the exact FP32
-// quadrature.  Per-cell sums in ray order, as the exact kernels.
-__global__ void __launch_bounds__(32 * kSurWarps, ARGOT_SUR_FINISH_MIN_CTAS)
-    k_sur_finish(GridDev g, const float4 *__restrict__ raw, const float4 *__restrict__ emit_pos,
-                 const float *__restrict__ specn, const double *__restrict__ total, float tol, uint64_t b0,
-                 uint64_t b1, const uint64_t *__restrict__ blk_off, uint64_t base, const uint32_t *__restrict__ rays,
-                 uint64_t nray, const float *__restrict__ tau, const float *__restrict__ work,
-                 float *__restrict__ rates6, unsigned long long *__restrict__ counters) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  FinSmem &S = *reinterpret_cast<FinSmem *>(smem_raw);
-  load_bin_pairs(S.pairs);
-  __syncthreads();
+// network's contributions: their flag (work plane 6, which held eps) is set
+// to 1, every other ray's to 0.  Kernel 3, the FP32 rate kernel
+// (rate_block_f32<true>), then runs the exact quadrature for the flagged-0
+// rays only, at its own occupancy, and sums every cell in ray order.
+__global__ void __launch_bounds__(32 * kSurWarps)
+    k_sur_select(GridDev g, float tol, uint64_t b0, uint64_t b1, const uint64_t *__restrict__ blk_off, uint64_t base,
+                 const uint32_t *__restrict__ rays, uint64_t nray, const float *__restrict__ rates6,
+                 float *__restrict__ work, unsigned long long *__restrict__ counters) {
+  __shared__ SelSmem S;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int grp = lane >> 3, jj = lane & 7;
-  const unsigned gmask = 0xffu << (8 * grp);
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
@@ -457,8 +453,6 @@ __global__ void __launch_bounds__(32 * kSurWarps, ARGOT_SUR_FINISH_MIN_CTAS)
 #pragma unroll
     for (int s = 0; s < 6; s++) S.Sc[wib][lane][s] = own_valid ? rates6[s * ncell + own] : 0.f;
     for (int k = 0; k < kHistBins; k++) S.hist[wib][lane][k] = 0u;
-    int bix, biy, biz;
-    block_cell(g, b, 0, &bix, &biy, &biz);
     const uint64_t r0 = blk_off[b] - base, r1 = blk_off[b + 1] - base;
     __syncwarp();
     // ---- pass 1: histogram of beta per cell
@@ -466,8 +460,8 @@ __global__ void __launch_bounds__(32 * kSurWarps, ARGOT_SUR_FINISH_MIN_CTAS)
       const int tl = (int)(__ldg(rays + r) & 31u);
       float c[6];
 #pragma unroll
-      for (int j = 0; j < 6; j++) c[j] = __ldg(work + j * nray + r);
-      const int bin = beta_bin(c, __ldg(work + 6 * nray + r), S.Sc[wib][tl]);
+      for (int j = 0; j < 6; j++) c[j] = work[j * nray + r];
+      const int bin = beta_bin(c, work[6 * nray + r], S.Sc[wib][tl]);
       if (bin >= 0) atomicAdd(&S.hist[wib][tl][bin], 1u);
     }
     __syncwarp();
@@ -485,83 +479,17 @@ __global__ void __launch_bounds__(32 * kSurWarps, ARGOT_SUR_FINISH_MIN_CTAS)
       S.thr[wib][lane] = thr;
     }
     __syncwarp();
-    // ---- pass 2: accepted rays keep the prediction, the rest go exact
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (uint64_t rc = r0; rc < r1; rc += 32) {
-      const uint64_t r = rc + lane;
-      int tl = -1;
-      bool need_exact = false;
-      if (r < r1) {
-        tl = (int)(__ldg(rays + r) & 31u);
-        float c[6];
+    // ---- pass 2: the flags
+    for (uint64_t r = r0 + lane; r < r1; r += 32) {
+      const int tl = (int)(__ldg(rays + r) & 31u);
+      float c[6];
 #pragma unroll
-        for (int j = 0; j < 6; j++) c[j] = __ldg(work + j * nray + r);
-        const int bin = beta_bin(c, __ldg(work + 6 * nray + r), S.Sc[wib][tl]);
-        if (bin >= 0 && bin <= S.thr[wib][tl]) {
-#pragma unroll
-          for (int j = 0; j < 6; j++) S.out[wib][lane][j] = (double)c[j];
-          n_sur++;
-        } else {
-          const RayTask t = ray_task(g, raw, emit_pos, total, rays, tau, nray, r, bix, biy, biz);
-#pragma unroll
-          for (int s = 0; s < 3; s++) {
-            S.nd[wib][lane][s] = t.p.N[s];
-            S.nd[wib][lane][3 + s] = t.p.D[s];
-            S.p[wib][lane][s] = t.p.P[s];
-          }
-          S.e[wib][lane] = t.e;
-          need_exact = true;
-        }
-      }
-      S.t[wib][lane] = tl;
-      __syncwarp();
-      // exact FP32 quadrature, four rays at a time, eight lanes each
-      unsigned mexact = __ballot_sync(0xffffffffu, need_exact);
-      n_exact += need_exact;
-      while (mexact) {
-        int q[4];
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          q[k] = mexact ? __ffs(mexact) - 1 : -1;
-          if (mexact) mexact &= mexact - 1;
-        }
-        const int qq = q[grp];
-        if (qq >= 0) {
-          const float N0 = S.nd[wib][qq][0], N1 = S.nd[wib][qq][1], N2 = S.nd[wib][qq][2];
-          const float D0 = S.nd[wib][qq][3], D1 = S.nd[wib][qq][4], D2 = S.nd[wib][qq][5];
-          const float *sp = specn + (size_t)S.e[wib][qq] * kNu;
-          float part[6];
-          ray_bins_packed(S.pairs, sp, jj, N0, N1, N2, D0, D1, D2, part);
-          float g0 = part[0], g1 = part[1], g2 = part[2], h0 = part[3], h1 = part[4], h2 = part[5];
-#pragma unroll
-          for (int o = 1; o < 8; o <<= 1) {
-            g0 += __shfl_xor_sync(gmask, g0, o); g1 += __shfl_xor_sync(gmask, g1, o);
-            g2 += __shfl_xor_sync(gmask, g2, o); h0 += __shfl_xor_sync(gmask, h0, o);
-            h1 += __shfl_xor_sync(gmask, h1, o); h2 += __shfl_xor_sync(gmask, h2, o);
-          }
-          if (jj == 0) {
-            const double p0 = S.p[wib][qq][0], p1 = S.p[wib][qq][1], p2 = S.p[wib][qq][2];
-            S.out[wib][qq][0] = p0 * g0; S.out[wib][qq][1] = p1 * g1; S.out[wib][qq][2] = p2 * g2;
-            S.out[wib][qq][3] = p0 * h0 * kHNuL; S.out[wib][qq][4] = p1 * h1 * kHNuL;
-            S.out[wib][qq][5] = p2 * h2 * kHNuL;
-          }
-        }
-        __syncwarp();
-      }
-      __syncwarp();
-      // ---- per-cell sums in ray order
-      const int nk = (int)min((uint64_t)32, r1 - rc);
-      for (int k = 0; k < nk; k++) {
-        if (S.t[wib][k] == lane) {
-#pragma unroll
-          for (int s = 0; s < 6; s++) acc[s] += S.out[wib][k][s];
-        }
-      }
-      __syncwarp();
-    }
-    if (own_valid) {
-#pragma unroll
-      for (int s = 0; s < 6; s++) rates6[s * ncell + own] = (float)acc[s];
+      for (int j = 0; j < 6; j++) c[j] = work[j * nray + r];
+      const int bin = beta_bin(c, work[6 * nray + r], S.Sc[wib][tl]);
+      const bool served = bin >= 0 && bin <= S.thr[wib][tl];
+      work[6 * nray + r] = served ? 1.f : 0.f;
+      n_sur += served;
+      n_exact += !served;
     }
     __syncwarp();
   }
@@ -750,8 +678,6 @@ int argot_b200_photoion_rays_surrogate(const argot_b200_grid *gp, const void *pa
     if (!attr[dev]) {
       ARGOT_CUDA_TRY(cudaFuncSetAttribute(k_sur_predict, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)sizeof(PredSmem)));
-      ARGOT_CUDA_TRY(cudaFuncSetAttribute(k_sur_finish, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)sizeof(FinSmem)));
       attr[dev] = true;
     }
   }
@@ -765,10 +691,12 @@ int argot_b200_photoion_rays_surrogate(const argot_b200_grid *gp, const void *pa
                                                             t->emit_i0, t->emit_m, sur->dev, b0, b1, blk_off,
                                                             base, rays, nray, tau, rates6, work);
   ARGOT_CUDA_TRY(cudaGetLastError());
-  k_sur_finish<<<blocks, threads, sizeof(FinSmem), st>>>(g, raw, t->emit_pos, t->emit_specn, t->emit_total,
-                                                          sur->tol, b0, b1, blk_off, base, rays, nray, tau, work,
-                                                          rates6, counters);
+  k_sur_select<<<blocks, threads, 0, st>>>(g, sur->tol, b0, b1, blk_off, base, rays, nray, rates6, work,
+                                            counters);
   ARGOT_CUDA_TRY(cudaGetLastError());
+  rc = launch_rate_f32_served(g, raw, t->emit_pos, t->emit_specn, t->emit_total, b0, b1, blk_off, base, rays, nray,
+                              tau, rates6, work, st);
+  if (rc) return rc;
   set_status(0);
   return 0;
 }

@@ -233,6 +233,56 @@ def cpu_sample(wl, target_seconds: float = 15.0, max_cells: int = 1 << 20, R=Non
             "_probe_rays": probe["nray"]}
 
 
+def reference_gpu_sample(wl, target_rays: int = 2_000_000, seed: int = 1, reps: int = 3):
+    """ARGOT's own GPU entry points (calc_optical_depth_cuda,
+    calc_photoion_rate_cuda; compiled for sm_100a with the reference's nvcc
+    flags) on a bounded, seeded sample of the same workload: one contiguous
+    range of target cells holding about `target_rays` rays (the reference
+    keeps a 2 KB spectrum per ray in host and device memory, which bounds the
+    sample), run group by group as calc_ARGOT_part runs it.  Reported: the
+    hot path through the reference's calls (wall: its allocations, host
+    copies, transfers and kernels; accum_optical_depth on the host) and its
+    two kernels alone (CUDA events, the reference's launch geometry)."""
+    from oracle.oracle import Oracle, RefGpu, unit_box_grid
+    R = RefGpu(wl.edge)
+    try:
+        R.init(wl.lunit, wl.denstonh, wl.theta, os.cpu_count() or 1)
+        R.set_mesh(*wl.fields())
+        R.set_sources(wl.src_type, wl.src_param, wl.src_pos, wl.src_rate)
+        R.upload()
+        rng = np.random.default_rng(seed)
+        ncell = wl.edge ** 3
+        probe = min(256, ncell)
+        im0 = int(rng.integers(0, ncell - probe + 1))
+        per_cell = max(1.0, R.count_rays(im0, im0 + probe) / probe)
+        ncells = int(min(ncell, max(64, target_rays / per_cell)))
+        im0 = int(rng.integers(0, ncell - ncells + 1))
+        R.zero_rates_gpu()
+        out = R.run_range_gpu(im0, im0 + ncells, kernel_reps=reps, want=("seg",))
+    finally:
+        R.close()
+    cross = float(Oracle().count_crossings(unit_box_grid(wl.edge, wl.lunit, wl.denstonh), out["seg"]).sum())
+    calls = out["march_s"] + out["accum_s"] + out["rates_s"]
+    t_mk, t_rk = out["march_kernel_ms"] / 1e3, out["rate_kernel_ms"] / 1e3
+    hbm, _, peak_kind = measured_peaks()
+    march_gbs = (16.0 * cross + 36.0 * out["nseg"]) / t_mk / 1e9
+    return {"kind": "reference",
+            "build": "ARGOT src/calc_optical_depth_cuda.cu, src/calc_photoion_rate_cuda.cu, "
+                     "nvcc -use_fast_math -O3 for sm_100a",
+            "sample": (f"{ncells} consecutive target cells from index {im0} of {wl.name} "
+                       f"({out['nray']} rays, {cross:.3e} crossings, {out['groups']} groups)"),
+            "value": cross / calls, "unit": UNIT,
+            "kernels_value": cross / (t_mk + t_rk),
+            "march_crossings_per_s": cross / t_mk,
+            "march_roofline": {"achieved": march_gbs, "peak": hbm, "unit": "GB/s", "frac": march_gbs / hbm,
+                               "peak_kind": f"{peak_kind} hbm_gbs", "bytes_model": "16 B per crossing + 36 B per ray"},
+            "gamma_cells_per_s": ncells / t_rk,
+            "rates_rays_per_s": out["nray"] / t_rk,
+            "calls_s": {"calc_optical_depth_cuda": out["march_s"], "accum_optical_depth": out["accum_s"],
+                        "calc_photoion_rate_cuda": out["rates_s"], "ray_setup_host": out["setup_s"]},
+            "kernels_s": {"calc_optical_depth_kernel": t_mk, "calc_photoion_rate_kernel": t_rk}}
+
+
 # ------------------------------------------------------------ rate modes
 def load_surrogate(pb):
     """The trained weights (argot_b200/data/surrogate.npz) on the device and
@@ -474,6 +524,13 @@ def run_ours(args):
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(),
                                     "kind": "reference", "sample": f"failed: {exc}"}
     pb.close()
+    if rank == 0 and ws == 1 and not args.no_reference_gpu:
+        torch.cuda.empty_cache()
+        try:
+            line["reference_gpu"] = reference_gpu_sample(wl)
+        except Exception as exc:  # the baseline must not hide our own number
+            line["reference_gpu"] = {"value": None, "unit": UNIT, "kind": "reference",
+                                     "sample": f"failed: {exc}"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -714,6 +771,8 @@ def main(argv=None):
                         "rates of the previous one on two streams (0: one stream, kernels in sequence)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-reference-gpu", action="store_true",
+                   help="skip the sample of ARGOT's own GPU kernels built for sm_100a")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--ref-seconds", type=float, default=15.0)
     args = p.parse_args(argv)

@@ -1,9 +1,12 @@
-"""Build recipes for the two CPU checkers (test infrastructure only).
+"""Build recipes for the checkers and baselines (test infrastructure only).
 
 1. O1, the parity oracle: ARGOT's own hot-path C, compiled unmodified from the
    reference tree, one shared library per mesh edge, into
    ``oracle/_ref/libargot_ref_n<EDGE>.so``.
-2. The restatement (``oracle/argot_oracle.c``, ref-order FP32/FP64 functions and
+2. The reference's GPU entry points of this path compiled for sm_100a
+   (``build_ref_gpu``, ``oracle/_ref/libargot_refgpu_n<EDGE>.so``): the
+   reference-GPU baseline of the benchmark.
+3. The restatement (``oracle/argot_oracle.c``, ref-order FP32/FP64 functions and
    the FP64 precision oracle) into ``oracle/_build/libargot_oracle.so``.
 
 Both directories are git-ignored; the built libraries travel with the working
@@ -40,8 +43,10 @@ from __future__ import annotations
 import argparse
 import os
 import re
+import shutil
 import subprocess
 import sys
+import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_OUT = os.path.join(HERE, "_ref")
@@ -67,6 +72,8 @@ SOURCES = [
 ]
 
 EDGES = (16, 32, 48, 64, 96, 128, 192, 256)
+# the reference's GPU build: the test problem and the benchmark workloads
+GPU_EDGES = (16, 64, 128, 192, 256)
 
 FLAGS = ["-D__HELIUM__", "-D__PHOTON_CONSERVING__", "-D__RADIATION_TRANSFER__",
          "-D__ARGOT_PROFILE__"]
@@ -134,6 +141,80 @@ def build_ref(edge: int, ref: str = DEFAULT_REF, fast_math: bool = False,
     return out
 
 
+def refgpu_lib_path(edge: int) -> str:
+    return os.path.join(REF_OUT, f"libargot_refgpu_n{edge}.so")
+
+
+# the reference's GPU entry points for this path and their pinned allocators
+GPU_SOURCES = ["calc_optical_depth_cuda.cu", "calc_photoion_rate_cuda.cu", "allocate_pinned_segment.cu"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise FileNotFoundError("nvcc not found")
+
+
+def build_ref_gpu(edge: int, ref: str = DEFAULT_REF, verbose: bool = False) -> str:
+    """ARGOT's own GPU entry points for this path (GPU_SOURCES), compiled
+    unmodified for sm_100a with the reference Makefile's nvcc flags
+    (``src/Makefile:208``: ``-use_fast_math -O3``), linked with the CPU
+    reference (SOURCES, which build the rays) and our glue
+    (``ref_driver.c``, ``ref_gpu_driver.cu``) into
+    ``oracle/_ref/libargot_refgpu_n<EDGE>.so``.
+
+    nvcc cannot take ``-I-`` (CUDA's own headers need their directory's
+    quoted includes), so the reference's ``src/`` is copied to a temporary
+    directory outside the repository, its ``run_param.h`` replaced by the
+    patched one, compiled there and deleted: nothing of the reference is
+    kept but the library."""
+    src_dir = os.path.join(ref, "src")
+    if not os.path.isdir(src_dir):
+        raise FileNotFoundError(f"reference sources not found at {src_dir}")
+    os.makedirs(REF_OUT, exist_ok=True)
+    out = refgpu_lib_path(edge)
+    tmp = tempfile.mkdtemp(prefix="argot_refgpu_")
+    try:
+        tsrc = os.path.join(tmp, "src")
+        shutil.copytree(src_dir, tsrc, ignore=shutil.ignore_patterns("*.o", "*.a", "*.so"))
+        with open(os.path.join(src_dir, "run_param.h")) as f:
+            text = patched_run_param(f.read(), edge)
+        with open(os.path.join(tsrc, "run_param.h"), "w") as f:
+            f.write(text)
+        inc = ["-I" + os.path.join(HERE, "shim"), "-I" + tsrc, "-I" + os.path.join(tsrc, "prim_chem")]
+        objs = []
+
+        def run(cmd):
+            if verbose:
+                print(" ".join(cmd))
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                sys.stderr.write(r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, cmd)
+
+        for i, name in enumerate(SOURCES + ["ref_driver.c"]):
+            path = os.path.join(HERE, name) if name == "ref_driver.c" else os.path.join(tsrc, name)
+            o = os.path.join(tmp, f"c{i}.o")
+            run([_cc(), "-O2", "-std=gnu99", "-fopenmp", "-fPIC", "-w", "-fno-strict-aliasing",
+                 "-ffp-contract=off", *FLAGS, *inc, "-c", path, "-o", o])
+            objs.append(o)
+        gpu_flags = ["-gencode", "arch=compute_100a,code=sm_100a", "-use_fast_math", "-O3",
+                     "-Xcompiler", "-fPIC", "-w", *FLAGS, "-D__USE_GPU__", "-D__USE_GPU_ARGOT__", *inc]
+        for i, name in enumerate(GPU_SOURCES + ["ref_gpu_driver.cu"]):
+            path = os.path.join(HERE, name) if name == "ref_gpu_driver.cu" else os.path.join(tsrc, name)
+            o = os.path.join(tmp, f"g{i}.o")
+            run([_nvcc(), *gpu_flags, "-c", path, "-o", o])
+            objs.append(o)
+        run([_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", out, *objs,
+             "-cudart", "static", "-Xcompiler", "-fopenmp", "-Xlinker", "--no-undefined",
+             "-Xlinker", "--exclude-libs,ALL", "-Xlinker", "-Bsymbolic", "-lm",
+             "-lpthread", "-ldl", "-lrt"])
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return out
+
+
 def build_oracle(verbose: bool = False) -> str:
     os.makedirs(ORC_OUT, exist_ok=True)
     out = oracle_lib_path()
@@ -155,6 +236,9 @@ def build_all(edges=EDGES, ref: str = DEFAULT_REF, verbose: bool = False):
         built.append(build_ref(64, ref, True, verbose))
         built.append(build_ref(16, ref, False, verbose, isolated=True))
         built.append(build_ref(32, ref, False, verbose, isolated=True))
+        import concurrent.futures as cf
+        with cf.ThreadPoolExecutor(max_workers=min(len(GPU_EDGES), os.cpu_count() or 1)) as ex:
+            built += list(ex.map(lambda e: build_ref_gpu(e, ref, verbose), GPU_EDGES))
     return built
 
 

@@ -154,12 +154,13 @@ class RefLib:
 
     _cache: dict = {}
 
-    def __init__(self, edge: int, fast_math: bool = False, isolated: bool = False):
-        path = _build.ref_lib_path(edge, fast_math, isolated)
-        if not os.path.exists(path):
-            if not _build.reference_available():
-                raise FileNotFoundError(f"{path} missing and the reference is absent")
-            _build.build_ref(edge, fast_math=fast_math, isolated=isolated)
+    def __init__(self, edge: int, fast_math: bool = False, isolated: bool = False, path: str = None):
+        if path is None:
+            path = _build.ref_lib_path(edge, fast_math, isolated)
+            if not os.path.exists(path):
+                if not _build.reference_available():
+                    raise FileNotFoundError(f"{path} missing and the reference is absent")
+                _build.build_ref(edge, fast_math=fast_math, isolated=isolated)
         # each edge is a distinct library with its own static state
         self.lib = L = C.CDLL(path, mode=C.RTLD_LOCAL)
         self.edge = edge
@@ -313,3 +314,59 @@ class RefLib:
                                    np.ascontiguousarray(spectra, np.float64),
                                    np.ascontiguousarray(tau3, np.float32), C.byref(wall))
         return wall.value
+
+
+class RefGpu(RefLib):
+    """ARGOT's own GPU entry points (calc_optical_depth_cuda,
+    calc_photoion_rate_cuda, zero_out_photoion_rate_cuda) compiled for
+    sm_100a with the reference's nvcc flags, with the CPU reference that
+    builds their rays (``oracle/ref_gpu_driver.cu``).  Needs a GPU."""
+
+    def __init__(self, edge: int):
+        path = _build.refgpu_lib_path(edge)
+        if not os.path.exists(path):
+            if not _build.reference_available():
+                raise FileNotFoundError(f"{path} missing and the reference is absent")
+            _build.build_ref_gpu(edge)
+        super().__init__(edge, path=path)
+        L = self.lib
+        L.refgpu_edge.restype = C.c_int
+        L.refgpu_init.restype = C.c_int
+        L.refgpu_zero_rates.restype = C.c_int
+        L.refgpu_get_rates.argtypes = [_f32p]
+        L.refgpu_get_rates.restype = C.c_int
+        L.refgpu_run_range.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_uint64,
+                                       _f64p]
+        L.refgpu_run_range.restype = C.c_int
+        assert L.refgpu_edge() == edge
+
+    def upload(self):
+        """mesh and run parameters to the device (after set_mesh and
+        set_sources)"""
+        rc = self.lib.refgpu_init()
+        assert rc == 0, f"refgpu_init: {rc}"
+
+    def zero_rates_gpu(self):
+        assert self.lib.refgpu_zero_rates() == 0
+
+    def rates_gpu(self):
+        out = np.zeros((6, self.edge ** 3), np.float32)
+        assert self.lib.refgpu_get_rates(out) == 0
+        return out
+
+    def run_range_gpu(self, im0, im1, kernel_reps=0, want=()):
+        """the reference's GPU path over target cells [im0, im1); returns the
+        counts and timings of refgpu_run_range (and the segment end points
+        and stitched columns when asked)"""
+        nray = self.count_rays(im0, im1)
+        seg = np.zeros((nray, 6), np.float32) if "seg" in want else None
+        tau = np.zeros((nray, 3), np.float32) if "tau" in want else None
+        out = np.zeros(10, np.float64)
+        rc = self.lib.refgpu_run_range(im0, im1, int(kernel_reps), _vp(seg), _vp(tau), nray, out)
+        assert rc == 0, f"refgpu_run_range: {rc}"
+        return dict(nray=int(out[0]), nseg=int(out[1]), setup_s=out[2], march_s=out[3], accum_s=out[4],
+                    rates_s=out[5], march_kernel_ms=out[6], rate_kernel_ms=out[7], groups=int(out[8]),
+                    seg=seg, tau=tau)
+
+    def close(self):
+        self.lib.refgpu_free()

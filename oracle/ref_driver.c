@@ -260,6 +260,51 @@ uint64_t ref_count_rays(int im_start, int im_end, uint64_t *per_cell)
   return total;
 }
 
+/* End of the group of target cells that starts at im: grown while its ray
+ * count stays within MAX_NRAY_PER_TARGET, as calc_ARGOT_part does; *nray
+ * receives the group's ray count. */
+int ref_next_group(int im, int im_end, uint64_t *nray)
+{
+  const uint64_t max_rays = (uint64_t)MAX_NRAY_PER_TARGET;
+  uint64_t n = 0;
+  int ge = im;
+  while (ge < im_end) {
+    uint64_t c = ref_count_rays(ge, ge + 1, NULL);
+    if (ge > im && n + c > max_rays) break;
+    n += c;
+    ge++;
+  }
+  *nray = n;
+  return ge;
+}
+
+/* The first half of calc_ARGOT_part for one group [im, ge) whose ray count
+ * is nray (from ref_next_group), for a caller that marches and integrates
+ * with other functions (the reference's GPU entry points): the group's light
+ * rays into ray[nray], their segments counted (returns nseg); then
+ * ref_assign_group fills seg[nseg]. */
+int64_t ref_setup_group(int im, int ge, struct light_ray *ray, uint64_t nray)
+{
+  if (!g_have_tree) return -1;
+  g_run.nray = nray;
+  setup_light_ray_range(im, ge, ray, 1, g_clist, g_src, g_index, &g_run);
+  count_ray_segment(ray, &g_run, &g_omp);
+  return (int64_t)g_run.nseg;
+}
+
+void ref_assign_group(struct light_ray *ray, struct ray_segment *seg)
+{
+  assign_ray_segment(ray, seg, &g_run, &g_mpi, &g_omp);
+}
+
+void ref_accum_group(struct light_ray *ray, struct ray_segment *seg)
+{
+  accum_optical_depth(ray, seg, &g_run, &g_omp);
+}
+
+struct run_param *ref_run_param(void) { return &g_run; }
+struct fluid_mesh *ref_mesh(void) { return g_mesh; }
+
 /*
  * Runs the reference's hot path over target cells [im_start, im_end), in
  * groups whose ray count stays within the reference's MAX_NRAY_PER_TARGET
@@ -277,21 +322,13 @@ int64_t ref_run_range(int im_start, int im_end, int do_photo,
   if (!g_have_tree) return -1;
   uint64_t nray_total = 0;
   double t_setup = 0, t_march = 0, t_accum = 0, t_photo = 0;
-  const uint64_t max_rays = (uint64_t)MAX_NRAY_PER_TARGET;
   struct light_ray *ray = NULL;
   uint64_t ray_cap = 0;
 
   int im = im_start;
   while (im < im_end) {
-    /* grow the group while the ray count fits */
     uint64_t nray = 0;
-    int ge = im;
-    while (ge < im_end) {
-      uint64_t c = ref_count_rays(ge, ge + 1, NULL);
-      if (ge > im && nray + c > max_rays) break;
-      nray += c;
-      ge++;
-    }
+    const int ge = ref_next_group(im, im_end, &nray);
     double t0 = now_s();
     if (nray > ray_cap) {
       free(ray);
