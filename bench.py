@@ -527,7 +527,7 @@ def run_ours(args):
     if rank == 0 and ws == 1 and not args.no_reference_gpu:
         torch.cuda.empty_cache()
         try:
-            line["reference_gpu"] = reference_gpu_sample(wl)
+            line["reference_gpu"] = reference_gpu_sample(wl, target_rays=args.reference_gpu_rays)
         except Exception as exc:  # the baseline must not hide our own number
             line["reference_gpu"] = {"value": None, "unit": UNIT, "kind": "reference",
                                      "sample": f"failed: {exc}"}
@@ -773,10 +773,21 @@ def main(argv=None):
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-reference-gpu", action="store_true",
                    help="skip the sample of ARGOT's own GPU kernels built for sm_100a")
+    p.add_argument("--reference-gpu-only", action="store_true",
+                   help="run only the reference-GPU sample of the config and print it (a profiling case)")
+    p.add_argument("--reference-gpu-rays", type=int, default=2_000_000,
+                   help="rays in the reference-GPU sample")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--ref-seconds", type=float, default=15.0)
     args = p.parse_args(argv)
-    if args.impl == "reference":
+    if args.reference_gpu_only:
+        wl = make_workload(args.config, 0)
+        if isinstance(wl, list):
+            wl = max(wl, key=lambda w: (w.edge, w.nsrc))
+        print(json.dumps({"config": wl.name,
+                          "reference_gpu": reference_gpu_sample(wl, target_rays=args.reference_gpu_rays)}),
+              flush=True)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.config.startswith("batched"):
         run_batched(args)
