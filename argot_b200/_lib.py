@@ -67,6 +67,14 @@ SIGNATURES = {
     "accum_optical_depth": (None, [vp, vp, vp, vp]),
     "argot_b200_set_dropin_march_mode": (i32, [i32]),
     "smooth_photoion_rate": (None, [vp, vp, vp, vp, vp]),
+    "calc_diffuse_photon_radiation": (None, [vp, vp, vp, vp, vp, vp, vp]),
+    "argot_b200_art_angle_table": (i32, [i32, vp, vp, vp]),
+    "argot_b200_art_step_factors": (None, [vp]),
+    "argot_b200_art_create": (i32, [vp, vp, i32, vp, vp]),
+    "argot_b200_art_destroy": (None, [vp]),
+    "argot_b200_art_num_angles": (i32, [vp]),
+    "argot_b200_art_workspace": (u64, [GP, i32]),
+    "argot_b200_art_rates": (i32, [vp, GP, f64, vp, vp, vp, i32, vp, vp]),
     "argot_b200_set_dropin_smooth_faces": (i32, [i32]),
     "argot_b200_pack_fields": (i32, [GP, vp, vp, vp, vp, vp, vp]),
     "argot_b200_pack_fluid_mesh": (i32, [GP, vp, vp, vp]),

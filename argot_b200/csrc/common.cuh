@@ -56,6 +56,12 @@ struct RateTables {
 // the rate kernels (photoion.cu), once per device.
 int ensure_tables(int device);
 
+// Photo-ionisation cross sections [cm^2] at nu in units of the HI Lyman
+// limit (prim_chem/cross_section.c:20-53).
+double sigma_hi(double nu);
+double sigma_hei(double nu);
+double sigma_heii(double nu);
+
 // Host copies of the tables (computed with the reference's formulas).
 void host_tables(double *nu, float *cs3);
 // Weights of the six rate integrals per bin (6 x 256): sigma_s(nu) and

@@ -45,17 +45,17 @@ GridDev make_grid(const argot_b200_grid &g) {
 // units of the HI Lyman limit), bin centres (source.c:38-53; the bin width
 // is divided by a float-converted 256 as there).  Cross sections: the
 // analytic fits of prim_chem/cross_section.c:20-53 for HI, HeI and HeII.
-static double sigma_hi(double nu) {
+double sigma_hi(double nu) {
   if (nu < kThrHI) return 0.0;
   double e = std::sqrt(nu - kThrHI);
   return 6.3e-18 / (nu * nu * nu * nu) * std::exp(4.0 - 4.0 * std::atan(e) / e) /
          (1.0 - std::exp(-2.0 * kPi / e));
 }
-static double sigma_hei(double nu) {
+double sigma_hei(double nu) {
   if (nu < kThrHeI) return 0.0;
   return 7.83e-18 * (1.66 * std::pow(nu / kThrHeI, -2.05) - 0.66 * std::pow(nu / kThrHeI, -3.05));
 }
-static double sigma_heii(double nu) {
+double sigma_heii(double nu) {
   if (nu < kThrHeII) return 0.0;
   double e = std::sqrt(nu / kThrHeII - 1.0);
   return 6.3e-18 * 256.0 / (nu * nu * nu * nu) * std::exp(4.0 - 4.0 * std::atan(e) / e) /

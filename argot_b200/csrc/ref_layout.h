@@ -125,6 +125,24 @@ struct cuda_mem_space {
   float *optical_depth_dev, *dtime_dev, *diff_chem_dev, *diff_uene_dev;
 };
 
+// src/diffuse_photon/diffuse_photon.h:76-79,130-154 (GPU build: the host
+// parameters carry no radiation mesh)
+struct angle_info {
+  float xovr, yovr, zovr;
+  short base_id, corner_id;
+};
+struct step_func_factor {
+  float HI[2], HeI[2], HeII[2];
+};
+struct host_diffuse_param {
+  int corner_id_num[8];
+  step_func_factor *step_fact;
+  angle_info *angle;
+};
+
+static_assert(sizeof(angle_info) == 16, "angle_info layout");
+static_assert(sizeof(step_func_factor) == 24, "step_func_factor layout");
+static_assert(sizeof(host_diffuse_param) == 48, "host_diffuse_param layout");
 static_assert(sizeof(prim_chem) == 52, "prim_chem layout");
 static_assert(sizeof(fluid_mesh) == 156, "fluid_mesh layout");
 static_assert(offsetof(fluid_mesh, chem) == 44, "fluid_mesh.chem");

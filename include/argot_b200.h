@@ -413,6 +413,56 @@ ARGOT_B200_API int argot_b200_batch_graph_launch(argot_b200_batch *b, void *stre
 ARGOT_B200_API int argot_b200_batch_tune(argot_b200_batch *b, int reps, argot_b200_batch_config *best,
                                          float *best_ms, void *stream);
 
+/* ---- ART diffuse radiation (src/diffuse_photon, one rank) -------------- */
+/* Recombination photons along long characteristics in 12 nside^2 HEALPix
+ * directions (calc_diffuse_photon_radiation.c, ray_tracing.c,
+ * calc_rmesh_data.c, calc_GH_tot.c): per direction every cell of the start
+ * face launches a ray, which wraps through the side faces with its
+ * intensity reset (one isolated rank) and ends at the far face; the mean
+ * over directions of the per-cell ionisation and heating rates is added to
+ * the six rate planes. */
+typedef struct argot_b200_art argot_b200_art;
+/* The reference's angle table for nside (set_angle_info + sort_angle_id,
+ * src/diffuse_photon/set_angle.c): dir3[3 n] direction cosines (float, with
+ * the +-1e-31 guard), base_corner2[2 n] start face (0..5) and octant, in
+ * processing order; corner_count8 (optional) angles per octant.  Returns
+ * n = 12 nside^2 (or a negative code). */
+ARGOT_B200_API int argot_b200_art_angle_table(int nside, float *dir3, int *base_corner2, int *corner_count8);
+/* set_step_func_factor (src/diffuse_photon/set_step_func_factor.c):
+ * ionisation and heating factors of HI, HeI, HeII */
+ARGOT_B200_API void argot_b200_art_step_factors(float *step6);
+/* a direction set on the current device (from argot_b200_art_angle_table or
+ * the caller's own table in the same layout) */
+ARGOT_B200_API int argot_b200_art_create(const float *dir3, const int *base_corner2, int nang, const float *step6,
+                                         argot_b200_art **out);
+ARGOT_B200_API void argot_b200_art_destroy(argot_b200_art *a);
+ARGOT_B200_API int argot_b200_art_num_angles(const argot_b200_art *a);
+/* device workspace bytes for argot_b200_art_rates with angles_per_pass */
+ARGOT_B200_API uint64_t argot_b200_art_workspace(const argot_b200_grid *g, int angles_per_pass);
+/* fields8_dev: 8 planes of ncell floats: dens, fHI, fHII, fHeI, fHeII,
+ * fHeIII, felec, uene (fluid_mesh dens, prev_chem fractions, prev_uene);
+ * uenetok: run_param.uenetok (uene -> T).  ADDS the diffuse rates to
+ * rates6_dev (layout of rates6 above).  The grid is one rank covering the
+ * box.  crossings_dev (optional) is added the number of ray-cell steps.
+ * Device errors (a ray beyond its step bound) are reported by
+ * argot_b200_check_device_error. */
+ARGOT_B200_API int argot_b200_art_rates(const argot_b200_art *a, const argot_b200_grid *g, double uenetok,
+                                        const float *fields8_dev, float *rates6_dev, void *work_dev,
+                                        int angles_per_pass, unsigned long long *crossings_dev, void *stream);
+
+/* Replaces src/diffuse_photon/calc_diffuse_photon_radiation.c:37-128 as built
+ * with __USE_GPU__ (src/diffuse_photon/diffuse_prototype.h:27) on a single
+ * rank: the caller's angle table and step factors (hd_param, filled by its
+ * setup_diffuse_photon), the mesh of cuda_mem[0].mesh_dev, whose
+ * prev_chem.{Gamma,Heat}{HI,HeI,HeII} receive the diffuse rates (added).
+ * mesh, cd_param and this_omp are not used. */
+struct host_diffuse_param;
+struct cuda_diffuse_param;
+ARGOT_B200_API void calc_diffuse_photon_radiation(struct fluid_mesh *mesh, struct run_param *this_run,
+                                                  struct cuda_mem_space *cuda_mem, struct cuda_param *this_cuda,
+                                                  struct host_diffuse_param *hd_param,
+                                                  struct cuda_diffuse_param *cd_param, struct omp_param *this_omp);
+
 /* Reads and clears the device-side error flag of the current device (set
  * when a march exceeded its step bound, which only non-finite input can
  * cause); synchronises `stream`.  Returns 0 or ARGOT_B200_EDEVICE. */

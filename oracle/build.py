@@ -29,11 +29,19 @@ what it calls:
   source.c, cross_section.c, prim_chem/cross_section.c
                             (A5 tables)
   mpi_rank.c, timing.c      (helpers)
+  smooth_photoion_rate.c, output_data.c, input_data.c, make_directory.c
+                            (smoothing, file formats)
+  diffuse_photon/*.c        (ART diffuse radiation, CPU build)
 
-plus two files of ours: ``oracle/shim/mpi.h`` (single-rank MPI) and
-``oracle/ref_driver.c`` (flat-array glue).  Flags follow the reference's
+plus files of ours: ``oracle/shim/mpi.h`` (single-rank MPI),
+``oracle/shim/chealpix.h`` (HEALPix pix2ang_ring, which chealpix would
+provide) and ``oracle/ref_driver.c`` (flat-array glue).  ``-fgnu89-inline``
+gives the diffuse sources' plain ``inline`` functions an external
+definition, as the compilers the reference was written for did.  Flags follow the reference's
 ``src/Makefile`` switches for this path (``-D__HELIUM__ -D__PHOTON_CONSERVING__
--D__RADIATION_TRANSFER__ -D__ARGOT_PROFILE__``), ``-O2`` without
+-D__RADIATION_TRANSFER__ -D__ARGOT_PROFILE__``, and the Makefile's default
+``-D__HEATCOOL__``, which on these sources only sets the diffuse-radiation
+step-function range), ``-O2`` without
 ``-ffast-math`` (the parity build); ``--fast-math`` adds the reference's own
 ``-ffast-math`` for the spread study.  ``-ffp-contract=off`` pins IEEE
 single-operation rounding (the x86-64 baseline target has no FMA anyway).
@@ -69,6 +77,18 @@ SOURCES = [
     "output_data.c",
     "input_data.c",
     "make_directory.c",
+    # ART diffuse radiation (CPU build)
+    "diffuse_photon/set_angle.c",
+    "diffuse_photon/set_start_pos.c",
+    "diffuse_photon/set_step_func_factor.c",
+    "diffuse_photon/setup_diffuse.c",
+    "diffuse_photon/init_hd_param.c",
+    "diffuse_photon/ray_tracing.c",
+    "diffuse_photon/calc_rmesh_data.c",
+    "diffuse_photon/calc_GH_tot.c",
+    "diffuse_photon/calc_diffuse_photon_radiation.c",
+    "diffuse_photon/operation_mpi_window.c",
+    "diffuse_photon/diffuse_photon_mpi.c",
 ]
 
 EDGES = (16, 32, 48, 64, 96, 128, 192, 256)
@@ -76,7 +96,7 @@ EDGES = (16, 32, 48, 64, 96, 128, 192, 256)
 GPU_EDGES = (16, 64, 128, 192, 256)
 
 FLAGS = ["-D__HELIUM__", "-D__PHOTON_CONSERVING__", "-D__RADIATION_TRANSFER__",
-         "-D__ARGOT_PROFILE__"]
+         "-D__ARGOT_PROFILE__", "-D__HEATCOOL__"]
 
 
 def _cc() -> str:
@@ -120,7 +140,7 @@ def build_ref(edge: int, ref: str = DEFAULT_REF, fast_math: bool = False,
     with open(os.path.join(inc, "run_param.h"), "w") as f:
         f.write(text)
     out = ref_lib_path(edge, fast_math, isolated)
-    cmd = [_cc(), "-O2", "-std=gnu99", "-fopenmp", "-fPIC", "-shared", "-w",
+    cmd = [_cc(), "-O2", "-std=gnu99", "-fgnu89-inline", "-fopenmp", "-fPIC", "-shared", "-w",
            "-fno-strict-aliasing", "-ffp-contract=off"]
     if fast_math:
         cmd.append("-ffast-math")
@@ -128,7 +148,8 @@ def build_ref(edge: int, ref: str = DEFAULT_REF, fast_math: bool = False,
     if isolated:
         cmd.append("-D__ISOLATED__")
     cmd += ["-I" + inc, "-I-", "-I" + os.path.join(HERE, "shim"),
-            "-I" + src_dir, "-I" + os.path.join(src_dir, "prim_chem")]
+            "-I" + src_dir, "-I" + os.path.join(src_dir, "prim_chem"),
+            "-I" + os.path.join(src_dir, "diffuse_photon")]
     cmd += [os.path.join(src_dir, s) for s in SOURCES]
     cmd += [os.path.join(HERE, "ref_driver.c"), "-o", out, "-lm",
             "-Wl,--no-undefined"]
@@ -182,7 +203,8 @@ def build_ref_gpu(edge: int, ref: str = DEFAULT_REF, verbose: bool = False) -> s
             text = patched_run_param(f.read(), edge)
         with open(os.path.join(tsrc, "run_param.h"), "w") as f:
             f.write(text)
-        inc = ["-I" + os.path.join(HERE, "shim"), "-I" + tsrc, "-I" + os.path.join(tsrc, "prim_chem")]
+        inc = ["-I" + os.path.join(HERE, "shim"), "-I" + tsrc, "-I" + os.path.join(tsrc, "prim_chem"),
+               "-I" + os.path.join(tsrc, "diffuse_photon")]
         objs = []
 
         def run(cmd):
@@ -196,7 +218,7 @@ def build_ref_gpu(edge: int, ref: str = DEFAULT_REF, verbose: bool = False) -> s
         for i, name in enumerate(SOURCES + ["ref_driver.c"]):
             path = os.path.join(HERE, name) if name == "ref_driver.c" else os.path.join(tsrc, name)
             o = os.path.join(tmp, f"c{i}.o")
-            run([_cc(), "-O2", "-std=gnu99", "-fopenmp", "-fPIC", "-w", "-fno-strict-aliasing",
+            run([_cc(), "-O2", "-std=gnu99", "-fgnu89-inline", "-fopenmp", "-fPIC", "-w", "-fno-strict-aliasing",
                  "-ffp-contract=off", *FLAGS, *inc, "-c", path, "-o", o])
             objs.append(o)
         gpu_flags = ["-gencode", "arch=compute_100a,code=sm_100a", "-use_fast_math", "-O3",

@@ -189,6 +189,12 @@ class RefLib:
         L.ref_read_files.argtypes = [C.c_char_p, C.c_char_p, _f32p, _f32p, _f32p, _f32p, _i32p, _f32p,
                                      _f32p, _f64p, C.c_int64]
         L.ref_read_files.restype = C.c_int64
+        L.ref_art_init.argtypes = [C.c_double]
+        L.ref_art_init.restype = C.c_int
+        L.ref_art_table.argtypes = [_f32p, _i32p, _i32p, _f32p]
+        L.ref_art_set_mesh.argtypes = [_f32p]
+        L.ref_art_run.argtypes = [_f32p]
+        L.ref_art_run.restype = C.c_double
         assert L.ref_mesh_edge() == edge
         self.isolated = isolated
 
@@ -292,6 +298,33 @@ class RefLib:
         assert n == nray, (n, nray)
         return dict(tgt=tgt, src=src, seg=seg, tau=tau, spec_sum=ssum, spectra=spectra,
                     times=times, nray=nray)
+
+    # ---- ART diffuse radiation (src/diffuse_photon, CPU build)
+    def art_init(self, uenetok):
+        """setup_diffuse_photon: the angle table and step-function factors;
+        returns the number of angles (12 N_SIDE^2)"""
+        self.n_ang = int(self.lib.ref_art_init(float(uenetok)))
+        return self.n_ang
+
+    def art_table(self):
+        n = self.n_ang
+        d = np.zeros((n, 3), np.float32)
+        bc = np.zeros((n, 2), np.int32)
+        c8 = np.zeros(8, np.int32)
+        st = np.zeros(6, np.float32)
+        self.lib.ref_art_table(d, bc, c8, st)
+        return d, bc, c8, st
+
+    def art_set_mesh(self, planes8):
+        """dens, fHI, fHII, fHeI, fHeII, fHeIII, felec, prev_uene"""
+        self.lib.ref_art_set_mesh(np.ascontiguousarray(planes8, np.float32).reshape(8, -1))
+
+    def art_run(self):
+        """calc_diffuse_photon_radiation: the six diffuse rate planes and the
+        wall time"""
+        out = np.zeros((6, self.edge ** 3), np.float32)
+        t = self.lib.ref_art_run(out)
+        return out, t
 
     def march_segments(self, pos6):
         pos6 = np.ascontiguousarray(pos6, np.float32)

@@ -33,6 +33,8 @@
 #include "tree_clist.h"
 #include "mpi_param.h"
 #include "omp_param.h"
+#include "diffuse_photon.h"
+#include "diffuse_prototype.h"
 
 static struct run_param g_run;
 static struct fluid_mesh *g_mesh = NULL;
@@ -560,4 +562,72 @@ int64_t ref_read_files(const char *mesh_file, const char *src_file, float *dens,
   }
   free(s);
   return n;
+}
+
+
+/* ------------------------------------------------------------------------
+ * ART diffuse radiation (src/diffuse_photon, CPU build, single rank): the
+ * angle table and step-function factors of setup_diffuse_photon
+ * (setup_diffuse.c:8-15), and calc_diffuse_photon_radiation
+ * (calc_diffuse_photon_radiation.c:37-128), which adds the diffuse rates to
+ * mesh[].prev_chem.  Its inputs are the mesh's prev_chem fractions, dens
+ * and prev_uene.
+ */
+static struct host_diffuse_param g_hd;
+static int g_have_hd = 0;
+
+int ref_art_init(double uenetok)
+{
+  if (!g_have_hd) { init_hd_param(&g_hd); g_have_hd = 1; }
+  g_run.uenetok = uenetok;
+  setup_diffuse_photon(&g_hd, &g_run);
+  return N_ANG;
+}
+
+/* dir3[3 N_ANG] (xovr, yovr, zovr), bc2[2 N_ANG] (base_id, corner_id) in the
+ * processing order, corner8 the angles per corner, step6 (HI, HeI, HeII x
+ * ionisation, heating) */
+void ref_art_table(float *dir3, int *bc2, int *corner8, float *step6)
+{
+  for (int i = 0; i < N_ANG; i++) {
+    dir3[3 * i + 0] = g_hd.angle[i].xovr;
+    dir3[3 * i + 1] = g_hd.angle[i].yovr;
+    dir3[3 * i + 2] = g_hd.angle[i].zovr;
+    bc2[2 * i + 0] = g_hd.angle[i].base_id;
+    bc2[2 * i + 1] = g_hd.angle[i].corner_id;
+  }
+  for (int c = 0; c < 8; c++) corner8[c] = g_hd.corner_id_num[c];
+  step6[0] = g_hd.step_fact->HI[0]; step6[1] = g_hd.step_fact->HI[1];
+  step6[2] = g_hd.step_fact->HeI[0]; step6[3] = g_hd.step_fact->HeI[1];
+  step6[4] = g_hd.step_fact->HeII[0]; step6[5] = g_hd.step_fact->HeII[1];
+}
+
+/* planes8: dens, fHI, fHII, fHeI, fHeII, fHeIII, felec, prev_uene */
+void ref_art_set_mesh(const float *planes8)
+{
+  const uint64_t n = (uint64_t)NMESH_LOCAL;
+  for (uint64_t i = 0; i < n; i++) {
+    memset(&g_mesh[i], 0, sizeof(struct fluid_mesh));
+    g_mesh[i].dens = planes8[0 * n + i];
+    g_mesh[i].prev_chem.fHI = planes8[1 * n + i];
+    g_mesh[i].prev_chem.fHII = planes8[2 * n + i];
+    g_mesh[i].prev_chem.fHeI = planes8[3 * n + i];
+    g_mesh[i].prev_chem.fHeII = planes8[4 * n + i];
+    g_mesh[i].prev_chem.fHeIII = planes8[5 * n + i];
+    g_mesh[i].prev_chem.felec = planes8[6 * n + i];
+    g_mesh[i].prev_uene = planes8[7 * n + i];
+    g_mesh[i].chem = g_mesh[i].prev_chem;
+  }
+}
+
+/* the diffuse rates alone (prev_chem rates zeroed first) into out6; returns
+ * the wall time of calc_diffuse_photon_radiation */
+double ref_art_run(float *out6)
+{
+  zero_out_photoion_rate(g_mesh, &g_run);
+  const double t0 = now_s();
+  calc_diffuse_photon_radiation(g_mesh, &g_run, &g_hd, &g_omp);
+  const double t1 = now_s();
+  ref_get_rates(out6);
+  return t1 - t0;
 }

@@ -2,8 +2,9 @@
  * Single-rank stand-in for the subset of MPI that ARGOT's ray-tracing hot
  * path calls (test infrastructure only: it lets the reference's own
  * calc_optical_depth.c / accum_optical_depth.c / assign_ray_segment.c /
- * calc_photoion_rate.c / smooth_photoion_rate.c be compiled and run on one
- * host without an MPI library).
+ * calc_photoion_rate.c / smooth_photoion_rate.c and the diffuse-radiation
+ * sources of src/diffuse_photon be compiled and run on one host without an
+ * MPI library).
  *
  * Semantics with one rank (rank 0 of a world of size 1):
  *  - MPI_Win_create records the window base and displacement unit, so that
@@ -122,5 +123,27 @@ static inline int MPI_Accumulate(const void *o, int oc, MPI_Datatype ot, int ran
   }
   return MPI_SUCCESS;
 }
+
+/* memory for windows, and the struct datatype of the diffuse-radiation
+ * code (src/diffuse_photon/diffuse_photon_mpi.c): one block of `count`
+ * elements of one basic type, sized here */
+static inline int MPI_Alloc_mem(MPI_Aint size, MPI_Info info, void *baseptr)
+{
+  (void)info;
+  *(void **)baseptr = malloc((size_t)size);
+  return MPI_SUCCESS;
+}
+static inline int MPI_Free_mem(void *base) { free(base); return MPI_SUCCESS; }
+static inline int MPI_Type_struct(int n, const int *blocklen, const MPI_Aint *disp,
+                                  const MPI_Datatype *types, MPI_Datatype *out)
+{
+  size_t bytes = 0;
+  for (int i = 0; i < n; i++)
+    bytes = (size_t)disp[i] + (size_t)blocklen[i] * argot_shim_type_size(types[i]);
+  *out = ARGOT_SHIM_SIZED_TYPE(bytes);
+  return MPI_SUCCESS;
+}
+static inline int MPI_Type_commit(MPI_Datatype *t) { (void)t; return MPI_SUCCESS; }
+static inline int MPI_Type_free(MPI_Datatype *t) { (void)t; return MPI_SUCCESS; }
 
 #endif /* ARGOT_ORACLE_MPI_SHIM_H */
