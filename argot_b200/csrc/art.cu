@@ -22,8 +22,8 @@
 // sums stay separate as the reference needs them.  Rays of one angle are
 // parallel lines, several may cross a cell, so the accumulators take vector
 // float atomics (one 16-byte reduction per crossing).  The per-cell
-// quantities (absorption, source function) are two float4 per cell read
-// through L1.  A second kernel folds the batch's angles into the six
+// quantities (absorption, source function) are one 32-byte record per cell,
+// one 256-bit load per step.  A second kernel folds the batch's angles into the six
 // per-cell totals in angle order, as calc_GH_tot does angle after angle.
 #include <algorithm>
 #include <cmath>
@@ -55,6 +55,20 @@ struct ArtAngle {
   float ox, oy, oz;
   int base;
 };
+
+// Per-cell data of the march: absorption coefficients [cm^-1] and source
+// functions of the three frequencies in one 32-byte record, read with one
+// 256-bit load per step.
+struct __align__(32) ArtCell {
+  float a1, a2, a3, s1, s2, s3, pad0, pad1;
+};
+__device__ __forceinline__ ArtCell load_cell(const ArtCell *p) {
+  ArtCell c;
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(c.a1), "=f"(c.a2), "=f"(c.a3), "=f"(c.s1), "=f"(c.s2), "=f"(c.s3), "=f"(c.pad0), "=f"(c.pad1)
+      : "l"(p));
+  return c;
+}
 
 struct ArtGeom {
   int nx, ny, nz;
@@ -114,8 +128,7 @@ __device__ double rec_heiii_b(double t) {
 // prev_uene of fluid_mesh).
 __global__ void __launch_bounds__(256) k_art_cells(uint64_t n, const float *__restrict__ f, double denstonh,
                                                   double uenetok, float cs_hi, float cs_hei, float cs_heii,
-                                                  float4 *__restrict__ absorp, float4 *__restrict__ srcf,
-                                                  float *__restrict__ gh6) {
+                                                  ArtCell *__restrict__ cells, float *__restrict__ gh6) {
   for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < n; c += (uint64_t)gridDim.x * blockDim.x) {
     const float dens = f[c], fhi = f[n + c], fhii = f[2 * n + c], fhei = f[3 * n + c];
     const float fheii = f[4 * n + c], fheiii = f[5 * n + c], felec = f[6 * n + c], uene = f[7 * n + c];
@@ -137,8 +150,8 @@ __global__ void __launch_bounds__(256) k_art_cells(uint64_t n, const float *__re
     const double e1 = (rec_hii_a(t) - rec_hii_b(t)) * ne * nhii * kNuLeV * kThrHI * kEVtoErg / (4.0 * kPi);
     const double e2 = (rec_heii_a(t) - rec_heii_b(t)) * ne * nheii * kNuLeV * kThrHeI * kEVtoErg / (4.0 * kPi);
     const double e3 = (rec_heiii_a(t) - rec_heiii_b(t)) * ne * nheiii * kNuLeV * kThrHeII * kEVtoErg / (4.0 * kPi);
-    absorp[c] = make_float4(a1, a2, a3, 0.f);
-    srcf[c] = make_float4((float)(e1 / (double)a1), (float)(e2 / (double)a2), (float)(e3 / (double)a3), 0.f);
+    cells[c] = ArtCell{a1, a2, a3, (float)(e1 / (double)a1), (float)(e2 / (double)a2), (float)(e3 / (double)a3),
+                       0.f, 0.f};
 #pragma unroll
     for (int s = 0; s < 6; s++) gh6[s * n + c] = 0.f;
   }
@@ -170,8 +183,8 @@ __device__ __forceinline__ void att(float tau, float *et, float *em1) {
 // float4 (sum of I (1 - e^-tau) per frequency, chord length).  A ray that
 // exceeds its step bound sets *err and stops.
 __global__ void __launch_bounds__(256) k_art_trace(ArtGeom g, const ArtAngle *__restrict__ ang, int a0, int na,
-                                                  uint32_t face_max, const float4 *__restrict__ absorp,
-                                                  const float4 *__restrict__ srcf, float4 *__restrict__ acc,
+                                                  uint32_t face_max, const ArtCell *__restrict__ cells,
+                                                  float4 *__restrict__ acc,
                                                   unsigned long long *__restrict__ crossings, int *__restrict__ err) {
   const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
@@ -180,7 +193,9 @@ __global__ void __launch_bounds__(256) k_art_trace(ArtGeom g, const ArtAngle *__
     const int al = (int)(tid / face_max);
     const uint32_t r = (uint32_t)(tid % face_max);
     const ArtAngle A = ang[a0 + al];
-    // start cell on the face (set_start_pos.c:150-190)
+    // start cell on the face (set_start_pos.c:150-190); consecutive threads
+    // take consecutive cells along z where the face contains z, so that a
+    // warp's loads and reductions fall on contiguous cells
     int i0, j0, k0;
     bool ok = true;
     if (A.base <= 1) {
@@ -191,7 +206,7 @@ __global__ void __launch_bounds__(256) k_art_trace(ArtGeom g, const ArtAngle *__
       j0 = (int)(r / g.nz); k0 = (int)(r % g.nz); i0 = A.base == 2 ? 0 : g.nx - 1;
     } else {
       ok = r < (uint32_t)(g.nz * g.nx);
-      k0 = (int)(r / g.nx); i0 = (int)(r % g.nx); j0 = A.base == 4 ? 0 : g.ny - 1;
+      i0 = (int)(r / g.nz); k0 = (int)(r % g.nz); j0 = A.base == 4 ? 0 : g.ny - 1;
     }
     if (ok) {
       float x = __double2float_rn(__dadd_rn((double)g.xminl, __dmul_rn(__dadd_rn((double)i0, 0.521212345), (double)g.dx)));
@@ -242,18 +257,18 @@ __global__ void __launch_bounds__(256) k_art_trace(ArtGeom g, const ArtAngle *__
         if (rdz == rmin) iz += zn;
         rmin = __double2float_rn(__dmul_rn((double)rmin, g.lunit));
         // intensities (calc_intensity, ray_tracing.c:71-157)
-        const float4 ab = __ldg(absorp + pos), sf = __ldg(srcf + pos);
+        const ArtCell cl = load_cell(cells + pos);
         float et, em;
         float4 add;
-        att(__fmul_rn(ab.x, rmin), &et, &em);
+        att(__fmul_rn(cl.a1, rmin), &et, &em);
         add.x = i1 * em;
-        i1 = fmaf(i1, et, sf.x * em);
-        att(__fmul_rn(ab.y, rmin), &et, &em);
+        i1 = fmaf(i1, et, cl.s1 * em);
+        att(__fmul_rn(cl.a2, rmin), &et, &em);
         add.y = i2 * em;
-        i2 = fmaf(i2, et, sf.y * em);
-        att(__fmul_rn(ab.z, rmin), &et, &em);
+        i2 = fmaf(i2, et, cl.s2 * em);
+        att(__fmul_rn(cl.a3, rmin), &et, &em);
         add.z = i3 * em;
-        i3 = fmaf(i3, et, sf.z * em);
+        i3 = fmaf(i3, et, cl.s3 * em);
         add.w = rmin;
         atomicAdd(accA + pos, add);
         // leaving the box: stop at the far face, wrap through the side faces
@@ -289,42 +304,43 @@ __global__ void __launch_bounds__(256) k_art_trace(ArtGeom g, const ArtAngle *__
 }
 
 // The batch's angles, in order, into the six per-cell totals
-// (calc_GH_tot.c:178-228: the reference's double expressions on its float
-// fields).  step: ionisation and heating factors of HI, HeI, HeII.
+// (calc_GH_tot.c:178-228).  The reference evaluates each angle's terms in
+// double with six divisions; here the divisions by the cell's absorption
+// coefficients are hoisted out of the angle loop as FP32 reciprocals and
+// each angle costs one reciprocal of its chord length and FP32 FMAs, the
+// totals kept in float as the reference keeps them.  step: ionisation and
+// heating factors of HI, HeI, HeII.
 struct ArtStep {
   float f[6];
 };
 __global__ void __launch_bounds__(256) k_art_fold(uint64_t n, int na, const float4 *__restrict__ acc,
-                                                 const float4 *__restrict__ absorp, const float4 *__restrict__ srcf,
-                                                 ArtStep st, float *__restrict__ gh6) {
+                                                 const ArtCell *__restrict__ cells, ArtStep st,
+                                                 float *__restrict__ gh6) {
   for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < n; c += (uint64_t)gridDim.x * blockDim.x) {
-    const float4 ab = absorp[c], sf = srcf[c];
+    const ArtCell cl = load_cell(cells + c);
+    const float4 ab = make_float4(cl.a1, cl.a2, cl.a3, 0.f), sf = make_float4(cl.s1, cl.s2, cl.s3, 0.f);
+    const float ia1 = 1.f / ab.x, ia2 = 1.f / ab.y, ia3 = 1.f / ab.z;
+    const float c2j = (float)kRintJHI2 * ia2, c3j = (float)kRintJHI3 * ia3;
+    const float c2h = (float)kRintHHI2 * ia2, c3h = (float)kRintHHI3 * ia3;
+    const float c3ej = (float)kRintJHeI3 * ia3, c3eh = (float)kRintHHeI3 * ia3;
+    const float src_ghi = fmaf(sf.z, (float)kRintJHI3, fmaf(sf.y, (float)kRintJHI2, sf.x));
+    const float src_hhi = fmaf(sf.z, (float)kRintHHI3, fmaf(sf.y, (float)kRintHHI2, sf.x));
+    const float src_ghei = fmaf(sf.z, (float)kRintJHeI3, sf.y);
+    const float src_hhei = fmaf(sf.z, (float)kRintHHeI3, sf.y);
     float g[6];
 #pragma unroll
     for (int s = 0; s < 6; s++) g[s] = gh6[s * n + c];
-    const double s1 = sf.x, s2 = sf.y, s3 = sf.z;
-    const double src_ghi = s1 + s2 * kRintJHI2 + s3 * kRintJHI3;
-    const double src_hhi = s1 + s2 * kRintHHI2 + s3 * kRintHHI3;
-    const double src_ghei = s2 + s3 * kRintJHeI3;
-    const double src_hhei = s2 + s3 * kRintHHeI3;
-    const double src_heii = s3;
     for (int a = 0; a < na; a++) {
       const float4 v = acc[(uint64_t)a * n + c];
-      const double len = v.w;
-      const double q1 = (double)__fdiv_rn(v.x, ab.x), q2 = (double)__fdiv_rn(v.y, ab.y);
-      const double q3 = (double)__fdiv_rn(v.z, ab.z);
-      const double i2j = (double)v.y * kRintJHI2 / (double)ab.y, i3j = (double)v.z * kRintJHI3 / (double)ab.z;
-      const double i2h = (double)v.y * kRintHHI2 / (double)ab.y, i3h = (double)v.z * kRintHHI3 / (double)ab.z;
-      double ig = (q1 + i2j + i3j) / len, ih = (q1 + i2h + i3h) / len;
-      g[0] = (float)((double)g[0] + (ig + src_ghi) * (double)st.f[0]);
-      g[3] = (float)((double)g[3] + (ih + src_hhi) * (double)st.f[1]);
-      ig = (q2 + (double)v.z * kRintJHeI3 / (double)ab.z) / len;
-      ih = (q2 + (double)v.z * kRintHHeI3 / (double)ab.z) / len;
-      g[1] = (float)((double)g[1] + (ig + src_ghei) * (double)st.f[2]);
-      g[4] = (float)((double)g[4] + (ih + src_hhei) * (double)st.f[3]);
-      ig = q3 / len;
-      g[2] = (float)((double)g[2] + (ig + src_heii) * (double)st.f[4]);
-      g[5] = (float)((double)g[5] + (ig + src_heii) * (double)st.f[5]);
+      const float il = 1.f / v.w;
+      const float t1 = v.x * ia1, t2 = v.y * ia2;
+      g[0] = fmaf(fmaf(fmaf(v.z, c3j, fmaf(v.y, c2j, t1)), il, src_ghi), st.f[0], g[0]);
+      g[3] = fmaf(fmaf(fmaf(v.z, c3h, fmaf(v.y, c2h, t1)), il, src_hhi), st.f[1], g[3]);
+      g[1] = fmaf(fmaf(fmaf(v.z, c3ej, t2), il, src_ghei), st.f[2], g[1]);
+      g[4] = fmaf(fmaf(fmaf(v.z, c3eh, t2), il, src_hhei), st.f[3], g[4]);
+      const float t3 = fmaf(v.z * ia3, il, sf.z);
+      g[2] = fmaf(t3, st.f[4], g[2]);
+      g[5] = fmaf(t3, st.f[5], g[5]);
     }
 #pragma unroll
     for (int s = 0; s < 6; s++) gh6[s * n + c] = g[s];
@@ -483,14 +499,13 @@ namespace {
 int art_run(const argot_b200_art *a, const ArtGeom &g, double denstonh, double uenetok, const float *fields8,
             float *rates6, void *work, int apass, unsigned long long *crossings, int *err, cudaStream_t st) {
   const uint64_t n = (uint64_t)g.nx * g.ny * g.nz;
-  float4 *absorp = (float4 *)work;
-  float4 *srcf = absorp + n;
-  float4 *acc = srcf + n;
+  ArtCell *cells = (ArtCell *)work;
+  float4 *acc = (float4 *)(cells + n);
   float *gh6 = (float *)(acc + (uint64_t)apass * n);
   const int blocks = art_blocks(n);
   const float cs1 = (float)sigma_hi(kThrHI + 1.0e-7), cs2 = (float)sigma_hei(kThrHeI + 1.0e-7);
   const float cs3 = (float)sigma_heii(kThrHeII + 1.0e-7);
-  k_art_cells<<<blocks, 256, 0, st>>>(n, fields8, denstonh, uenetok, cs1, cs2, cs3, absorp, srcf, gh6);
+  k_art_cells<<<blocks, 256, 0, st>>>(n, fields8, denstonh, uenetok, cs1, cs2, cs3, cells, gh6);
   ARGOT_CUDA_TRY(cudaGetLastError());
   const uint32_t face_max = (uint32_t)std::max<uint64_t>(
       (uint64_t)g.nx * g.ny, std::max<uint64_t>((uint64_t)g.ny * g.nz, (uint64_t)g.nz * g.nx));
@@ -498,10 +513,10 @@ int art_run(const argot_b200_art *a, const ArtGeom &g, double denstonh, double u
     const int na = std::min(apass, a->nang - a0);
     ARGOT_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(float4) * n * (uint64_t)na, st));
     const uint64_t threads = (uint64_t)na * face_max;
-    k_art_trace<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(g, a->dev_ang, a0, na, face_max, absorp, srcf,
-                                                                    acc, crossings, err);
+    k_art_trace<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(g, a->dev_ang, a0, na, face_max, cells, acc,
+                                                                    crossings, err);
     ARGOT_CUDA_TRY(cudaGetLastError());
-    k_art_fold<<<blocks, 256, 0, st>>>(n, na, acc, absorp, srcf, a->step, gh6);
+    k_art_fold<<<blocks, 256, 0, st>>>(n, na, acc, cells, a->step, gh6);
     ARGOT_CUDA_TRY(cudaGetLastError());
   }
   const float r_nang = (float)(1.0e0 / a->nang);
@@ -599,7 +614,7 @@ int art_dropin(run_param *run, cuda_mem_space *cm, cuda_param *cp, host_diffuse_
                                            std::max<uint64_t>((uint64_t)g.ny * g.nz, (uint64_t)g.nz * g.nx));
   int apass = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)nang, (1ull << 20) / face));
   apass = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)apass, (2ull << 30) / (16 * n)));
-  const size_t need = sizeof(float) * 14 * n + 16 + (size_t)(n * (2 * 16 + 24) + n * 16 * (uint64_t)apass);
+  const size_t need = sizeof(float) * 14 * n + 32 + (size_t)(n * (32 + 24) + n * 16 * (uint64_t)apass);
   if (need > D.bytes) {
     if (D.buf) cudaFree(D.buf);
     D.buf = nullptr;
@@ -609,7 +624,7 @@ int art_dropin(run_param *run, cuda_mem_space *cm, cuda_param *cp, host_diffuse_
   }
   float *f8 = (float *)D.buf;
   float *r6 = f8 + 8 * n;
-  void *work = (void *)(((uintptr_t)(r6 + 6 * n) + 15) & ~(uintptr_t)15);
+  void *work = (void *)(((uintptr_t)(r6 + 6 * n) + 31) & ~(uintptr_t)31);
   cudaStream_t st = (cp && cp->num_cuda_dev > 0) ? (cudaStream_t)cp->strm[0] : (cudaStream_t)0;
   int *err = err_flag(0);
   if (!err) return ARGOT_B200_ENOMEM;
@@ -731,15 +746,15 @@ void calc_diffuse_photon_radiation(::fluid_mesh *mesh, ::run_param *this_run, ::
 uint64_t argot_b200_art_workspace(const argot_b200_grid *g, int angles_per_pass) {
   if (!grid_valid(g) || angles_per_pass < 1) return 0;
   const uint64_t n = (uint64_t)g->nx * g->ny * g->nz;
-  return n * (2 * sizeof(float4) + 6 * sizeof(float)) + n * sizeof(float4) * (uint64_t)angles_per_pass;
+  return n * (sizeof(ArtCell) + 6 * sizeof(float)) + n * sizeof(float4) * (uint64_t)angles_per_pass;
 }
 
 int argot_b200_art_rates(const argot_b200_art *a, const argot_b200_grid *gp, double uenetok, const float *fields8,
                          float *rates6, void *work, int angles_per_pass, unsigned long long *crossings,
                          void *stream) {
   ArtGeom g;
-  if (!a || !fields8 || !rates6 || !work || angles_per_pass < 1 || !art_geom_from_grid(gp, &g) ||
-      !(uenetok > 0.0)) {
+  if (!a || !fields8 || !rates6 || !work || ((uintptr_t)work & 31) || angles_per_pass < 1 ||
+      !art_geom_from_grid(gp, &g) || !(uenetok > 0.0)) {
     set_status(ARGOT_B200_EINVAL);
     return ARGOT_B200_EINVAL;
   }

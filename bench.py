@@ -36,7 +36,9 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 CONFIGS = ("largest", "plain", "precision", "learned", "tiny", "plain256", "batched", "batched_small",
-           "ionized", "ionized64")
+           "ionized", "ionized64", "art", "art256", "art64")
+ART_METRIC = "ART diffuse ray-cell steps/s (768 HEALPix directions, 1 B200)"
+ART_UENETOK = 1.0e4
 METRIC = "ray-cell crossings/s (march+stitch+rates, 1 B200)"
 # DRAM bytes per ray-cell crossing of k_march_rays<Kahan> measured by ncu on
 # the 256^3 / 16-source case (1.0045 TB/s over a 128.5 ms launch = 129.1 GB
@@ -68,6 +70,14 @@ def make_workload(name: str, rank: int = 0):
     if name == "ionized64":
         # profiling case for the surrogate kernels (fills the GPU, ~1 GB on the device)
         return W.ionized(64, 64, seed=9 + seed_shift)
+    if name == "art":
+        # the diffuse-radiation path on the precision mesh (128^3)
+        return W.precision(seed=2 + seed_shift)
+    if name == "art256":
+        return W.largest(seed=5 + seed_shift)
+    if name == "art64":
+        # profiling case for the ART kernels
+        return W.plain(seed=1 + seed_shift)
     if name == "batched":
         return W.batched(48, seed=3 + seed_shift)
     if name == "batched_small":
@@ -721,6 +731,142 @@ def batched_e2e(B, wls, dev, steps=2):
             "includes": "H2D fields + pack of every problem, batch graph replay, D2H rates"}
 
 
+# ------------------------------------------------------------ ART
+def art_fields(wl):
+    """The eight input planes of the diffuse-radiation path from a
+    workload's mesh: dens, fHI, fHII, fHeI, fHeII, fHeIII, felec, uene, with
+    fHII = 1 - fHI, fHeIII = 1 - fHeI - fHeII, the electrons of both, and a
+    temperature of 100 K in neutral gas rising to 2e4 K with fHII (uene in
+    units where T = uene * ART_UENETOK * wmol, as run_param.uenetok)."""
+    helium_fact = 0.0811258278  # prim_chem/chemistry.h:25
+    dens, fhi, fhei, fheii = [np.asarray(a, np.float64) for a in wl.fields()]
+    fhii = 1.0 - fhi
+    fheiii = np.clip(1.0 - fhei - fheii, 0.0, 1.0)
+    felec = fhii + helium_fact * (fheii + 2.0 * fheiii)
+    temp = 100.0 + (2.0e4 - 100.0) * fhii
+    wmol = 1.0 / ((1.0 + felec) * 0.755 + 0.25 * 0.245)
+    uene = temp / (ART_UENETOK * wmol)
+    return np.stack([dens, fhi, fhii, fhei, fheii, fheiii, felec, uene]).astype(np.float32)
+
+
+def art_reference(wl, planes, threads=None):
+    """ARGOT's own CPU calc_diffuse_photon_radiation (OpenMP over all host
+    cores) on the same mesh: (wall seconds, rates)"""
+    from oracle.oracle import RefLib
+    R = RefLib(wl.edge)
+    R.init(wl.lunit, wl.denstonh, wl.theta, threads or os.cpu_count() or 1)
+    R.art_init(ART_UENETOK)
+    R.art_set_mesh(planes)
+    rates, t = R.art_run()
+    return t, rates
+
+
+def run_art(args):
+    """The ART diffuse-radiation path (argot_b200_art_rates, all 768
+    directions) on one GPU: K timed passes with the fields resident, CUDA
+    events; e2e through the same call from pinned host buffers."""
+    import torch
+    from argot_b200 import _lib as L
+    from argot_b200 import diffuse as D
+    from argot_b200.pipeline import unit_box_grid
+    ws, rank, local = dist_env()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    init_dist(ws, "nccl")
+    wl = make_workload(args.config, rank)
+    planes = art_fields(wl)
+    g = unit_box_grid(wl.edge, wl.lunit, wl.denstonh)
+    n = wl.ncell
+    f = torch.from_numpy(planes).to(dev)
+    rates = torch.zeros(6 * n, dtype=torch.float32, device=dev)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    art = D.Diffuse()
+    apass = art.default_pass(g)
+    stream = torch.cuda.current_stream(dev)
+    lib = L.load()
+
+    def step(count=None):
+        art.rates(g, ART_UENETOK, f, rates, angles_per_pass=apass, crossings=count, stream=stream.cuda_stream)
+
+    for w in range(args.warmup):
+        step(cnt if w == 0 else None)
+    torch.cuda.synchronize()
+    L.check(lib.argot_b200_check_device_error(stream.cuda_stream), "device error")
+    steps_per_pass = int(cnt.item())
+    clocks = ClockSampler(local)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    t = allmax(ws, e0.elapsed_time(e1) / 1e3, dev)
+    total = allsum(ws, float(steps_per_pass) * args.steps, dev)
+    hbm, _, peak_kind = measured_peaks()
+    # algorithmic bytes of one pass: per step two float4 of cell data read
+    # and one float4 reduction; per cell and direction one float4 folded;
+    # per cell 8 planes in, 6 planes of totals and 6 rate planes
+    alg = 48.0 * steps_per_pass + 16.0 * n * art.nang + 4.0 * n * (8 + 6 + 12)
+    achieved = alg / (t / args.steps) / 1e9
+    # e2e: the 8 planes from pinned host memory, the pass, the rates back
+    pin_f = torch.from_numpy(planes).pin_memory()
+    out = torch.empty(6 * n, dtype=torch.float32).pin_memory()
+    times = []
+    for s_ in range(4):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        f.copy_(pin_f, non_blocking=True)
+        rates.zero_()
+        step()
+        out.copy_(rates, non_blocking=True)
+        torch.cuda.synchronize()
+        if s_ > 0:
+            times.append(time.perf_counter() - t0)
+    te = statistics.median(times)
+    got = out.view(6, -1).numpy().copy()
+    art.close()
+    line = {
+        "metric": ART_METRIC, "value": total / t, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded lognormal mesh, ionisation around clustered sources)",
+        "config": {"workload": f"art on {wl.name}", "mesh": f"{wl.edge}^3", "directions": art.nang,
+                   "angles_per_pass": apass, "steps_per_pass": steps_per_pass,
+                   "l2": "cell data 1 GB at 256^3, 67 MB at 128^3; accumulators larger than L2; no flush",
+                   "parallelism": f"{ws} independent meshes (one per GPU)"},
+        "roofline": {"kernel": "k_art_cells + k_art_trace + k_art_fold (one pass)", "bound": "hbm",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_kind": f"{peak_kind} hbm_gbs", "traffic": None,
+                     "bytes_model": "48 B per ray-cell step + 16 B per cell and direction + 104 B per cell"},
+        "e2e": {"value": float(steps_per_pass) / te, "unit": UNIT, "h2d_bytes_per_step": int(planes.nbytes),
+                "d2h_bytes_per_step": int(6 * n * 4), "s_per_step": te},
+        "clocks": clk,
+        "gpu_launches": (1 + 3 * ((art.nang + apass - 1) // apass) + 1) * args.steps,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            tr, ref = art_reference(wl, planes)
+            rel = np.abs(got.astype(np.float64) - ref) / np.maximum(np.abs(ref.astype(np.float64)), 1e-300)
+            big = np.abs(ref) > 1e-6 * np.abs(ref).max(axis=1, keepdims=True)
+            line["cpu_baseline"] = {"value": steps_per_pass / tr, "unit": UNIT, "cores": os.cpu_count(),
+                                    "kind": "reference",
+                                    "sample": f"one whole ART pass on the same {wl.edge}^3 mesh, {tr:.1f} s"}
+            line["max_rel_err_vs_reference"] = float(rel[big].max())
+        except Exception as exc:
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                                    "sample": f"failed: {exc}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 # ------------------------------------------------------------ reference arm
 def run_reference(args):
     ws, rank, _ = dist_env()
@@ -750,6 +896,56 @@ def run_reference(args):
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def run_reference_art(args):
+    """the reference's CPU ART on the same mesh, one whole pass per step"""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle.oracle import RefLib
+    wl = make_workload(args.config, 0)
+    planes = art_fields(wl)
+    R = RefLib(wl.edge)
+    R.init(wl.lunit, wl.denstonh, wl.theta, os.cpu_count() or 1)
+    R.art_init(ART_UENETOK)
+    R.art_set_mesh(planes)
+    ts = []
+    for s in range(args.warmup + args.steps):
+        _, t = R.art_run()
+        if s >= args.warmup:
+            ts.append(t)
+    t = statistics.median(ts)
+    steps = art_step_count(wl)
+    v = steps / t
+    print(json.dumps({
+        "metric": ART_METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "impl": "reference", "data": "synthetic (seeded lognormal mesh)",
+        "config": {"workload": f"art on {wl.name}", "mesh": f"{wl.edge}^3"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                         "sample": f"whole ART passes, median {t:.1f} s"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def art_step_count(wl):
+    """ray-cell steps of one ART pass (the reference's float DDA gives the
+    same cells): counted by the GPU kernel when one is present, else by a
+    NumPy walk of every ray"""
+    import torch
+    if torch.cuda.is_available():
+        from argot_b200 import diffuse as D
+        from argot_b200.pipeline import unit_box_grid
+        g = unit_box_grid(wl.edge, wl.lunit, wl.denstonh)
+        f = torch.from_numpy(art_fields(wl)).cuda()
+        r = torch.zeros(6 * wl.ncell, dtype=torch.float32, device="cuda")
+        c = torch.zeros(1, dtype=torch.int64, device="cuda")
+        art = D.Diffuse()
+        art.rates(g, ART_UENETOK, f, r, crossings=c)
+        torch.cuda.synchronize()
+        art.close()
+        return int(c.item())
+    raise SystemExit("the ART step count needs the GPU kernel")
 
 
 def main(argv=None):
@@ -787,8 +983,12 @@ def main(argv=None):
         print(json.dumps({"config": wl.name,
                           "reference_gpu": reference_gpu_sample(wl, target_rays=args.reference_gpu_rays)}),
               flush=True)
+    elif args.impl == "reference" and args.config.startswith("art"):
+        run_reference_art(args)
     elif args.impl == "reference":
         run_reference(args)
+    elif args.config.startswith("art"):
+        run_art(args)
     elif args.config.startswith("batched"):
         run_batched(args)
     else:

@@ -437,7 +437,8 @@ ARGOT_B200_API int argot_b200_art_create(const float *dir3, const int *base_corn
                                          argot_b200_art **out);
 ARGOT_B200_API void argot_b200_art_destroy(argot_b200_art *a);
 ARGOT_B200_API int argot_b200_art_num_angles(const argot_b200_art *a);
-/* device workspace bytes for argot_b200_art_rates with angles_per_pass */
+/* device workspace bytes for argot_b200_art_rates with angles_per_pass (the
+ * workspace must be 32-byte aligned, as cudaMalloc returns it) */
 ARGOT_B200_API uint64_t argot_b200_art_workspace(const argot_b200_grid *g, int angles_per_pass);
 /* fields8_dev: 8 planes of ncell floats: dens, fHI, fHII, fHeI, fHeII,
  * fHeIII, felec, uene (fluid_mesh dens, prev_chem fractions, prev_uene);
