@@ -745,8 +745,9 @@ void calc_diffuse_photon_radiation(::fluid_mesh *mesh, ::run_param *this_run, ::
                                    ::cuda_param *this_cuda, ::host_diffuse_param *hd_param,
                                    ::cuda_diffuse_param *cd_param, ::omp_param *this_omp) {
   (void)mesh; (void)cd_param; (void)this_omp;
-  set_status(argot::art_dropin((argot::run_param *)this_run, (argot::cuda_mem_space *)cuda_mem,
-                               (argot::cuda_param *)this_cuda, (argot::host_diffuse_param *)hd_param));
+  argot::dropin_status((argot::run_param *)this_run, "calc_diffuse_photon_radiation",
+                       argot::art_dropin((argot::run_param *)this_run, (argot::cuda_mem_space *)cuda_mem,
+                                         (argot::cuda_param *)this_cuda, (argot::host_diffuse_param *)hd_param));
 }
 
 uint64_t argot_b200_art_workspace(const argot_b200_grid *g, int angles_per_pass) {

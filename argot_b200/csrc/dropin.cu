@@ -290,6 +290,14 @@ int do_smooth(fluid_mesh *mesh, run_param *run, cuda_mem_space *cm, cuda_param *
 
 }  // namespace dropin_detail
 using namespace dropin_detail;
+
+void dropin_status(const run_param *run, const char *entry, int rc) {
+  set_status(rc);
+  if (rc && run && run->proc_file) {
+    std::fprintf(run->proc_file, "# argot_b200 %s: %s (%d)\n", entry, argot_b200_error_string(rc), rc);
+    std::fflush(run->proc_file);
+  }
+}
 }  // namespace argot
 
 using argot::set_status;
@@ -320,27 +328,31 @@ int argot_b200_set_dropin_smooth_faces(int faces) {
 void smooth_photoion_rate(::fluid_mesh *mesh, ::run_param *this_run, ::cuda_mem_space *cuda_mem,
                           ::cuda_param *this_cuda, struct mpi_param *this_mpi) {
   (void)this_mpi;
-  set_status(argot::do_smooth((argot::fluid_mesh *)mesh, (argot::run_param *)this_run,
-                              (argot::cuda_mem_space *)cuda_mem, (argot::cuda_param *)this_cuda));
+  argot::dropin_status((argot::run_param *)this_run, "smooth_photoion_rate",
+                       argot::do_smooth((argot::fluid_mesh *)mesh, (argot::run_param *)this_run,
+                                        (argot::cuda_mem_space *)cuda_mem, (argot::cuda_param *)this_cuda));
 }
 
 void calc_optical_depth_cuda(::ray_segment *seg, ::cuda_mem_space *cuda_mem,
                              struct cuda_param *this_cuda, ::run_param *this_run) {
-  set_status(argot::do_march((argot::ray_segment *)seg, (argot::cuda_mem_space *)cuda_mem,
-                      (argot::cuda_param *)this_cuda, (argot::run_param *)this_run));
+  argot::dropin_status((argot::run_param *)this_run, "calc_optical_depth_cuda",
+                       argot::do_march((argot::ray_segment *)seg, (argot::cuda_mem_space *)cuda_mem,
+                                       (argot::cuda_param *)this_cuda, (argot::run_param *)this_run));
 }
 
 void calc_photoion_rate_cuda(::cuda_mem_space *cuda_mem, ::light_ray *ray, ::light_ray_IO *ray_IO,
                              struct cuda_param *this_cuda, ::run_param *this_run) {
-  set_status(argot::do_rates((argot::cuda_mem_space *)cuda_mem, (argot::light_ray *)ray, (argot::light_ray_IO *)ray_IO,
-                      (argot::cuda_param *)this_cuda, (argot::run_param *)this_run));
+  argot::dropin_status((argot::run_param *)this_run, "calc_photoion_rate_cuda",
+                       argot::do_rates((argot::cuda_mem_space *)cuda_mem, (argot::light_ray *)ray,
+                                       (argot::light_ray_IO *)ray_IO, (argot::cuda_param *)this_cuda,
+                                       (argot::run_param *)this_run));
 }
 
 void zero_out_photoion_rate_cuda(::cuda_mem_space *cuda_mem, ::cuda_param *this_cuda,
                                  struct run_param *this_run) {
   argot::cuda_mem_space *cm = (argot::cuda_mem_space *)cuda_mem;
   argot::run_param *run = (argot::run_param *)this_run;
-  if (!cm || !run || !cm[0].mesh_dev) { set_status(ARGOT_B200_EINVAL); return; }
+  if (!cm || !run || !cm[0].mesh_dev) { argot::dropin_status(run, "zero_out_photoion_rate_cuda", ARGOT_B200_EINVAL); return; }
   const uint64_t n = (uint64_t)run->nmesh_x_local * run->nmesh_y_local * run->nmesh_z_local;
   argot::DeviceScope dscope;
   if (!dscope.ok) { set_status(ARGOT_B200_ECUDA); return; }
@@ -350,7 +362,7 @@ void zero_out_photoion_rate_cuda(::cuda_mem_space *cuda_mem, ::cuda_param *this_
     cudaError_t e = cudaStreamSynchronize(st);
     rc = e == cudaSuccess ? 0 : argot::status_from_cuda(e);
   }
-  set_status(rc);
+  argot::dropin_status(run, "zero_out_photoion_rate_cuda", rc);
 }
 
 // One rank: the send buffer of accum_optical_depth.c:59-104 is the only

@@ -140,6 +140,11 @@ struct host_diffuse_param {
   angle_info *angle;
 };
 
+// Records a drop-in entry point's status for argot_b200_last_error and, on
+// failure, writes one line to the caller's run->proc_file (the reference's
+// log) when it has one.
+void dropin_status(const run_param *run, const char *entry, int rc);
+
 static_assert(sizeof(angle_info) == 16, "angle_info layout");
 static_assert(sizeof(step_func_factor) == 24, "step_func_factor layout");
 static_assert(sizeof(host_diffuse_param) == 48, "host_diffuse_param layout");

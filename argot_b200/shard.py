@@ -103,3 +103,28 @@ def broadcast_field(packed, src: int = 0, group=None):
     import torch.distributed as dist
     dist.broadcast(packed, src, group=group)
     return packed
+
+
+def rate_change(prev6, cur6, floor: float = 0.0) -> float:
+    """Largest relative change of the six rate planes between two passes of
+    the iteration (|cur - prev| / |cur| over the cells whose |cur| exceeds
+    `floor`), on this rank's cells."""
+    import torch
+    d = (cur6 - prev6).abs()
+    m = cur6.abs()
+    keep = m > floor
+    if not bool(keep.any()):
+        return 0.0
+    return float(torch.max(d[keep] / m[keep]).item())
+
+
+def converged(local_change: float, tol: float, group=None) -> bool:
+    """The all-reduce (MAX) of the per-rank changes against tol, identical on
+    every rank: the convergence test of the radiation iteration when the
+    target cells are sharded over ranks."""
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.tensor([local_change], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return bool(t.item() <= tol)

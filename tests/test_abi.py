@@ -110,3 +110,28 @@ def test_batch_and_surrogate_reject_bad_arguments():
     g = unit_box_grid(8, 1.0, 1.0)
     assert lib.argot_b200_photoion_rays_surrogate(C.byref(g), None, None, None, 0, 1, None, 0, None, 0, None,
                                                   None, None, None, None) == L.EINVAL
+
+
+def test_dropin_failure_is_logged_to_proc_file(tmp_path):
+    """A drop-in that fails records its status and writes one line to the
+    caller's run->proc_file, the reference's log."""
+    import ctypes as C
+    import ctypes.util
+    from argot_b200 import _lib as L, abi
+    libc = C.CDLL(ctypes.util.find_library("c"))
+    libc.fopen.restype = C.c_void_p
+    libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+    libc.fclose.argtypes = [C.c_void_p]
+    log = tmp_path / "proc.log"
+    fp = libc.fopen(str(log).encode(), b"w")
+    assert fp
+    run = abi.RunParam()
+    run.proc_file = fp
+    run.nmesh_x_local = run.nmesh_y_local = run.nmesh_z_local = 8
+    cm = (abi.CudaMemSpace * 1)()   # no mesh on the device: invalid
+    lib = L.load()
+    lib.calc_optical_depth_cuda(None, C.addressof(cm), None, C.addressof(run))
+    assert lib.argot_b200_last_error() == L.EINVAL
+    libc.fclose(fp)
+    text = log.read_text()
+    assert "calc_optical_depth_cuda" in text and "(-1)" in text

@@ -142,8 +142,21 @@ def _task_sharded_reference(rank, ws, out_dir):
     return all(c1 > c0 for c0, c1 in ranges)
 
 
+def _task_converged(rank, ws, arg):
+    """every rank reaches the same verdict from its own cells' change"""
+    import torch
+    prev = torch.ones(6 * 100)
+    cur = prev.clone()
+    cur[rank] = 1.0 + 1e-3 * (rank + 1)   # rank r changed by (r + 1) 1e-3
+    ch = shard.rate_change(prev, cur)
+    loose = shard.converged(ch, 5e-3)      # max change 2e-3 <= 5e-3
+    tight = shard.converged(ch, 1.5e-3)    # rank 1's 2e-3 > 1.5e-3 for everyone
+    c = float(cur[rank])
+    return loose and not tight and abs(ch - (c - 1.0) / c) < 1e-7
+
+
 TASKS = {"gather": _task_gather, "broadcast": _task_broadcast, "reductions": _task_reductions,
-         "sharded_reference": _task_sharded_reference}
+         "converged": _task_converged, "sharded_reference": _task_sharded_reference}
 
 
 def _worker(rank, ws, port, task, out_dir):
@@ -170,7 +183,7 @@ def _run(task):
     return flags, arrays
 
 
-@pytest.mark.parametrize("task", ["gather", "broadcast", "reductions"])
+@pytest.mark.parametrize("task", ["gather", "broadcast", "reductions", "converged"])
 def test_gloo_exchange(task):
     flags, _ = _run(task)
     assert flags == ["1"] * WS
