@@ -269,10 +269,28 @@ def reference_gpu_sample(wl, target_rays: int = 2_000_000, seed: int = 1, reps: 
         im0 = int(rng.integers(0, ncell - ncells + 1))
         R.zero_rates_gpu()
         out = R.run_range_gpu(im0, im0 + ncells, kernel_reps=reps, want=("seg",))
+        ref_rates = R.rates_gpu()
+        # the same loop with this library's drop-in entry points linked in
+        from argot_b200 import _lib as L
+        R.use_entry_points(L.load())
+        R.zero_rates_gpu()
+        ours = R.run_range_gpu(im0, im0 + ncells, kernel_reps=0)
+        our_rates = R.rates_gpu()
+        R.use_entry_points(None)
     finally:
         R.close()
     cross = float(Oracle().count_crossings(unit_box_grid(wl.edge, wl.lunit, wl.denstonh), out["seg"]).sum())
     calls = out["march_s"] + out["accum_s"] + out["rates_s"]
+    ours_calls = ours["march_s"] + ours["accum_s"] + ours["rates_s"]
+    nz = ref_rates != 0
+    drop = {"what": "the same loop (reference tree, host light rays) with libargot_b200's "
+                    "calc_optical_depth_cuda / calc_photoion_rate_cuda linked in",
+            "value": cross / ours_calls, "unit": UNIT,
+            "calls_s": {"calc_optical_depth_cuda": ours["march_s"], "accum_optical_depth": ours["accum_s"],
+                        "calc_photoion_rate_cuda": ours["rates_s"]},
+            "max_rel_diff_vs_reference_gpu": (float(np.max(np.abs(our_rates[nz].astype(np.float64) -
+                                                                  ref_rates[nz]) / np.abs(ref_rates[nz])))
+                                              if nz.any() else None)}
     t_mk, t_rk = out["march_kernel_ms"] / 1e3, out["rate_kernel_ms"] / 1e3
     hbm, _, peak_kind = measured_peaks()
     march_gbs = (16.0 * cross + 36.0 * out["nseg"]) / t_mk / 1e9
@@ -290,7 +308,8 @@ def reference_gpu_sample(wl, target_rays: int = 2_000_000, seed: int = 1, reps: 
             "rates_rays_per_s": out["nray"] / t_rk,
             "calls_s": {"calc_optical_depth_cuda": out["march_s"], "accum_optical_depth": out["accum_s"],
                         "calc_photoion_rate_cuda": out["rates_s"], "ray_setup_host": out["setup_s"]},
-            "kernels_s": {"calc_optical_depth_kernel": t_mk, "calc_photoion_rate_kernel": t_rk}}
+            "kernels_s": {"calc_optical_depth_kernel": t_mk, "calc_photoion_rate_kernel": t_rk},
+            "dropin": drop}
 
 
 # ------------------------------------------------------------ rate modes

@@ -371,7 +371,18 @@ class RefGpu(RefLib):
         L.refgpu_run_range.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_uint64,
                                        _f64p]
         L.refgpu_run_range.restype = C.c_int
+        L.refgpu_use_entry_points.argtypes = [C.c_void_p, C.c_void_p]
         assert L.refgpu_edge() == edge
+
+    def use_entry_points(self, lib=None):
+        """run the group loop with another library's calc_optical_depth_cuda
+        and calc_photoion_rate_cuda (a drop-in), or the reference's own
+        (lib None)"""
+        if lib is None:
+            self.lib.refgpu_use_entry_points(None, None)
+        else:
+            self.lib.refgpu_use_entry_points(C.cast(lib.calc_optical_depth_cuda, C.c_void_p),
+                                             C.cast(lib.calc_photoion_rate_cuda, C.c_void_p))
 
     def upload(self):
         """mesh and run parameters to the device (after set_mesh and

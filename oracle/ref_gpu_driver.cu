@@ -17,7 +17,10 @@
  * copies and kernels).  A second, kernel-only pass launches the two
  * reference kernels themselves with the reference's launch geometry on
  * device-resident copies of the same segments and rays, timed with CUDA
- * events on the launching stream.  No arithmetic of the path lives here.
+ * events on the launching stream.  The same loop can call another
+ * library's functions of the same signatures instead (a drop-in
+ * replacement) for a like-for-like timing.  No arithmetic of the path lives
+ * here.
  */
 #include <cstdio>
 #include <cstdlib>
@@ -58,6 +61,21 @@ __global__ void calc_optical_depth_kernel(const struct fluid_mesh *__restrict__,
                                           const struct run_param *__restrict__, uint64_t);
 __global__ void calc_photoion_rate_kernel(struct fluid_mesh *, const struct light_ray_IO *__restrict__,
                                           const struct run_param *__restrict__, uint64_t);
+
+/* the march and rate entry points the group loop calls: the reference's
+ * own by default, or another library's functions with the same signatures
+ * (refgpu_use_entry_points), so that ARGOT's loop can be timed with a
+ * drop-in replacement linked in */
+typedef void (*march_fn)(struct ray_segment *, struct cuda_mem_space *, struct cuda_param *, struct run_param *);
+typedef void (*rates_fn)(struct cuda_mem_space *, struct light_ray *, struct light_ray_IO *, struct cuda_param *,
+                         struct run_param *);
+static march_fn g_march = calc_optical_depth_cuda;
+static rates_fn g_rates = calc_photoion_rate_cuda;
+
+extern "C" void refgpu_use_entry_points(void *march, void *rates) {
+  g_march = march ? (march_fn)march : calc_optical_depth_cuda;
+  g_rates = rates ? (rates_fn)rates : calc_photoion_rate_cuda;
+}
 
 static struct cuda_param g_cp;
 static struct cuda_mem_space g_cm[NMAX_CUDA_DEV];
@@ -282,11 +300,11 @@ extern "C" int refgpu_run_range(int im_start, int im_end, int kernel_reps, float
         o[3] = seg[k].xpos_end; o[4] = seg[k].ypos_end; o[5] = seg[k].zpos_end;
       }
     }
-    calc_optical_depth_cuda(seg, g_cm, &g_cp, run);
+    g_march(seg, g_cm, &g_cp, run);
     const double t2 = now_s();
     ref_accum_group(ray, seg);
     const double t3 = now_s();
-    calc_photoion_rate_cuda(g_cm, ray, io, &g_cp, run);
+    g_rates(g_cm, ray, io, &g_cp, run);
     const double t4 = now_s();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) { free(ray); return -(int)e - 1000; }

@@ -56,3 +56,26 @@ def test_reference_gpu_path_computes_the_path(cuda_ok):
         assert out["march_kernel_ms"] > 0 and out["rate_kernel_ms"] > 0
     finally:
         R.close()
+
+
+def test_reference_loop_with_this_librarys_entry_points(cuda_ok):
+    """ARGOT's group loop (its tree, its host light rays, its accum) with
+    libargot_b200's calc_optical_depth_cuda / calc_photoion_rate_cuda linked
+    in: columns bit for bit those of the reference's CPU build, rates within
+    the device exp's few ulps."""
+    from argot_b200 import _lib as L
+    g = golden("golden_path.npz")
+    R, edge = _refgpu(g)
+    try:
+        R.use_entry_points(L.load())
+        R.zero_rates_gpu()
+        out = R.run_range_gpu(0, edge ** 3, want=("seg", "tau"))
+        assert np.array_equal(out["tau"], g["tau"])
+        rates = R.rates_gpu().astype(np.float64)
+        want = g["rates"].astype(np.float64)
+        nz = want > 0
+        assert np.array_equal(rates > 0, nz)
+        assert (np.abs(rates - want)[nz] / want[nz]).max() < 2e-6
+    finally:
+        R.use_entry_points(None)
+        R.close()
