@@ -68,6 +68,14 @@ void host_tables(double *nu, float *cs3);
 // sigma_s(nu) * ((float)nu - nu_s)^+ for s = HI, HeI, HeII.
 void host_rate_weights(double *w6);
 
+// Position of bin k in an emitter's normalised spectrum (emit_specn): the
+// bins are stored in the pair order of the packed rate loop, pair
+// p = (k % 8) + 8 (k / 16) holding bins k0 = (p % 8) + 16 (p / 8) and k0 + 8
+// at 2 p and 2 p + 1, so one 8-byte load fetches a pair.
+__host__ __device__ __forceinline__ int spec_pair_index(int k) {
+  return 2 * ((k & 7) + 8 * (k >> 4)) + ((k >> 3) & 1);
+}
+
 // Emitters and tree on the device.
 struct DevNode {
   float cx, cy, cz, len;   // centre (float, as stored by the reference), side
@@ -88,7 +96,7 @@ struct argot_b200_dev_tree {
   int *src_list;           // n_src: source index per leaf slot
   float4 *emit_pos;        // n_emit (x, y, z, 0)
   double *emit_spec64;     // n_emit x 256
-  float *emit_specn;       // n_emit x 256: spectrum / total
+  float *emit_specn;       // n_emit x 256: spectrum / total, in bin-pair order (spec_pair_index)
   double *emit_total;      // n_emit
   // surrogate inputs (set by argot_b200_dev_tree_set_blackbody): log10 T of
   // an emitter whose spectrum is a single-temperature blackbody (NaN

@@ -439,7 +439,9 @@ int argot_b200_dev_tree_upload(const argot_b200_tree *t, argot_b200_dev_tree **o
     for (int k = 0; k < kNu; k++) s += spec[e * kNu + k];
     total[e] = s;
     const double inv = s > 0.0 ? 1.0 / s : 0.0;
-    for (int k = 0; k < kNu; k++) specn[e * kNu + k] = (float)(spec[e * kNu + k] * inv);
+    // bin-pair order of the packed rate loop: position 2 p + h holds bin
+    // (p % 8) + 16 (p / 8) + 8 h (spec_pair_index)
+    for (int k = 0; k < kNu; k++) specn[e * kNu + spec_pair_index(k)] = (float)(spec[e * kNu + k] * inv);
   }
   cudaError_t err = cudaSuccess;
   auto alloc = [&](void **p, size_t bytes) {

@@ -193,7 +193,7 @@ static __device__ __noinline__ void rate_bins_f32(const RayCols &c, const float 
       const float dl2 = fmaf(D0, a0, fmaf(D1, a1, D2 * a2));
       const float e = ex2_approx(-tl2);
       const float ed = ex2_approx(-dl2);
-      const float w = __ldg(specn + k) * e * phi_pc(dl2 * ln2, ed);
+      const float w = __ldg(specn + spec_pair_index(k)) * e * phi_pc(dl2 * ln2, ed);
       g0 = fmaf(c_tab.cs[0][k], w, g0);
       g1 = fmaf(c_tab.cs[1][k], w, g1);
       g2 = fmaf(c_tab.cs[2][k], w, g2);
@@ -265,19 +265,22 @@ __device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab,
 #pragma unroll 4
   for (int i = 0; i < kBinPairs / 8; i++) {
     const BinPair &b = tab[j + 8 * i];
-    const int k0 = j + 16 * i;
-    const float2 tl = __ffma2_rn(n0, b.l2e[0], __ffma2_rn(n1, b.l2e[1], __fmul2_rn(n2, b.l2e[2])));
-    const float2 dl = __ffma2_rn(d0, b.l2e[0], __ffma2_rn(d1, b.l2e[1], __fmul2_rn(d2, b.l2e[2])));
-    const float2 s = make_float2(__ldg(sp + k0), __ldg(sp + k0 + 8));
+    const float2 l0 = b.l2e[0], l1 = b.l2e[1], l2 = b.l2e[2];
+    const float2 c0 = b.cs[0], c1 = b.cs[1], c2 = b.cs[2];
+    const float2 w0 = b.hw[0], w1 = b.hw[1], w2 = b.hw[2];
+    const float2 tl = __ffma2_rn(n0, l0, __ffma2_rn(n1, l1, __fmul2_rn(n2, l2)));
+    const float2 dl = __ffma2_rn(d0, l0, __ffma2_rn(d1, l1, __fmul2_rn(d2, l2)));
+    // the pair's two spectrum bins in one 8-byte load (pair order)
+    const float2 s = __ldg(reinterpret_cast<const float2 *>(sp) + j + 8 * i);
     const float2 e = make_float2(ex2_approx(-tl.x), ex2_approx(-tl.y));
     const float2 ph = make_float2(phi_pc_lazy(dl.x), phi_pc_lazy(dl.y));
     const float2 w = __fmul2_rn(__fmul2_rn(s, e), ph);
-    acc[0] = __ffma2_rn(b.cs[0], w, acc[0]);
-    acc[1] = __ffma2_rn(b.cs[1], w, acc[1]);
-    acc[2] = __ffma2_rn(b.cs[2], w, acc[2]);
-    acc[3] = __ffma2_rn(b.hw[0], w, acc[3]);
-    acc[4] = __ffma2_rn(b.hw[1], w, acc[4]);
-    acc[5] = __ffma2_rn(b.hw[2], w, acc[5]);
+    acc[0] = __ffma2_rn(c0, w, acc[0]);
+    acc[1] = __ffma2_rn(c1, w, acc[1]);
+    acc[2] = __ffma2_rn(c2, w, acc[2]);
+    acc[3] = __ffma2_rn(w0, w, acc[3]);
+    acc[4] = __ffma2_rn(w1, w, acc[4]);
+    acc[5] = __ffma2_rn(w2, w, acc[5]);
   }
 #pragma unroll
   for (int q = 0; q < 6; q++) out[q] = acc[q].x + acc[q].y;
