@@ -865,7 +865,7 @@ def run_art(args):
         "e2e": {"value": float(steps_per_pass) / te, "unit": UNIT, "h2d_bytes_per_step": int(planes.nbytes),
                 "d2h_bytes_per_step": int(6 * n * 4), "s_per_step": te},
         "clocks": clk,
-        "gpu_launches": (1 + 3 * ((art.nang + apass - 1) // apass) + 1) * args.steps,
+        "gpu_launches": (2 + 2 * ((art.nang + apass - 1) // apass)) * args.steps,
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
