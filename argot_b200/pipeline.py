@@ -256,10 +256,12 @@ class Problem:
         s_rates.wait_stream(main)
         try:
             self.stream = s_march
+            if not keep_rays:
+                # every ray of the group in one launch: the walk over all
+                # target blocks fills the GPU where one part's would not
+                self.emit(self.groups[0], rays)
             events = []
             for g, r, t in views:
-                if not keep_rays:
-                    self.emit(g, r)
                 self.march(g, r, t, precision, crossings)
                 e = torch.cuda.Event()
                 e.record(s_march)
