@@ -273,6 +273,10 @@ def reference_gpu_sample(wl, target_rays: int = 2_000_000, seed: int = 1, reps: 
         # the same loop with this library's drop-in entry points linked in
         from argot_b200 import _lib as L
         R.use_entry_points(L.load())
+        # a first pass warms the library's pools and modules; the second is
+        # timed (the reference's entry points allocate on every call anyway)
+        R.zero_rates_gpu()
+        R.run_range_gpu(im0, im0 + ncells, kernel_reps=0)
         R.zero_rates_gpu()
         ours = R.run_range_gpu(im0, im0 + ncells, kernel_reps=0)
         our_rates = R.rates_gpu()
