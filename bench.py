@@ -268,6 +268,8 @@ def reference_gpu_sample(wl, target_rays: int = 2_000_000, seed: int = 1, reps: 
         ncells = int(min(ncell, max(64, target_rays / per_cell)))
         im0 = int(rng.integers(0, ncell - ncells + 1))
         R.zero_rates_gpu()
+        R.run_range_gpu(im0, im0 + ncells, kernel_reps=0)  # warm-up (module loading)
+        R.zero_rates_gpu()
         out = R.run_range_gpu(im0, im0 + ncells, kernel_reps=reps, want=("seg",))
         ref_rates = R.rates_gpu()
         # the same loop with this library's drop-in entry points linked in
