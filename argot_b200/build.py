@@ -76,7 +76,27 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+    build_legacy(verbose)
     return LIB
+
+
+LEGACY_SRC = os.path.join(HERE, "legacy", "legacy.c")
+LEGACY_LIB = os.path.join(HERE, "libargot_b200_legacy.so")
+
+
+def build_legacy(verbose: bool = False) -> str:
+    """libargot_b200_legacy.so: the older entry-point names
+    (include/argot_b200_legacy.h) forwarded to libargot_b200.so, found next
+    to it at run time."""
+    deps = [LEGACY_SRC, LIB, os.path.join(INCLUDE, "argot_b200_legacy.h"), os.path.join(INCLUDE, "argot_b200.h")]
+    if not _stale(LEGACY_LIB, deps):
+        return LEGACY_LIB
+    cmd = [os.environ.get("CC", "gcc"), "-O2", "-fPIC", "-shared", "-I" + INCLUDE, LEGACY_SRC, "-o", LEGACY_LIB,
+           "-L" + HERE, "-l:libargot_b200.so", "-Wl,-rpath,$ORIGIN", "-Wl,--no-undefined"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return LEGACY_LIB
 
 
 if __name__ == "__main__":

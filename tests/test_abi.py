@@ -135,3 +135,25 @@ def test_dropin_failure_is_logged_to_proc_file(tmp_path):
     libc.fclose(fp)
     text = log.read_text()
     assert "calc_optical_depth_cuda" in text and "(-1)" in text
+
+
+def test_legacy_names_forward_to_the_library():
+    """libargot_b200_legacy.so exports ARGOT's older GPU entry-point names
+    (calc_optical_depth, calc_photoion_rate) and forwards them: the status
+    lands in the main library's argot_b200_last_error."""
+    import ctypes as C
+    from argot_b200 import _lib as L
+    lib = L.load()
+    legacy = C.CDLL(os.path.join(ROOT, "argot_b200", "libargot_b200_legacy.so"), mode=C.RTLD_LOCAL)
+    for name in ("calc_optical_depth", "calc_photoion_rate"):
+        assert hasattr(legacy, name)
+    text = open(os.path.join(ROOT, "include", "argot_b200_legacy.h")).read()
+    assert set(re.findall(r"ARGOT_B200_API\s+void\s+(\w+)\s*\(", text)) == {"calc_optical_depth",
+                                                                          "calc_photoion_rate"}
+    lib.argot_b200_set_dropin_march_mode(0)
+    legacy.calc_optical_depth(None, None, None, None)
+    assert lib.argot_b200_last_error() == L.EINVAL
+    lib.argot_b200_set_dropin_march_mode(0)
+    assert lib.argot_b200_last_error() == 0
+    legacy.calc_photoion_rate(None, None, None, None, None)
+    assert lib.argot_b200_last_error() == L.EINVAL

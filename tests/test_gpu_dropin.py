@@ -133,3 +133,29 @@ def test_dropin_rates_vs_reference(cuda_ok):
                                 C.addressof(cp), C.addressof(run))
     back2 = mesh.cpu().numpy().view(np.dtype(abi.FluidMesh))["prev_chem"]["GammaHI"]
     assert np.allclose(back2, 2 * want[0], rtol=1e-6)
+
+
+def test_legacy_calc_optical_depth_bitwise(cuda_ok):
+    """the older name (libargot_b200_legacy.so) runs the same march"""
+    import os
+    from argot_b200 import _lib as L, abi
+    from conftest import ROOT
+    lib = L.load()
+    legacy = C.CDLL(os.path.join(ROOT, "argot_b200", "libargot_b200_legacy.so"), mode=C.RTLD_LOCAL)
+    g = golden("golden_march.npz")
+    edge = int(g["edge"])
+    _, mesh = _mesh_dev(tuple(g[k] for k in ("dens", "fHI", "fHeI", "fHeII")))
+    segs = g["seg"]
+    seg = np.zeros(len(segs), dtype=np.dtype(abi.RaySegment))
+    seg["ray_indx"] = np.arange(len(segs))
+    for i, k in enumerate(("xpos_start", "ypos_start", "zpos_start", "xpos_end", "ypos_end", "zpos_end")):
+        seg[k] = segs[:, i]
+    run = _run_param(edge, float(g["lunit"]), float(g["denstonh"]), nseg=len(segs))
+    cp, cm = _cuda(torch.cuda.current_stream().cuda_stream)
+    cm[0].mesh_dev = mesh.data_ptr()
+    lib.argot_b200_set_dropin_march_mode(0)
+    legacy.calc_optical_depth(C.c_void_p(seg.ctypes.data), C.c_void_p(C.addressof(cm)), C.c_void_p(C.addressof(cp)),
+                              C.c_void_p(C.addressof(run)))
+    assert lib.argot_b200_last_error() == 0
+    got = np.stack([seg["optical_depth_HI"], seg["optical_depth_HeI"], seg["optical_depth_HeII"]], 1)
+    assert np.array_equal(got, g["tau"])
