@@ -68,6 +68,7 @@ SIGNATURES = {
     "argot_b200_set_dropin_march_mode": (i32, [i32]),
     "smooth_photoion_rate": (None, [vp, vp, vp, vp, vp]),
     "calc_diffuse_photon_radiation": (None, [vp, vp, vp, vp, vp, vp, vp]),
+    "argot_b200_run_group": (i32, [GP, vp, vp, u64, u64, vp, vp, u64, vp, vp, i32, i32, i32, i32, vp, vp, vp]),
     "argot_b200_art_angle_table": (i32, [i32, vp, vp, vp]),
     "argot_b200_art_step_factors": (None, [vp]),
     "argot_b200_art_create": (i32, [vp, vp, i32, vp, vp]),

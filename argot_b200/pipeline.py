@@ -233,6 +233,19 @@ class Problem:
             self.rates(g, rays, tau, rates6, mode)
         return rates6
 
+    def part_count(self, n: int) -> int:
+        """the number of parts argot_b200_run_group cuts the single group
+        into for n (its block ranges of about equal ray counts)"""
+        g = self.groups[0]
+        off = np.asarray(self.blk_off_host, dtype=np.int64)
+        cuts = [g.b0]
+        for p in range(1, n):
+            want = off[g.b0] + int(float(off[g.b1] - off[g.b0]) * p / n)
+            b = int(np.searchsorted(off[cuts[-1]:g.b1], want, side="left")) + cuts[-1]
+            if cuts[-1] < b < g.b1:
+                cuts.append(b)
+        return len(cuts)
+
     def parts(self, rays, tau, n: int):
         """The single group cut into about n parts along its blocks, each with
         its views of the ray buffer (offset base) and of the column buffer
@@ -247,32 +260,14 @@ class Problem:
         return out
 
     def _run_overlapped(self, precision, mode, rates6, rays, tau, crossings, keep_rays, n):
-        if getattr(self, "_ovl", None) is None or self._ovl[0] != (n, rays.data_ptr(), tau.data_ptr()):
-            self._ovl = ((n, rays.data_ptr(), tau.data_ptr()), self.parts(rays, tau, n),
-                         torch.cuda.Stream(self.device), torch.cuda.Stream(self.device))
-        _, views, s_march, s_rates = self._ovl
-        main = self.stream
-        s_march.wait_stream(main)
-        s_rates.wait_stream(main)
-        try:
-            self.stream = s_march
-            if not keep_rays:
-                # every ray of the group in one launch: the walk over all
-                # target blocks fills the GPU where one part's would not
-                self.emit(self.groups[0], rays)
-            events = []
-            for g, r, t in views:
-                self.march(g, r, t, precision, crossings)
-                e = torch.cuda.Event()
-                e.record(s_march)
-                events.append(e)
-            self.stream = s_rates
-            for (g, r, t), e in zip(views, events):
-                s_rates.wait_event(e)
-                self.rates(g, r, t, rates6, mode)
-        finally:
-            self.stream = main
-        main.wait_stream(s_rates)
+        """one call of argot_b200_run_group over the single group"""
+        g = self.groups[0]
+        if getattr(self, "_blk_off_host_u64", None) is None:
+            self._blk_off_host_u64 = np.ascontiguousarray(self.blk_off_host, dtype=np.uint64)
+        L.check(self.lib.argot_b200_run_group(
+            C.byref(self.grid), _p(self.packed), self._dtree, g.b0, g.b1, _p(self.blk_off),
+            self._blk_off_host_u64.ctypes.data, g.base, _p(rays), _p(tau), 0 if keep_rays else 1, precision, mode,
+            n, _p(rates6), _p(crossings), self.sp), "run_group")
         return rates6
 
     def close(self):

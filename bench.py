@@ -501,7 +501,7 @@ def run_ours(args):
     hbm, bf16, peak_kind = measured_peaks()
     alg_bytes = 16.0 * n_cross + 36.0 * nray_mine
     achieved = alg_bytes / t_march / 1e9
-    launches_per_step = (2 * len(pb.parts(rays, tau, overlap)) if overlap > 1
+    launches_per_step = (2 * pb.part_count(overlap) if overlap > 1
                          else len(pb.groups) * (2 + (0 if single else 1)))
 
     # end to end through the C ABI from pinned host buffers (the timed

@@ -290,6 +290,22 @@ ARGOT_B200_API int argot_b200_photoion_rays(const argot_b200_grid *g, const void
                              const float *tau_dev, int mode, float *rates6_dev,
                              void *stream);
 
+/* The device fast path of one ray group in one call: optionally the ray
+ * generation (emit = 1), then march and rates, the group's blocks [b0, b1)
+ * cut into `parts` ranges of about equal ray counts (blk_offsets_host, the
+ * host copy of blk_offsets_dev); the march of part p+1 runs on one internal
+ * stream while the rates of part p run on another, so the latency-bound
+ * march and the SFU-bound rates share the GPU.  rays_dev / tau_dev hold the
+ * group's rays from `base` (tau: part p's three column planes start at
+ * 3 x its first ray).  The result equals the separate calls bit for bit;
+ * `stream` is ordered after all of it (and may be under graph capture). */
+ARGOT_B200_API int argot_b200_run_group(const argot_b200_grid *g, const void *packed_dev,
+                                        const argot_b200_dev_tree *t, uint64_t b0, uint64_t b1,
+                                        const uint64_t *blk_offsets_dev, const uint64_t *blk_offsets_host,
+                                        uint64_t base, uint32_t *rays_dev, float *tau_dev, int emit,
+                                        int precision, int mode, int parts, float *rates6_dev,
+                                        unsigned long long *crossings_dev, void *stream);
+
 /* smooth_photoion_rate (src/smooth_photoion_rate.c:27-1588, single rank):
  * the 27-point smoothing of the six rate planes (layout of rates6 above),
  * centre weighted by 30, normalised by 1/56, in the reference's order and

@@ -157,3 +157,20 @@ def test_legacy_names_forward_to_the_library():
     assert lib.argot_b200_last_error() == 0
     legacy.calc_photoion_rate(None, None, None, None, None)
     assert lib.argot_b200_last_error() == L.EINVAL
+
+
+def test_run_group_rejects_bad_arguments():
+    import ctypes as C
+    from argot_b200 import _lib as L
+    from argot_b200.pipeline import unit_box_grid
+    lib = L.load()
+    g = unit_box_grid(8, 1.0, 1.0)
+    off = np.zeros(17, np.uint64)
+    # no buffers
+    assert lib.argot_b200_run_group(C.byref(g), None, None, 0, 1, None, off.ctypes.data, 0, None, None, 0, 1, 1,
+                                    4, None, None, None) == L.EINVAL
+    # parts out of range, emit not 0/1
+    fake = C.c_void_p(16)
+    for parts, emit in ((0, 0), (5000, 0), (4, 2)):
+        assert lib.argot_b200_run_group(C.byref(g), fake, fake, 0, 1, fake, off.ctypes.data, 0, fake, fake, emit, 1,
+                                        1, parts, fake, None, None) == L.EINVAL
