@@ -45,6 +45,9 @@ METRIC = "ray-cell crossings/s (march+stitch+rates, 1 B200)"
 # for 6.030e10 crossings); the workloads here are too large to capture, so
 # `traffic` scales this figure.
 MARCH_DRAM_BYTES_PER_CROSSING = 2.141
+# the same capture's L2 bytes (lts__t_bytes.sum, 401.3 GB over the launch's
+# 6.030e10 crossings): what the L2 serves per crossing
+MARCH_L2_BYTES_PER_CROSSING = 6.654
 UNIT = "crossings/s"
 
 
@@ -539,8 +542,9 @@ def run_ours(args):
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": f"{peak_kind} hbm_gbs",
                      "traffic": MARCH_DRAM_BYTES_PER_CROSSING * n_cross,
+                     "l2_traffic": MARCH_L2_BYTES_PER_CROSSING * n_cross,
                      "traffic_source": "ncu DRAM bytes per crossing on 256^3 / 16 sources "
-                                       "(2.141 B), scaled by this launch's crossings",
+                                       "(2.141 B; L2 6.654 B), scaled by this launch's crossings",
                      "algorithmic_bytes": alg_bytes,
                      "bytes_model": "16 B per crossing + 36 B per ray"},
         "clocks": clk,
