@@ -91,7 +91,10 @@ SOURCES = [
     "diffuse_photon/diffuse_photon_mpi.c",
 ]
 
-EDGES = (16, 32, 48, 64, 96, 128, 192, 256)
+# 19: a ragged mesh (no axis a multiple of the 2x4x4 target blocks); 24: an
+# even edge that is no power of two (the reference's ART pass groups its
+# start rays 2x2, set_start_pos.c:88, so it needs even edges)
+EDGES = (16, 19, 24, 32, 48, 64, 96, 128, 192, 256)
 # the reference's GPU build: the test problem and the benchmark workloads
 GPU_EDGES = (16, 64, 128, 192, 256)
 

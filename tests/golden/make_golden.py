@@ -14,6 +14,9 @@ golden_march.npz    16^3 lognormal mesh; segments incl. edge cases
 golden_path.npz     16^3 mesh, 6 sources: the reference's light rays for
                     every cell (target, source position, spectrum sum,
                     columns) and per-cell rates (one thread)
+golden_path_ragged.npz
+                    the same on a ragged 19^3 mesh (no axis a multiple of
+                    the 2x4x4 target blocks), 7 sources, opening angle 0.6
 """
 import os
 import sys
@@ -56,6 +59,18 @@ def edge_case_segments(edge: int, rng) -> np.ndarray:
     return np.asarray(segs + rnd, np.float32)
 
 
+def path_fixture(R, wl, edge, name):
+    R.set_sources(wl.src_type, wl.src_param, wl.src_pos, wl.src_rate)
+    R.zero_rates()
+    out = R.run_range(0, edge ** 3, True, want=("tgt", "src", "seg", "tau", "spec_sum"))
+    rates = R.get_rates()
+    np.savez_compressed(os.path.join(OUT, name), edge=edge, dens=wl.dens, fHI=wl.fHI,
+                        fHeI=wl.fHeI, fHeII=wl.fHeII, src_pos=wl.src_pos, src_rate=wl.src_rate,
+                        src_type=wl.src_type, src_param=wl.src_param, theta=wl.theta,
+                        lunit=wl.lunit, denstonh=wl.denstonh, tgt=out["tgt"], src=out["src"],
+                        seg=out["seg"], tau=out["tau"], spec_sum=out["spec_sum"], rates=rates)
+
+
 def main():
     rng = np.random.default_rng(20261203)
     edge = 16
@@ -83,15 +98,13 @@ def main():
                         denstonh=wl.denstonh)
 
     # the whole path on every cell
-    R.set_sources(wl.src_type, wl.src_param, wl.src_pos, wl.src_rate)
-    R.zero_rates()
-    out = R.run_range(0, edge ** 3, True, want=("tgt", "src", "seg", "tau", "spec_sum"))
-    rates = R.get_rates()
-    np.savez_compressed(os.path.join(OUT, "golden_path.npz"), edge=edge, dens=wl.dens, fHI=wl.fHI,
-                        fHeI=wl.fHeI, fHeII=wl.fHeII, src_pos=wl.src_pos, src_rate=wl.src_rate,
-                        src_type=wl.src_type, src_param=wl.src_param, theta=wl.theta,
-                        lunit=wl.lunit, denstonh=wl.denstonh, tgt=out["tgt"], src=out["src"],
-                        seg=out["seg"], tau=out["tau"], spec_sum=out["spec_sum"], rates=rates)
+    path_fixture(R, wl, edge, "golden_path.npz")
+    wl = W.tiny(19, 7, seed=5)
+    wl.theta = 0.6
+    R = RefLib(19)
+    R.init(wl.lunit, wl.denstonh, wl.theta, 1)
+    R.set_mesh(*wl.fields())
+    path_fixture(R, wl, 19, "golden_path_ragged.npz")
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)))

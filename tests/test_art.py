@@ -109,7 +109,7 @@ def _rel(got, want):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("edge", [16, 32])
+@pytest.mark.parametrize("edge", [16, 24, 32])
 def test_art_rates_match_reference(cuda_ok, edge):
     R, lunit, denstonh = _ref(edge)
     planes = _fields(edge, 7 * edge)

@@ -1,6 +1,7 @@
 """Batching: problems of uneven size (mesh edges, source counts, density
-contrasts) in one persistent launch, directly and as a replayed CUDA graph,
-under every configuration the autotuner may pick.  Every problem's rates
+contrasts; 19^3 is ragged, no axis a multiple of the 2x4x4 target blocks)
+in one persistent launch, directly and as a replayed CUDA graph, under
+every configuration the autotuner may pick.  Every problem's rates
 must equal the problem run alone (march + EXACT_F32 rates) bit for bit."""
 import numpy as np
 import pytest
@@ -12,7 +13,7 @@ def _workloads():
     from argot_b200 import workload as W
     rng = np.random.default_rng(12)
     out = []
-    for i, (edge, nsrc) in enumerate([(16, 4), (24, 40), (32, 12), (20, 64), (40, 8), (28, 24)]):
+    for i, (edge, nsrc) in enumerate([(16, 4), (24, 40), (32, 12), (20, 64), (40, 8), (28, 24), (19, 10)]):
         out.append(W._lognormal_ionized(f"b{i}", edge, nsrc, float(rng.uniform(0.5, 1.5)), 1e49, 1e51,
                                         100 + i))
     return out

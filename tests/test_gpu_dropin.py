@@ -55,10 +55,11 @@ def _cuda(stream):
     return cp, cm
 
 
-def test_calc_optical_depth_cuda_bitwise(cuda_ok):
+@pytest.mark.parametrize("name", ["golden_march.npz", "golden_path_ragged.npz"])
+def test_calc_optical_depth_cuda_bitwise(cuda_ok, name):
     from argot_b200 import _lib as L, abi
     lib = L.load()
-    g = golden("golden_march.npz")
+    g = golden(name)
     edge = int(g["edge"])
     fields = tuple(g[k] for k in ("dens", "fHI", "fHeI", "fHeII"))
     _, mesh = _mesh_dev(fields)
@@ -87,12 +88,13 @@ def test_calc_optical_depth_cuda_bitwise(cuda_ok):
     assert np.max(np.abs(got2 - g["tau"])[ok] / g["tau"][ok]) < 3e-4
 
 
-def test_dropin_rates_vs_reference(cuda_ok):
+@pytest.mark.parametrize("edge", [16, 19])
+def test_dropin_rates_vs_reference(cuda_ok, edge):
     """zero_out_photoion_rate_cuda + calc_photoion_rate_cuda on the
-    reference's own light rays, against the reference's calc_photoion_rate."""
+    reference's own light rays, against the reference's calc_photoion_rate
+    (19^3: a ragged mesh)."""
     from argot_b200 import _lib as L, abi, workload as W
     lib = L.load()
-    edge = 16
     wl = W.tiny(edge, 5, seed=77)
     R = ref_lib(edge)
     R.init(wl.lunit, wl.denstonh, 0.5, 1)

@@ -57,7 +57,7 @@ def test_march_segments_kahan_vs_fp64(cuda_ok, oracle):
     assert tau_nu_error(tau, t64) < tau_nu_error(g["tau"], t64)
 
 
-@pytest.mark.parametrize("edge,nsrc,theta", [(16, 6, 0.5), (32, 24, 0.5), (32, 40, 0.7)])
+@pytest.mark.parametrize("edge,nsrc,theta", [(16, 6, 0.5), (19, 7, 0.6), (32, 24, 0.5), (32, 40, 0.7)])
 def test_ray_lists_match_reference_tree(cuda_ok, edge, nsrc, theta):
     """Device tree walk emits, per target cell, the reference's rays in the
     reference's order (setup_light_ray_to)."""
@@ -82,6 +82,35 @@ def test_ray_lists_match_reference_tree(cuda_ok, edge, nsrc, theta):
     assert np.array_equal(pos4[emit[mine], :3], out["src"][ref])
     # and the columns of the reference-order march are the reference's
     assert np.array_equal(tau[mine], out["tau"][ref])
+
+
+def test_ragged_golden_device_path(cuda_ok):
+    """The whole device path on the ragged 19^3 golden problem (no axis a
+    multiple of the 2x4x4 target blocks): per cell, the reference's rays in
+    the reference's order, its columns bit for bit, its rates within the
+    FP64 kernel's tolerance."""
+    from argot_b200 import workload as W
+    from argot_b200 import _lib as L
+    from gpu_util import run_problem
+    g = golden("golden_path_ragged.npz")
+    edge = int(g["edge"])
+    wl = W.tiny(edge, len(g["src_rate"]), seed=5)
+    wl.theta = float(g["theta"])
+    for k in ("dens", "fHI", "fHeI", "fHeII", "src_pos", "src_rate"):
+        assert np.array_equal(getattr(wl, k), g[k]), k
+    pb, emit, tgt, tau, rates = run_problem(wl, L.PRECISION_REFERENCE, L.RATE_EXACT_F64)
+    assert len(emit) == len(g["tgt"])
+    pos4, _ = pb.emitters()
+    cell = lambda t: (t[:, 0].astype(np.int64) * edge + t[:, 1]) * edge + t[:, 2]  # noqa: E731
+    mine = np.argsort(cell(tgt), kind="stable")
+    ref = np.argsort(cell(g["tgt"]), kind="stable")
+    assert np.array_equal(cell(tgt)[mine], cell(g["tgt"])[ref])
+    assert np.array_equal(pos4[emit[mine], :3], g["src"][ref])
+    assert np.array_equal(tau[mine], g["tau"][ref])
+    # the device exp (<= 1 ulp in double) moves the float rates by a few ulps
+    want = g["rates"].astype(np.float64)
+    rel = np.abs(rates - want) / np.maximum(np.abs(want), 1e-300)
+    assert rel.max() < 2e-6, rel.max(axis=1)
 
 
 def test_march_rays_kahan_vs_fp64(cuda_ok, oracle):

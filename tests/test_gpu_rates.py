@@ -36,33 +36,36 @@ def test_exact_f64_matches_oracle_on_device_rays(cuda_ok, oracle):
     assert rel.max() < F64_RTOL, rel.max(axis=1)
 
 
-def test_exact_f64_end_to_end_vs_reference_build(cuda_ok):
+@pytest.mark.parametrize("edge,nsrc,seed", [(32, 24, 31), (19, 9, 37)])
+def test_exact_f64_end_to_end_vs_reference_build(cuda_ok, edge, nsrc, seed):
     """Whole path on the device (tree walk, reference-order march, FP64
-    rates) against ARGOT's own C on the same seeded 32^3 problem."""
+    rates) against ARGOT's own C on the same seeded problem; 19^3 is a
+    ragged mesh (no axis a multiple of the 2x4x4 target blocks)."""
     from argot_b200 import workload as W
     from argot_b200 import _lib as L
     from gpu_util import run_problem
-    wl = W.tiny(32, 24, seed=31)
+    wl = W.tiny(edge, nsrc, seed=seed)
     _, _, _, _, rates = run_problem(wl, L.PRECISION_REFERENCE, L.RATE_EXACT_F64)
-    R = ref_lib(32)
+    R = ref_lib(edge)
     R.init(wl.lunit, wl.denstonh, wl.theta, 1)
     R.set_mesh(*wl.fields())
     R.set_sources(wl.src_type, wl.src_param, wl.src_pos, wl.src_rate)
     R.zero_rates()
-    R.run_range(0, 32 ** 3, True, want=())
+    R.run_range(0, edge ** 3, True, want=())
     want = R.get_rates()
     rel = np.abs(rates - want) / np.maximum(np.abs(want), 1e-300)
     assert rel.max() < F64_RTOL, rel.max(axis=1)
 
 
-def test_exact_f32_vs_fp64_oracle(cuda_ok, oracle):
+@pytest.mark.parametrize("edge", [32, 19])
+def test_exact_f32_vs_fp64_oracle(cuda_ok, oracle, edge):
     from argot_b200 import workload as W
     from argot_b200 import _lib as L
     from gpu_util import run_problem, ray_segments
     from oracle.oracle import unit_box_grid
-    wl = W.tiny(32, 16, seed=41, sigma_ln=1.2)
+    wl = W.tiny(edge, 16, seed=41, sigma_ln=1.2)
     pb, emit, tgt, tau, rates = run_problem(wl, L.PRECISION_KAHAN, L.RATE_EXACT_F32)
-    grid = unit_box_grid(32, wl.lunit, wl.denstonh)
+    grid = unit_box_grid(edge, wl.lunit, wl.denstonh)
     segs = ray_segments(pb, emit, tgt)
     t64 = oracle.march_f64(grid, wl.fields(), segs)
     want = oracle.photoion_f64(grid, wl.fields(), t64, tgt, segs[:, :3], _ref_spectra(pb, emit))

@@ -63,8 +63,9 @@ def test_march_f64_close_to_reference(oracle):
     assert np.allclose(t[inside], length[inside], rtol=1e-12, atol=1e-12)
 
 
-def test_path_golden_columns_and_rates(oracle):
-    g = golden("golden_path.npz")
+@pytest.mark.parametrize("name", ["golden_path.npz", "golden_path_ragged.npz"])
+def test_path_golden_columns_and_rates(oracle, name):
+    g = golden(name)
     grid = _grid(g)
     tau = oracle.march_f32ref(grid, _fields(g), g["seg"])
     assert np.array_equal(tau, g["tau"])
@@ -120,18 +121,21 @@ def test_stitch_single_rank(oracle):
 
 
 # ---------------------------------------------------------- live reference
-def test_restatement_equals_reference_build(oracle):
+@pytest.mark.parametrize("edge,nsrc,seed,theta", [(16, 5, 99, 0.5), (19, 6, 23, 0.6)])
+def test_restatement_equals_reference_build(oracle, edge, nsrc, seed, theta):
     """Ref-order restatement vs the reference compiled here, bit for bit, on
-    a fresh seeded problem (march, stitching, rates)."""
+    a fresh seeded problem (march, stitching, rates); 19^3 is a ragged mesh
+    (no axis a multiple of the 2x4x4 target blocks)."""
     from argot_b200 import workload as W
-    wl = W.tiny(16, 5, seed=99)
-    R = ref_lib(16)
+    wl = W.tiny(edge, nsrc, seed=seed)
+    wl.theta = theta
+    R = ref_lib(edge)
     R.init(wl.lunit, wl.denstonh, wl.theta, 1)
     R.set_mesh(*wl.fields())
     R.set_sources(wl.src_type, wl.src_param, wl.src_pos, wl.src_rate)
     R.zero_rates()
-    out = R.run_range(0, 16 ** 3, True, want=("tgt", "src", "seg", "tau", "spectra"))
-    grid = unit_box_grid(16, wl.lunit, wl.denstonh)
+    out = R.run_range(0, edge ** 3, True, want=("tgt", "src", "seg", "tau", "spectra"))
+    grid = unit_box_grid(edge, wl.lunit, wl.denstonh)
     tau = oracle.march_f32ref(grid, wl.fields(), out["seg"])
     assert np.array_equal(tau, out["tau"])
     rates = oracle.photoion_f64ref(grid, wl.fields(), out["tau"], out["tgt"], out["src"],
