@@ -580,6 +580,7 @@ int art_dropin(run_param *run, cuda_mem_space *cm, cuda_param *cp, host_diffuse_
   const uint64_t n = (uint64_t)g.nx * g.ny * g.nz;
   if (n >= (1ull << 32)) return ARGOT_B200_EINVAL;
   g.dx = run->delta_x; g.dy = run->delta_y; g.dz = run->delta_z;
+  if (!(g.dx > 0.f && g.dy > 0.f && g.dz > 0.f)) return ARGOT_B200_EINVAL;
   g.xminl = run->xmin_local; g.yminl = run->ymin_local; g.zminl = run->zmin_local;
   g.xmaxl = run->xmax_local; g.ymaxl = run->ymax_local; g.zmaxl = run->zmax_local;
   g.xmin = run->xmin; g.ymin = run->ymin; g.zmin = run->zmin;

@@ -70,7 +70,9 @@ int march_mode() {
   return g_march_mode;
 }
 
-GridDev grid_from_run(const run_param *r) {
+// The local mesh of run_param as the library's grid; false when its sizes
+// or cell widths are not positive.
+bool grid_from_run(const run_param *r, GridDev *out) {
   argot_b200_grid g{};
   g.nx = r->nmesh_x_local; g.ny = r->nmesh_y_local; g.nz = r->nmesh_z_local;
   g.ix0 = r->rank_x * r->nmesh_x_local;
@@ -81,7 +83,9 @@ GridDev grid_from_run(const run_param *r) {
   g.xmin_local = r->xmin_local; g.ymin_local = r->ymin_local; g.zmin_local = r->zmin_local;
   g.dx = r->delta_x; g.dy = r->delta_y; g.dz = r->delta_z;
   g.lunit = r->lunit; g.denstonh = r->denstonh;
-  return make_grid(g);
+  if (!grid_valid(&g)) return false;
+  *out = make_grid(g);
+  return true;
 }
 
 // Makes device 0 current for the call and restores the caller's device.
@@ -128,9 +132,9 @@ int join_lanes(DropinState &s, cudaStream_t caller) {
 int do_march(ray_segment *seg, cuda_mem_space *cm, cuda_param *cp, run_param *run) {
   if (!seg || !cm || !run) return ARGOT_B200_EINVAL;
   const uint64_t nseg = run->nseg;
-  const GridDev g = grid_from_run(run);
+  GridDev g;
+  if (!grid_from_run(run, &g) || !cm[0].mesh_dev) return ARGOT_B200_EINVAL;
   const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
-  if (g.nx <= 0 || g.ny <= 0 || g.nz <= 0 || !cm[0].mesh_dev) return ARGOT_B200_EINVAL;
   DeviceScope dscope;
   if (!dscope.ok) return ARGOT_B200_ECUDA;
   std::lock_guard<std::mutex> lock(g_mu);
@@ -188,9 +192,9 @@ void fill_ray_io(const light_ray *ray, light_ray_IO *io, uint64_t nray) {
 int do_rates(cuda_mem_space *cm, light_ray *ray, light_ray_IO *ray_io, cuda_param *cp, run_param *run) {
   if (!cm || !run || (run->nray && (!ray || !ray_io))) return ARGOT_B200_EINVAL;
   const uint64_t nray = run->nray;
-  const GridDev g = grid_from_run(run);
+  GridDev g;
+  if (!grid_from_run(run, &g) || !cm[0].mesh_dev) return ARGOT_B200_EINVAL;
   const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
-  if (g.nx <= 0 || g.ny <= 0 || g.nz <= 0 || !cm[0].mesh_dev) return ARGOT_B200_EINVAL;
   DeviceScope dscope;
   if (!dscope.ok) return ARGOT_B200_ECUDA;
   std::lock_guard<std::mutex> lock(g_mu);
@@ -352,10 +356,14 @@ void zero_out_photoion_rate_cuda(::cuda_mem_space *cuda_mem, ::cuda_param *this_
                                  struct run_param *this_run) {
   argot::cuda_mem_space *cm = (argot::cuda_mem_space *)cuda_mem;
   argot::run_param *run = (argot::run_param *)this_run;
-  if (!cm || !run || !cm[0].mesh_dev) { argot::dropin_status(run, "zero_out_photoion_rate_cuda", ARGOT_B200_EINVAL); return; }
+  if (!cm || !run || !cm[0].mesh_dev || run->nmesh_x_local <= 0 || run->nmesh_y_local <= 0 ||
+      run->nmesh_z_local <= 0) {
+    argot::dropin_status(run, "zero_out_photoion_rate_cuda", ARGOT_B200_EINVAL);
+    return;
+  }
   const uint64_t n = (uint64_t)run->nmesh_x_local * run->nmesh_y_local * run->nmesh_z_local;
   argot::DeviceScope dscope;
-  if (!dscope.ok) { set_status(ARGOT_B200_ECUDA); return; }
+  if (!dscope.ok) { argot::dropin_status(run, "zero_out_photoion_rate_cuda", ARGOT_B200_ECUDA); return; }
   cudaStream_t st = argot::caller_stream((argot::cuda_param *)this_cuda);
   int rc = argot::launch_zero_rates(n, cm[0].mesh_dev, st);
   if (!rc) {

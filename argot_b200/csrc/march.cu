@@ -60,8 +60,9 @@ __global__ void __launch_bounds__(256) k_walk(GridDev g, const DevNode *__restri
                                               uint64_t b0, uint64_t b1, uint64_t *__restrict__ blk_count,
                                               uint32_t *__restrict__ cell_count,
                                               const uint64_t *__restrict__ blk_off, uint64_t base,
-                                              uint32_t *__restrict__ rays) {
+                                              uint32_t *__restrict__ rays, int *__restrict__ err) {
   const int lane = threadIdx.x & 31;
+  bool bad = false;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const unsigned lt = (1u << lane) - 1u;
@@ -73,7 +74,16 @@ __global__ void __launch_bounds__(256) k_walk(GridDev g, const DevNode *__restri
     const float pz = cell_centre(g.zmin, g.iz0 + iz, g.dz);
     int blocked_until = 0;
     uint32_t mine = 0;
-    uint64_t off = kEmit ? blk_off[b] - base : 0;
+    // emission: the block's rays go to [blk_off[b], blk_off[b + 1]) - base;
+    // a ray past that range (offsets not counted for this tree and angle)
+    // is dropped and the error flag set
+    uint64_t off = 0, end = 0;
+    if (kEmit) {
+      const uint64_t a = blk_off[b], e = blk_off[b + 1];
+      if (a < base || e < a) { bad = true; continue; }
+      off = a - base;
+      end = e - base;
+    }
     int cur = 0;
     while (cur < n_nodes) {
       const DevNode nd = nodes[cur];
@@ -86,7 +96,11 @@ __global__ void __launch_bounds__(256) k_walk(GridDev g, const DevNode *__restri
       const unsigned mopn = __ballot_sync(0xffffffffu, opn);
       if (macc) {
         if (kEmit) {
-          if (acc) rays[off + __popc(macc & lt)] = ((uint32_t)cur << 5) | (uint32_t)lane;
+          const uint64_t at = off + __popc(macc & lt);
+          if (acc) {
+            if (at < end) rays[at] = ((uint32_t)cur << 5) | (uint32_t)lane;
+            else bad = true;
+          }
           off += __popc(macc);
         } else {
           mine += acc;
@@ -103,7 +117,11 @@ __global__ void __launch_bounds__(256) k_walk(GridDev g, const DevNode *__restri
           for (int j = 0; j < nd.n; j++) {
             const uint32_t e = (uint32_t)(n_nodes + src_list[nd.src_first + j]);
             if (kEmit) {
-              if (opn) rays[off + __popc(mopn & lt)] = (e << 5) | (uint32_t)lane;
+              const uint64_t at = off + __popc(mopn & lt);
+              if (opn) {
+                if (at < end) rays[at] = (e << 5) | (uint32_t)lane;
+                else bad = true;
+              }
               off += __popc(mopn);
             } else {
               mine += opn;
@@ -120,6 +138,7 @@ __global__ void __launch_bounds__(256) k_walk(GridDev g, const DevNode *__restri
       if (lane == 0) blk_count[b] = tot;
     }
   }
+  if (kEmit && bad) atomicExch(err, 1);
 }
 
 // -------------------------------------------------------------- ray march
@@ -148,7 +167,8 @@ __global__ void __launch_bounds__(256, ARGOT_MARCH_MIN_CTAS) k_march_rays(GridDe
   unsigned long long steps_total = 0;
   bool bad = false;
   for (uint64_t b = b0 + warp; b < b1; b += nwarp) {
-    const uint64_t r0 = blk_off[b] - base, r1 = blk_off[b + 1] - base;
+    uint64_t r0, r1;
+    if (!block_rays(blk_off, b, base, nray, &r0, &r1)) { bad = true; continue; }
     int bix, biy, biz;
     block_cell(g, b, 0, &bix, &biy, &biz);
     for (uint64_t r = r0 + lane; r < r1; r += 32) {
@@ -352,7 +372,7 @@ int argot_b200_count_rays(const argot_b200_grid *gp, const argot_b200_dev_tree *
   const int blocks = grid_blocks_for((b1 - b0) * 32, threads);
   k_walk<false><<<blocks, threads, 0, (cudaStream_t)stream>>>(g, t->nodes, t->n_nodes, t->src_list,
                                                               t->theta_sq, b0, b1, blk_count, cell_count,
-                                                              nullptr, 0, nullptr);
+                                                              nullptr, 0, nullptr, nullptr);
   ARGOT_CUDA_TRY(cudaGetLastError());
   set_status(0);
   return 0;
@@ -402,12 +422,16 @@ int argot_b200_emit_rays(const argot_b200_grid *gp, const argot_b200_dev_tree *t
     return ARGOT_B200_EINVAL;
   }
   if (b0 == b1) { set_status(0); return 0; }
+  int dev = 0;
+  ARGOT_CUDA_TRY(cudaGetDevice(&dev));
+  int *err = err_flag(dev);
+  if (!err) { set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
   GridDev g = make_grid(*gp);
   const int threads = 256;
   const int blocks = grid_blocks_for((b1 - b0) * 32, threads);
   k_walk<true><<<blocks, threads, 0, (cudaStream_t)stream>>>(g, t->nodes, t->n_nodes, t->src_list,
                                                              t->theta_sq, b0, b1, nullptr, nullptr, blk_off,
-                                                             base, rays);
+                                                             base, rays, err);
   ARGOT_CUDA_TRY(cudaGetLastError());
   set_status(0);
   return 0;

@@ -279,4 +279,17 @@ __device__ __forceinline__ bool block_cell(const GridDev &g, uint64_t b, int lan
   return *ix < g.nx && *iy < g.ny && *iz < g.nz;
 }
 
+// The rays [r0, r1) of block b in a buffer of nray rays that starts at ray
+// `base` of the caller's offsets; false when blk_off[b], blk_off[b + 1] do
+// not lie in order within [base, base + nray] (the caller's offsets do not
+// match its buffers): the block is then skipped and the error flag set.
+__device__ __forceinline__ bool block_rays(const uint64_t *__restrict__ blk_off, uint64_t b, uint64_t base,
+                                           uint64_t nray, uint64_t *r0, uint64_t *r1) {
+  const uint64_t a = blk_off[b], e = blk_off[b + 1];
+  if (a < base || e < a || e - base > nray) return false;
+  *r0 = a - base;
+  *r1 = e - base;
+  return true;
+}
+
 }  // namespace argot

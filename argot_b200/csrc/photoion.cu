@@ -6,6 +6,7 @@
 namespace argot {
 
 int grid_blocks_for_rates(uint64_t n, int threads);
+int *err_flag(int dev);
 
 // the tables of this translation unit's rate kernels
 int ensure_tables(int device) { return ensure_rate_tables(device); }
@@ -24,7 +25,8 @@ __global__ void __launch_bounds__(32 * kRateWarps)
                   const double *__restrict__ spec64, const float *__restrict__ specn,
                   const double *__restrict__ total, uint64_t b0, uint64_t b1,
                   const uint64_t *__restrict__ blk_off, uint64_t base, const uint32_t *__restrict__ rays,
-                  uint64_t nray, const float *__restrict__ tau, float *__restrict__ rates6) {
+                  uint64_t nray, const float *__restrict__ tau, float *__restrict__ rates6,
+                  int *__restrict__ err) {
   __shared__ double buf[kRateWarps][32][7];
   __shared__ int tl[kRateWarps][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -44,7 +46,11 @@ __global__ void __launch_bounds__(32 * kRateWarps)
     }
     int bix, biy, biz;
     block_cell(g, b, 0, &bix, &biy, &biz);
-    const uint64_t r0 = blk_off[b] - base, r1 = blk_off[b + 1] - base;
+    uint64_t r0, r1;
+    if (!block_rays(blk_off, b, base, nray, &r0, &r1)) {
+      if (lane == 0) atomicExch(err, 1);
+      continue;
+    }
     for (uint64_t rc = r0; rc < r1; rc += 32) {
       const uint64_t r = rc + lane;
       int t = -1;
@@ -116,7 +122,7 @@ __global__ void __launch_bounds__(32 * kF32Warps, ARGOT_RATE_MIN_CTAS)
                const float *__restrict__ specn, const double *__restrict__ total, uint64_t b0, uint64_t b1,
                const uint64_t *__restrict__ blk_off, uint64_t base, const uint32_t *__restrict__ rays,
                uint64_t nray, const float *__restrict__ tau, float *__restrict__ rates6,
-               const float *__restrict__ pred) {
+               const float *__restrict__ pred, int *__restrict__ err) {
   __shared__ BinPair s_pairs[kBinPairs];
   __shared__ RateWarpSmem s_w[kF32Warps];
   load_bin_pairs(s_pairs);
@@ -124,9 +130,15 @@ __global__ void __launch_bounds__(32 * kF32Warps, ARGOT_RATE_MIN_CTAS)
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t b = b0 + warp; b < b1; b += nwarp)
-    rate_block_f32<kServed>(g, raw, emit_pos, specn, total, s_pairs, b, blk_off[b] - base, blk_off[b + 1] - base,
-                            rays, nray, tau, rates6, s_w[wib], lane, pred);
+  for (uint64_t b = b0 + warp; b < b1; b += nwarp) {
+    uint64_t r0, r1;
+    if (!block_rays(blk_off, b, base, nray, &r0, &r1)) {
+      if (lane == 0) atomicExch(err, 1);
+      continue;
+    }
+    rate_block_f32<kServed>(g, raw, emit_pos, specn, total, s_pairs, b, r0, r1, rays, nray, tau, rates6, s_w[wib],
+                            lane, pred);
+  }
 }
 
 // The FP32 rates of blocks [b0, b1) where the rays flagged in pred (7
@@ -135,10 +147,10 @@ __global__ void __launch_bounds__(32 * kF32Warps, ARGOT_RATE_MIN_CTAS)
 int launch_rate_f32_served(const GridDev &g, const float4 *raw, const float4 *emit_pos, const float *specn,
                            const double *total, uint64_t b0, uint64_t b1, const uint64_t *blk_off, uint64_t base,
                            const uint32_t *rays, uint64_t nray, const float *tau, float *rates6, const float *pred,
-                           cudaStream_t st) {
+                           int *err, cudaStream_t st) {
   if (b0 >= b1) return 0;
   k_rate_f32<true><<<grid_blocks_for_rates((b1 - b0) * 32, 32 * kF32Warps), 32 * kF32Warps, 0, st>>>(
-      g, raw, emit_pos, specn, total, b0, b1, blk_off, base, rays, nray, tau, rates6, pred);
+      g, raw, emit_pos, specn, total, b0, b1, blk_off, base, rays, nray, tau, rates6, pred, err);
   ARGOT_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -267,6 +279,8 @@ extern "C" int argot_b200_photoion_rays(const argot_b200_grid *gp, const void *p
   ARGOT_CUDA_TRY(cudaGetDevice(&dev));
   int rc = ensure_tables(dev);
   if (rc) return rc;
+  int *err = err_flag(dev);
+  if (!err) { set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
   GridDev g = make_grid(*gp);
   const uint64_t ncell = (uint64_t)gp->nx * gp->ny * gp->nz;
   const float4 *raw = (const float4 *)packed + ncell;
@@ -276,11 +290,11 @@ extern "C" int argot_b200_photoion_rays(const argot_b200_grid *gp, const void *p
   if (mode == ARGOT_B200_RATE_EXACT_F64)
     k_rate_blocks<ARGOT_B200_RATE_EXACT_F64><<<blocks, threads, 0, st>>>(
         g, raw, t->emit_pos, t->emit_spec64, t->emit_specn, t->emit_total, b0, b1, blk_off, base, rays, nray, tau,
-        rates6);
+        rates6, err);
   else
     k_rate_f32<false><<<grid_blocks_for_rates((b1 - b0) * 32, 32 * kF32Warps), 32 * kF32Warps, 0, st>>>(
         g, raw, t->emit_pos, t->emit_specn, t->emit_total, b0, b1, blk_off, base, rays, nray, tau, rates6,
-        nullptr);
+        nullptr, err);
   ARGOT_CUDA_TRY(cudaGetLastError());
   set_status(0);
   return 0;

@@ -42,7 +42,8 @@ int grid_blocks_for_rates(uint64_t n, int threads);
 int launch_rate_f32_served(const GridDev &g, const float4 *raw, const float4 *emit_pos, const float *specn,
                            const double *total, uint64_t b0, uint64_t b1, const uint64_t *blk_off, uint64_t base,
                            const uint32_t *rays, uint64_t nray, const float *tau, float *rates6, const float *pred,
-                           cudaStream_t st);
+                           int *err, cudaStream_t st);
+int *err_flag(int dev);
 
 constexpr int kEnvBins = 64;        // error envelope bins over predicted q
 constexpr float kEnvQLo = -7.0f;     // ... in [-7, 0]
@@ -250,7 +251,7 @@ __global__ void __launch_bounds__(32 * kSurWarps, ARGOT_SUR_PREDICT_MIN_CTAS)
                   const double *__restrict__ emit_i0, const float *__restrict__ emit_m,
                   const SurWeights *__restrict__ wts, uint64_t b0, uint64_t b1, const uint64_t *__restrict__ blk_off,
                   uint64_t base, const uint32_t *__restrict__ rays, uint64_t nray, const float *__restrict__ tau,
-                  float *__restrict__ rates6, float *__restrict__ work) {
+                  float *__restrict__ rates6, float *__restrict__ work, int *__restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   PredSmem &S = *reinterpret_cast<PredSmem *>(smem_raw);
   {
@@ -274,7 +275,11 @@ __global__ void __launch_bounds__(32 * kSurWarps, ARGOT_SUR_PREDICT_MIN_CTAS)
     double acc[6] = {0, 0, 0, 0, 0, 0};
     int bix, biy, biz;
     block_cell(g, b, 0, &bix, &biy, &biz);
-    const uint64_t r0 = blk_off[b] - base, r1 = blk_off[b + 1] - base;
+    uint64_t r0, r1;
+    if (!block_rays(blk_off, b, base, nray, &r0, &r1)) {
+      if (lane == 0) atomicExch(err, 1);
+      continue;
+    }
     for (uint64_t rc = r0; rc < r1; rc += 32) {
       // ---- phase A: per-ray parameters and quadrature nodes
       const uint64_t r = rc + lane;
@@ -439,7 +444,7 @@ __device__ __forceinline__ double beta_edge(int b) { return exp2(0.5 * (double)(
 __global__ void __launch_bounds__(32 * kSurWarps)
     k_sur_select(GridDev g, float tol, uint64_t b0, uint64_t b1, const uint64_t *__restrict__ blk_off, uint64_t base,
                  const uint32_t *__restrict__ rays, uint64_t nray, const float *__restrict__ rates6,
-                 float *__restrict__ work, unsigned long long *__restrict__ counters) {
+                 float *__restrict__ work, unsigned long long *__restrict__ counters, int *__restrict__ err) {
   __shared__ SelSmem S;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
@@ -447,13 +452,17 @@ __global__ void __launch_bounds__(32 * kSurWarps)
   const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
   unsigned long long n_sur = 0, n_exact = 0;
   for (uint64_t b = b0 + warp; b < b1; b += nwarp) {
+    uint64_t r0, r1;
+    if (!block_rays(blk_off, b, base, nray, &r0, &r1)) {
+      if (lane == 0) atomicExch(err, 1);
+      continue;
+    }
     int ix, iy, iz;
     const bool own_valid = block_cell(g, b, lane, &ix, &iy, &iz);
     const uint64_t own = own_valid ? cell_index(g, ix, iy, iz) : 0;
 #pragma unroll
     for (int s = 0; s < 6; s++) S.Sc[wib][lane][s] = own_valid ? rates6[s * ncell + own] : 0.f;
     for (int k = 0; k < kHistBins; k++) S.hist[wib][lane][k] = 0u;
-    const uint64_t r0 = blk_off[b] - base, r1 = blk_off[b + 1] - base;
     __syncwarp();
     // ---- pass 1: histogram of beta per cell
     for (uint64_t r = r0 + lane; r < r1; r += 32) {
@@ -670,6 +679,8 @@ int argot_b200_photoion_rays_surrogate(const argot_b200_grid *gp, const void *pa
   ARGOT_CUDA_TRY(cudaGetDevice(&dev));
   int rc = ensure_rate_tables(dev);
   if (rc) return rc;
+  int *err = err_flag(dev);
+  if (!err) { set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
   static std::mutex mu;
   static bool attr[64] = {false};
   {
@@ -689,13 +700,13 @@ int argot_b200_photoion_rays_surrogate(const argot_b200_grid *gp, const void *pa
   cudaStream_t st = (cudaStream_t)stream;
   k_sur_predict<<<blocks, threads, sizeof(PredSmem), st>>>(g, raw, t->emit_pos, t->emit_total, t->emit_logT,
                                                             t->emit_i0, t->emit_m, sur->dev, b0, b1, blk_off,
-                                                            base, rays, nray, tau, rates6, work);
+                                                            base, rays, nray, tau, rates6, work, err);
   ARGOT_CUDA_TRY(cudaGetLastError());
   k_sur_select<<<blocks, threads, 0, st>>>(g, sur->tol, b0, b1, blk_off, base, rays, nray, rates6, work,
-                                            counters);
+                                            counters, err);
   ARGOT_CUDA_TRY(cudaGetLastError());
   rc = launch_rate_f32_served(g, raw, t->emit_pos, t->emit_specn, t->emit_total, b0, b1, blk_off, base, rays, nray,
-                              tau, rates6, work, st);
+                              tau, rates6, work, err, st);
   if (rc) return rc;
   set_status(0);
   return 0;

@@ -137,6 +137,32 @@ def test_dropin_failure_is_logged_to_proc_file(tmp_path):
     assert "calc_optical_depth_cuda" in text and "(-1)" in text
 
 
+def test_dropins_reject_bad_mesh_sizes():
+    """Non-positive local mesh sizes or cell widths are rejected before
+    anything reaches the device.  The mesh pointer is a placeholder that is
+    never dereferenced, so this runs only where no GPU is present."""
+    import ctypes as C
+    import torch
+    from argot_b200 import _lib as L, abi
+    if torch.cuda.is_available():
+        pytest.skip("host-only argument checks")
+    lib = L.load()
+    cm = (abi.CudaMemSpace * 1)()
+    cm[0].mesh_dev = 0x1000
+    for nx, d in ((-1, 0.125), (8, 0.0), (0, 0.125)):
+        run = abi.RunParam()
+        run.nmesh_x_local, run.nmesh_y_local, run.nmesh_z_local = nx, 8, 8
+        run.delta_x = run.delta_y = run.delta_z = d
+        lib.zero_out_photoion_rate_cuda(C.addressof(cm), None, C.addressof(run))
+        assert lib.argot_b200_last_error() == (L.EINVAL if nx <= 0 else L.ECUDA), (nx, d)
+        seg = np.zeros(1, dtype=np.dtype(abi.RaySegment))
+        run.nseg = 1
+        lib.calc_optical_depth_cuda(seg.ctypes.data, C.addressof(cm), None, C.addressof(run))
+        assert lib.argot_b200_last_error() == L.EINVAL, (nx, d)
+        lib.calc_photoion_rate_cuda(C.addressof(cm), None, None, None, C.addressof(run))
+        assert lib.argot_b200_last_error() == L.EINVAL, (nx, d)
+
+
 def test_legacy_names_forward_to_the_library():
     """libargot_b200_legacy.so exports ARGOT's older GPU entry-point names
     (calc_optical_depth, calc_photoion_rate) and forwards them: the status

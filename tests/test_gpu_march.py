@@ -145,6 +145,51 @@ def test_grouped_rays_equal_single_pass(cuda_ok):
     assert np.array_equal(r1, r2)
 
 
+def test_offsets_that_do_not_match_the_buffers_are_flagged(cuda_ok):
+    """Block offsets past the caller's ray count (march, rates) or short of
+    a block's rays (emission) set the device error flag
+    and the kernels skip what does not fit.  The buffers here hold the full
+    ray count, so nothing outside them is touched even without the checks."""
+    import ctypes as C
+    import torch
+    from argot_b200 import workload as W
+    from argot_b200 import _lib as L
+    from argot_b200.pipeline import Problem, RayGroup
+    wl = W.tiny(16, 4, seed=2)
+    pb = Problem(wl)
+    g = pb.groups[0]
+    rays, tau = pb.alloc_group_buffers()
+    rates = torch.zeros(6 * pb.ncell, dtype=torch.float32, device="cuda")
+    pb.emit(g, rays)
+    pb.march(g, rays, tau)
+    pb.rates(g, rays, tau, rates)
+    torch.cuda.synchronize()
+    pb.check_device_error()
+    short = RayGroup(g.b0, g.b1, g.base, g.nray - 1)
+    for step in (lambda: pb.march(short, rays, tau), lambda: pb.rates(short, rays, tau, rates),
+                 lambda: pb.rates(short, rays, tau, rates, L.RATE_EXACT_F64)):
+        step()
+        torch.cuda.synchronize()
+        with pytest.raises(L.ArgotError):
+            pb.check_device_error()
+        pb.check_device_error()  # the flag was cleared
+    # emission: block 0's range one ray short, the later ranges shifted
+    off = pb.blk_off.clone()
+    off[1:] -= 1
+    assert int(pb.blk_count[0]) > 1
+    keep = rays.clone()
+    L.check(pb.lib.argot_b200_emit_rays(C.byref(pb.grid), pb._dtree, g.b0, g.b1, off.data_ptr(), g.base,
+                                        rays.data_ptr(), pb.sp), "emit")
+    torch.cuda.synchronize()
+    with pytest.raises(L.ArgotError):
+        pb.check_device_error()
+    # the rays of block 0 that fit are the same, the later blocks moved by one
+    n0 = int(pb.blk_count[0])
+    assert torch.equal(rays[:n0 - 1], keep[:n0 - 1])
+    assert torch.equal(rays[n0 - 1:g.nray - 1], keep[n0:g.nray])
+    pb.close()
+
+
 def test_stitch_segmented_sum(cuda_ok, oracle):
     import torch
     from argot_b200 import _lib as L
