@@ -229,7 +229,10 @@ ARGOT_B200_API int argot_b200_scan_blocks(const uint64_t *blk_count_dev, uint64_
 ARGOT_B200_API int argot_b200_scan_blocks_static(const uint64_t *blk_count_dev, uint64_t nb,
                                                  uint64_t base, uint64_t *blk_offsets_dev,
                                                  uint64_t *total, void *stream);
-/* Pass 2: write the ray words of blocks [b0, b1) at blk_offsets[b] - base. */
+/* Pass 2: write the ray words of blocks [b0, b1) at blk_offsets[b] - base.
+ * A block whose rays do not fit in [blk_offsets[b], blk_offsets[b + 1])
+ * (offsets counted for another tree or opening angle) writes only those
+ * that fit and sets the device error flag. */
 ARGOT_B200_API int argot_b200_emit_rays(const argot_b200_grid *g, const argot_b200_dev_tree *t,
                          uint64_t b0, uint64_t b1, const uint64_t *blk_offsets_dev,
                          uint64_t base, uint32_t *rays_dev, void *stream);
@@ -482,7 +485,9 @@ ARGOT_B200_API void calc_diffuse_photon_radiation(struct fluid_mesh *mesh, struc
 
 /* Reads and clears the device-side error flag of the current device (set
  * when a march exceeded its step bound, which only non-finite input can
- * cause); synchronises `stream`.  Returns 0 or ARGOT_B200_EDEVICE. */
+ * cause, or when a kernel skipped a block whose offsets lie outside
+ * [base, base + nray_group] of its call or do not cover the block's rays);
+ * synchronises `stream`.  Returns 0 or ARGOT_B200_EDEVICE. */
 ARGOT_B200_API int argot_b200_check_device_error(void *stream);
 
 /* frequency grid and cross sections as the reference tabulates them
