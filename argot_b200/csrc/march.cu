@@ -147,11 +147,13 @@ __global__ void __launch_bounds__(256) k_walk(GridDev g, const DevNode *__restri
 // neighbouring cells, so the 32 lanes march nearly parallel paths of nearly
 // equal length and their gathers hit the same cache lines.
 // Launch shape: 256 threads, at least ARGOT_MARCH_MIN_CTAS CTAs resident per
-// SM (which caps the registers per thread).  Measured on B200 (192^3, 1024
-// sources): 6 CTAs (40 registers, a few spills) beat 4 (64 registers) by 12%,
-// the march being bound by the latency of its cache-hit gathers.
+// SM (which caps the registers per thread).  The march is bound by the
+// latency of its cache-hit gathers, so resident warps pay for spills:
+// measured on B200, 6 CTAs (40 registers) beat 4 (64 registers) by 12% on
+// 192^3 / 1024 sources, and 8 CTAs (32 registers, every warp slot of the SM
+// filled) beat 6 by 9% on 256^3 / 4096 sources.
 #ifndef ARGOT_MARCH_MIN_CTAS
-#define ARGOT_MARCH_MIN_CTAS 6
+#define ARGOT_MARCH_MIN_CTAS 8
 #endif
 template <int kPrec>
 __global__ void __launch_bounds__(256, ARGOT_MARCH_MIN_CTAS) k_march_rays(GridDev g, const float4 *__restrict__ cells,

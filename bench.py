@@ -41,13 +41,13 @@ ART_METRIC = "ART diffuse ray-cell steps/s (768 HEALPix directions, 1 B200)"
 ART_UENETOK = 1.0e4
 METRIC = "ray-cell crossings/s (march+stitch+rates, 1 B200)"
 # DRAM bytes per ray-cell crossing of k_march_rays<Kahan> measured by ncu on
-# the 256^3 / 16-source case (1.0045 TB/s over a 128.5 ms launch = 129.1 GB
-# for 6.030e10 crossings); the workloads here are too large to capture, so
-# `traffic` scales this figure.
-MARCH_DRAM_BYTES_PER_CROSSING = 2.141
-# the same capture's L2 bytes (lts__t_bytes.sum, 401.3 GB over the launch's
+# the 256^3 / 16-source case (dram__bytes_read.sum + dram__bytes_write.sum =
+# 148.7 + 21.3 GB over a 118.4 ms launch for 6.030e10 crossings); the
+# workloads here are too large to capture, so `traffic` scales this figure.
+MARCH_DRAM_BYTES_PER_CROSSING = 2.818
+# the same capture's L2 bytes (lts__t_bytes.sum, 701.4 GB over the launch's
 # 6.030e10 crossings): what the L2 serves per crossing
-MARCH_L2_BYTES_PER_CROSSING = 6.654
+MARCH_L2_BYTES_PER_CROSSING = 11.630
 UNIT = "crossings/s"
 
 
@@ -558,7 +558,7 @@ def run_ours(args):
                      "traffic": MARCH_DRAM_BYTES_PER_CROSSING * n_cross,
                      "l2_traffic": MARCH_L2_BYTES_PER_CROSSING * n_cross,
                      "traffic_source": "ncu DRAM bytes per crossing on 256^3 / 16 sources "
-                                       "(2.141 B; L2 6.654 B), scaled by this launch's crossings",
+                                       "(2.818 B; L2 11.630 B), scaled by this launch's crossings",
                      "algorithmic_bytes": alg_bytes,
                      "bytes_model": "16 B per crossing + 36 B per ray"},
         "clocks": clk,
