@@ -243,6 +243,7 @@ def cpu_sample(wl, target_seconds: float = 15.0, max_cells: int = 1 << 20, R=Non
                        f"rates {times[3]:.2f})"),
             "march_crossings_per_s": cross / times[1] if times[1] > 0 else None,
             "gamma_cells_per_s": ncells / times[3] if times[3] > 0 else None,
+            "wall_s": hot,
             "_probe_rays": probe["nray"]}
 
 
@@ -919,17 +920,19 @@ def run_reference(args):
     if isinstance(wl, list):  # a batch: the largest problem stands for it
         wl = max(wl, key=lambda w: (w.edge, w.nsrc))
     R = reference_setup(wl)
-    vals = []
+    vals, walls = [], []
     info = None
     for s in range(args.warmup + args.steps):
         r = cpu_sample(wl, target_seconds=args.ref_seconds, R=R, seed=s)
         if s >= args.warmup:
             vals.append(r["value"])
+            walls.append(r["wall_s"])
             info = r
     v = statistics.median(vals)
     line = {
         "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(walls),
+        "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "impl": "reference",
         "data": "synthetic (seeded lognormal mesh + clustered sources)",
         "config": {"workload": wl.name, "mesh": f"{wl.edge}^3", "sources": wl.nsrc,
@@ -963,8 +966,8 @@ def run_reference_art(args):
     v = steps / t
     print(json.dumps({
         "metric": ART_METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "impl": "reference", "data": "synthetic (seeded lognormal mesh)",
+        "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "impl": "reference", "data": "synthetic (seeded lognormal mesh)",
         "config": {"workload": f"art on {wl.name}", "mesh": f"{wl.edge}^3"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                          "sample": f"whole ART passes, median {t:.1f} s"},
