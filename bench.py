@@ -1008,7 +1008,7 @@ def main(argv=None):
                    help="skip the one-pass comparison of the three rate kernels")
     p.add_argument("--shard", action="store_true",
                    help="N>1: one problem, target slabs sharded over the ranks (strong scaling)")
-    p.add_argument("--overlap", type=int, default=16,
+    p.add_argument("--overlap", type=int, default=32,
                    help="cut the ray group into N parts and overlap the march of one part with the "
                         "rates of the previous one on two streams (0: one stream, kernels in sequence)")
     p.add_argument("--no-e2e", action="store_true")
