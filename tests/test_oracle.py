@@ -145,6 +145,30 @@ def test_restatement_equals_reference_build(oracle, edge, nsrc, seed, theta):
     assert np.array_equal(acc, oracle.accum(len(tau), np.arange(len(tau), dtype=np.uint64), tau))
 
 
+@pytest.mark.parametrize("edge", [19, 24])
+def test_march_restatement_equals_reference_on_other_edges(oracle, edge):
+    """Random segments (starts anywhere in the box, ends at cell centres, and
+    axis-aligned ones along the last row and column) on meshes whose edge is
+    not a power of two: the restated march and the reference's, bit for bit."""
+    from argot_b200 import workload as W
+    R = ref_lib(edge)
+    wl = W.tiny(edge, 3, seed=edge)
+    R.init(wl.lunit, wl.denstonh, 0.5, 1)
+    R.set_mesh(*wl.fields())
+    rng = np.random.default_rng(edge)
+    d = 1.0 / edge
+    rnd = np.concatenate([rng.uniform(0, 1, (4000, 3)), (rng.integers(0, edge, (4000, 3)) + 0.5) * d], axis=1)
+    last = (edge - 1 + 0.5) * d
+    axis = np.array([[0.5 * d, last, last, last, last, last],
+                     [last, 0.5 * d, last, last, last, last],
+                     [last, last, 0.5 * d, last, last, last],
+                     [last, last, last, 0.5 * d, 0.5 * d, 0.5 * d]])
+    segs = np.concatenate([rnd, axis]).astype(np.float32)
+    want, _ = R.march_segments(segs)
+    got = oracle.march_f32ref(unit_box_grid(edge, wl.lunit, wl.denstonh), wl.fields(), segs)
+    assert np.array_equal(got, want)
+
+
 def test_reference_fast_math_spread(oracle):
     """The reference's own -ffast-math build differs from its strict build;
     record that the spread stays at FP32-rounding level."""
