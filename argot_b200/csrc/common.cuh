@@ -95,6 +95,7 @@ struct argot_b200_dev_tree {
   argot::DevNode *nodes;   // n_nodes (preorder)
   int *src_list;           // n_src: source index per leaf slot
   float4 *emit_pos;        // n_emit (x, y, z, 0)
+  float emit_lo[3], emit_hi[3];  // bounding box of the emitter positions
   double *emit_spec64;     // n_emit x 256
   float *emit_specn;       // n_emit x 256: spectrum / total, in bin-pair order (spec_pair_index)
   double *emit_total;      // n_emit

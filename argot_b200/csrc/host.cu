@@ -432,6 +432,16 @@ int argot_b200_dev_tree_upload(const argot_b200_tree *t, argot_b200_dev_tree **o
   std::vector<float> pos4(4 * ne);
   std::vector<double> spec(ne * kNu);
   argot_b200_tree_emitters(t, pos4.data(), spec.data());
+  for (int a = 0; a < 3; a++) {
+    d->emit_lo[a] = ne ? pos4[a] : 0.f;
+    d->emit_hi[a] = ne ? pos4[a] : 0.f;
+  }
+  for (size_t e = 0; e < ne; e++) {
+    for (int a = 0; a < 3; a++) {
+      d->emit_lo[a] = std::min(d->emit_lo[a], pos4[4 * e + a]);
+      d->emit_hi[a] = std::max(d->emit_hi[a], pos4[4 * e + a]);
+    }
+  }
   std::vector<float> specn(ne * kNu);
   std::vector<double> total(ne);
   for (size_t e = 0; e < ne; e++) {

@@ -148,55 +148,86 @@ __global__ void __launch_bounds__(256) k_walk(GridDev g, const DevNode *__restri
 // equal length and their gathers hit the same cache lines.
 // Launch shape: 256 threads, at least ARGOT_MARCH_MIN_CTAS CTAs resident per
 // SM (which caps the registers per thread).  The march is bound by the
-// latency of its cache-hit gathers, so resident warps pay for spills:
-// measured on B200, 6 CTAs (40 registers) beat 4 (64 registers) by 12% on
-// 192^3 / 1024 sources, and 8 CTAs (32 registers, every warp slot of the SM
-// filled) beat 6 by 9% on 256^3 / 4096 sources.
+// latency of its cache-hit gathers, so resident warps matter more than
+// registers: measured on B200 at 256^3 / 4096 sources with the fixed-point
+// walk, 8 CTAs (32 registers) 1.15 s, 7 CTAs 1.15 s, 6 CTAs (40 registers)
+// 1.21 s.  What lives across a ray's walk is kept out of registers: the
+// Kahan columns in per-thread shared-memory slots, the block's state (block
+// index, ray count, packed coordinates, first ray; the same for the warp's
+// lanes) in per-warp shared memory, read back after each ray.  That took the
+// 8-CTA launch from 1.76 s (spilling) to 1.15 s.  kInside: every emitter
+// lies inside the box (the host checks the emitters' bounding box), so rays
+// start at their emitter and the launch contains no call.
 #ifndef ARGOT_MARCH_MIN_CTAS
 #define ARGOT_MARCH_MIN_CTAS 8
 #endif
-template <int kPrec>
-__global__ void __launch_bounds__(256, ARGOT_MARCH_MIN_CTAS) k_march_rays(GridDev g, const float4 *__restrict__ cells,
-                                                    const float4 *__restrict__ emit_pos, uint64_t b0,
-                                                    uint64_t b1, const uint64_t *__restrict__ blk_off,
+constexpr int kMarchThreads = 256;
+template <int kPrec, bool kInside>
+__global__ void __launch_bounds__(kMarchThreads, ARGOT_MARCH_MIN_CTAS) k_march_rays(GridDev g, const float4 *__restrict__ cells,
+                                                    const float4 *__restrict__ emit_pos, uint32_t b0,
+                                                    uint32_t b1, const uint64_t *__restrict__ blk_off,
                                                     uint64_t base, const uint32_t *__restrict__ rays,
                                                     uint64_t nray, float *__restrict__ tau,
                                                     unsigned long long *__restrict__ crossings,
                                                     int *__restrict__ err) {
   const int lane = threadIdx.x & 31;
-  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned long long steps_total = 0;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarp = (gridDim.x * blockDim.x) >> 5;
+  __shared__ float kslot[6 * kMarchThreads];  // the Kahan columns, one slot per thread
+  // the block's state, the same for the warp's lanes: it is read back from
+  // shared memory after each ray instead of staying live in registers
+  // across the walk (block index, ray count, packed coordinates, first ray)
+  __shared__ uint32_t wstate[kMarchThreads / 32][5];
+  volatile uint32_t *ws = wstate[threadIdx.x >> 5];
   bool bad = false;
-  for (uint64_t b = b0 + warp; b < b1; b += nwarp) {
+  for (uint32_t b = b0 + warp; b < b1; b += nwarp) {
     uint64_t r0, r1;
     if (!block_rays(blk_off, b, base, nray, &r0, &r1)) { bad = true; continue; }
-    int bix, biy, biz;
-    block_cell(g, b, 0, &bix, &biy, &biz);
-    for (uint64_t r = r0 + lane; r < r1; r += 32) {
+    // the block's coordinates in blocks (the host checks nbx < 4096 and
+    // nby, nbz < 1024)
+    const uint32_t nyz = (uint32_t)g.nby * (uint32_t)g.nbz;
+    const uint32_t bx = b / nyz, by = (b - bx * nyz) / (uint32_t)g.nbz, bz = b - bx * nyz - by * (uint32_t)g.nbz;
+    __syncwarp();
+    if (lane == 0) {
+      ws[0] = b;
+      ws[1] = (uint32_t)(r1 - r0);
+      ws[2] = bx | (by << 12) | (bz << 22);
+      ws[3] = (uint32_t)r0;
+      ws[4] = (uint32_t)(r0 >> 32);
+    }
+    __syncwarp();
+    uint32_t bsteps = 0;
+    for (uint32_t j = lane; j < ws[1]; j += 32) {
+      const uint64_t r = (((uint64_t)ws[4] << 32) | ws[3]) + j;
+      const uint32_t bpos = ws[2];
       const uint32_t w = __ldg(rays + r);
       const uint32_t e = w >> 5;
       const int l = (int)(w & 31u);
-      const int gx = g.ix0 + bix + (l >> 4), gy = g.iy0 + biy + ((l >> 2) & 3), gz = g.iz0 + biz + (l & 3);
+      const int gx = g.ix0 + kBlkX * (int)(bpos & 4095u) + (l >> 4);
+      const int gy = g.iy0 + kBlkY * (int)((bpos >> 12) & 1023u) + ((l >> 2) & 3);
+      const int gz = g.iz0 + kBlkZ * (int)(bpos >> 22) + (l & 3);
       const float xe = cell_centre(g.xmin, gx, g.dx);
       const float ye = cell_centre(g.ymin, gy, g.dy);
       const float ze = cell_centre(g.zmin, gz, g.dz);
       const float4 ep = __ldg(emit_pos + e);
-      float xs, ys, zs;
-      ray_start(g, ep.x, ep.y, ep.z, xe, ye, ze, &xs, &ys, &zs);
+      float xs = ep.x, ys = ep.y, zs = ep.z;
+      if (!kInside) ray_start(g, ep.x, ep.y, ep.z, xe, ye, ze, &xs, &ys, &zs);
       int steps = 0;
       const Tau3 t = (kPrec == ARGOT_B200_PRECISION_REFERENCE)
                          ? march_reference(g, cells, xs, ys, zs, xe, ye, ze, &steps, &bad)
-                         : march_kahan(g, cells, xs, ys, zs, xe, ye, ze, &steps, &bad);
-      tau[r] = t.hi;
-      tau[nray + r] = t.hei;
-      tau[2 * nray + r] = t.heii;
-      steps_total += (unsigned long long)steps;
+                         : march_kahan<kMarchThreads>(g, cells, xs, ys, zs, xe, ye, ze, &steps, &bad,
+                                                      kslot + threadIdx.x);
+      const uint64_t ro = (((uint64_t)ws[4] << 32) | ws[3]) + j;
+      tau[ro] = t.hi;
+      tau[nray + ro] = t.hei;
+      tau[2 * nray + ro] = t.heii;
+      bsteps += (uint32_t)steps;
     }
-  }
-  if (crossings) {
-    for (int o = 16; o; o >>= 1) steps_total += __shfl_xor_sync(0xffffffffu, steps_total, o);
-    if (lane == 0 && steps_total) atomicAdd(crossings, steps_total);
+    if (crossings) {
+      for (int o = 16; o; o >>= 1) bsteps += __shfl_xor_sync(0xffffffffu, bsteps, o);
+      if (lane == 0 && bsteps) atomicAdd(crossings, (unsigned long long)bsteps);
+    }
+    b = ws[0];
   }
   if (bad) atomicExch(err, 1);
 }
@@ -451,20 +482,32 @@ int argot_b200_march_rays(const argot_b200_grid *gp, const void *packed, const a
     return ARGOT_B200_EINVAL;
   }
   if (b0 == b1) { set_status(0); return 0; }
+  GridDev g = make_grid(*gp);
+  if (g.nbx >= 4096 || g.nby >= 1024 || g.nbz >= 1024) {  // the kernel packs block coordinates in 32 bits
+    set_status(ARGOT_B200_ENOTSUP);
+    return ARGOT_B200_ENOTSUP;
+  }
   int dev = 0;
   ARGOT_CUDA_TRY(cudaGetDevice(&dev));
   int *err = err_flag(dev);
   if (!err) { set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
-  GridDev g = make_grid(*gp);
   cudaStream_t st = (cudaStream_t)stream;
   const int threads = 256;
   const int blocks = grid_blocks_for((b1 - b0) * 32, threads);
-  if (prec == ARGOT_B200_PRECISION_REFERENCE)
-    k_march_rays<ARGOT_B200_PRECISION_REFERENCE><<<blocks, threads, 0, st>>>(
-        g, (const float4 *)packed, t->emit_pos, b0, b1, blk_off, base, rays, nray, tau, crossings, err);
-  else
-    k_march_rays<ARGOT_B200_PRECISION_KAHAN><<<blocks, threads, 0, st>>>(
-        g, (const float4 *)packed, t->emit_pos, b0, b1, blk_off, base, rays, nray, tau, crossings, err);
+  const bool inside = t->emit_lo[0] >= gp->xmin && t->emit_lo[1] >= gp->ymin && t->emit_lo[2] >= gp->zmin &&
+                      t->emit_hi[0] <= gp->xmax && t->emit_hi[1] <= gp->ymax && t->emit_hi[2] <= gp->zmax;
+  const float4 *cells = (const float4 *)packed;
+#define ARGOT_MARCH_LAUNCH(P, I)                                                                       \
+  k_march_rays<P, I><<<blocks, threads, 0, st>>>(g, cells, t->emit_pos, (uint32_t)b0, (uint32_t)b1, blk_off, \
+                                                 base, rays, nray, tau, crossings, err)
+  if (prec == ARGOT_B200_PRECISION_REFERENCE) {
+    if (inside) ARGOT_MARCH_LAUNCH(ARGOT_B200_PRECISION_REFERENCE, true);
+    else ARGOT_MARCH_LAUNCH(ARGOT_B200_PRECISION_REFERENCE, false);
+  } else {
+    if (inside) ARGOT_MARCH_LAUNCH(ARGOT_B200_PRECISION_KAHAN, true);
+    else ARGOT_MARCH_LAUNCH(ARGOT_B200_PRECISION_KAHAN, false);
+  }
+#undef ARGOT_MARCH_LAUNCH
   ARGOT_CUDA_TRY(cudaGetLastError());
   set_status(0);
   return 0;

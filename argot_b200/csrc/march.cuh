@@ -101,19 +101,7 @@ static __device__ __noinline__ Tau3 march_reference(const GridDev &g, const floa
   return t;
 }
 
-// ---------------------------------------------------------------------------
-// Count-down march with compensated sums.  Same start / end cell rules as
-// the reference.  Along each axis the walk must cross exactly
-// |i_end - i_start| faces, so it keeps per axis the number of faces still
-// to cross and the distance along the ray to the next one.  Every step
-// takes the nearest face among the axes that still have faces to cross,
-// resets that axis's distance to the face spacing dX/|u_x| and shortens the
-// others by the step.  Distances therefore stay of cell size, and their
-// rounding scales with the cell rather than with the ray length as a running
-// position or an absolute path parameter would; the walk always ends in the
-// end cell after at most sum|di| steps.  The last chord is measured from
-// the face through which the end cell was entered.  Columns are FP32 with
-// compensated (Kahan) summation.
+// Compensated (Kahan) summation step: s + c carries the running sum.
 __device__ __forceinline__ void kahan_add(float &s, float &c, float v) {
   const float y = v - c;
   const float tt = s + y;
@@ -121,93 +109,158 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float v) {
   s = tt;
 }
 
-// The walk.  Per step: the nearest face among the axes with faces left;
-// the chord belongs to the current cell; the crossed axes advance the
-// 32-bit cell index by their precomputed strides and reset their distance
-// to the face spacing, the others shorten theirs.  The gather of the next
-// cell is issued before the current one is accumulated.  Chords are summed
-// with FMA into per-species partial sums that are folded into Kahan sums
-// every 16 steps (compensated summation over blocks of 16 terms).  The last
-// chord runs from the end cell's entry face to the end point.
+// ---------------------------------------------------------------------------
+// Count-down march with compensated sums.  Same start / end cell rules as
+// the reference.  Along each axis the walk must cross exactly
+// |i_end - i_start| faces.  Per axis it keeps the number of faces still to
+// cross and the path length from the start point to the next one; every
+// step takes the nearest face among the axes that still have faces to
+// cross, the chord from the previous crossing to it belongs to the current
+// cell, and the crossed axes advance to their following face by the face
+// spacing dX/|u_x|.  The walk always ends in the end cell after at most
+// sum|di| steps.  Columns are FP32 with compensated (Kahan) summation.
+//
+// Path lengths are unsigned fixed-point integers.  Every chord is a
+// difference of two path lengths to faces, and the face spacing of a
+// slanted axis is a multi-cell distance: FP32 countdowns round both (1e-7
+// of them per step and per reset), which drifts along the ray and, measured
+// on a 32^3 lognormal mesh, put 2e-5 relative error into minor-species
+// columns that one short chord dominates.  Integer differences are exact.
+// The unit is 2^-k of the largest cell side, with k per ray the largest
+// that keeps the ray length below 2^31 units (2^-22 of a cell for rays of
+// up to 256 cells); a face position is held as 32.32 bits, so the spacing
+// is added with a 64-bit carry and its rounding (2^-32 unit per face) never
+// accumulates to a unit.  The chord, an integer number of units below 2^31,
+// converts to FP32 with one rounding and the column sums are scaled back by
+// the unit at the end.  The per-ray set-up (cosines, spacings, first
+// faces) is formed once per ray in FP64: its inputs are differences of
+// box-scale coordinates.  Columns agree with an FP64 march to ~3e-7.
+//
+// The walk's geometry does not depend on the densities, so the compiler
+// issues a step's gather ahead of the previous steps' sums (an explicit
+// one-step-ahead gather held four more registers and measured no faster).
+// Chords are summed with FMA into per-species partial sums that are folded
+// into the Kahan sums every 16 steps (compensated summation over blocks of
+// 16 terms).  The last chord runs from the latest face crossing to the end
+// point.  kSlotStride > 0: the Kahan sums live in per-thread shared-memory
+// slots (`slot`, words kSlotStride apart), touched once per 16 steps, which
+// frees six registers for the walk.
+// Kahan step on a column kept in per-thread shared-memory slots: sum in
+// word q, compensation in word q + 3 (words kStride apart).
+template <int kStride>
+__device__ __forceinline__ void kahan_slot(float *slot, int q, float v) {
+  float s = slot[q * kStride], c = slot[(q + 3) * kStride];
+  kahan_add(s, c, v);
+  slot[q * kStride] = s;
+  slot[(q + 3) * kStride] = c;
+}
+
+__device__ __forceinline__ uint64_t fixed_32_32(double units) {
+  return (uint64_t)__double2ull_rz(units * 4294967296.0);
+}
+
+template <int kSlotStride = 0>
 static __device__ __forceinline__ Tau3 march_kahan(const GridDev &g, const float4 *__restrict__ cells,
                                                    float xs, float ys, float zs, float xe, float ye,
-                                                   float ze, int *steps, bool *bad) {
+                                                   float ze, int *steps, bool *bad, float *slot = nullptr) {
   const int ixe = axis_cell(xe, g.xminl, g.dx, g.nx);
   const int iye = axis_cell(ye, g.yminl, g.dy, g.ny);
   const int ize = axis_cell(ze, g.zminl, g.dz, g.nz);
   const int ix = axis_cell(xs, g.xminl, g.dx, g.nx);
   const int iy = axis_cell(ys, g.yminl, g.dy, g.ny);
   const int iz = axis_cell(zs, g.zminl, g.dz, g.nz);
-  const float x0 = xs - g.xminl, y0 = ys - g.yminl, z0 = zs - g.zminl;
-  const float dx = xe - xs, dy = ye - ys, dz = ze - zs;
-  const float len = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-  const float il = len > 0.f ? 1.0f / len : 0.f;
-  const float ax = fabsf(cosine_guard(dx * il)), ay = fabsf(cosine_guard(dy * il)),
-              az = fabsf(cosine_guard(dz * il));
-  const float iax = 1.0f / ax, iay = 1.0f / ay, iaz = 1.0f / az;
+  // differences of floats are exact in double
+  const double x0 = (double)xs - (double)g.xminl, y0 = (double)ys - (double)g.yminl,
+               z0 = (double)zs - (double)g.zminl;
+  const double dx = (double)xe - (double)xs, dy = (double)ye - (double)ys, dz = (double)ze - (double)zs;
+  const double len = sqrt(fma(dx, dx, fma(dy, dy, dz * dz)));
+  if (!(len <= 1.0e30)) *bad = true;  // non-finite end points
+  // 1/|cosine| per axis, with the reference's floor of 1e-31 on |cosine|
+  const double iax = len / fmax(fabs(dx), kTiny * len), iay = len / fmax(fabs(dy), kTiny * len),
+               iaz = len / fmax(fabs(dz), kTiny * len);
   int cx = abs(ixe - ix), cy = abs(iye - iy), cz = abs(ize - iz);
   const int stx = ixe > ix ? 1 : -1, sty = iye > iy ? 1 : -1, stz = ize > iz ? 1 : -1;
-  const float kInf = __int_as_float(0x7f800000);
-  float rx = cx ? fmaxf(fabsf(fmaf(g.dx, (float)(ix + (stx > 0)), -x0)) * iax, 0.f) : kInf;
-  float ry = cy ? fmaxf(fabsf(fmaf(g.dy, (float)(iy + (sty > 0)), -y0)) * iay, 0.f) : kInf;
-  float rz = cz ? fmaxf(fabsf(fmaf(g.dz, (float)(iz + (stz > 0)), -z0)) * iaz, 0.f) : kInf;
-  const float tdx = g.dx * iax, tdy = g.dy * iay, tdz = g.dz * iaz;
+  // the unit: 2^-k of the largest cell side, the ray length below 2^31 units
+  const double dmax = fmax((double)g.dx, fmax((double)g.dy, (double)g.dz));
+  const int k = min(40, 30 - ilogb(len / dmax + 2.0));
+  const double sc = ldexp(1.0, k) / dmax;  // box lengths -> units
+  // path lengths of the first face of each axis and the face spacings,
+  // 32.32 fixed point; an axis without faces to cross never comes next
+  const uint64_t kNone = ~0ull;
+  uint64_t tx = cx ? fixed_32_32(fabs(fma((double)g.dx, (double)(ix + (stx > 0)), -x0)) * iax * sc) : kNone;
+  uint64_t ty = cy ? fixed_32_32(fabs(fma((double)g.dy, (double)(iy + (sty > 0)), -y0)) * iay * sc) : kNone;
+  uint64_t tz = cz ? fixed_32_32(fabs(fma((double)g.dz, (double)(iz + (stz > 0)), -z0)) * iaz * sc) : kNone;
+  // a spacing is used only while its axis has faces left, then it is
+  // shorter than the ray (below 2^31 units)
+  const uint64_t Tx = fixed_32_32(fmin((double)g.dx * iax * sc, 2147483648.0));
+  const uint64_t Ty = fixed_32_32(fmin((double)g.dy * iay * sc, 2147483648.0));
+  const uint64_t Tz = fixed_32_32(fmin((double)g.dz * iaz * sc, 2147483648.0));
+  const uint32_t lu = (uint32_t)__double2uint_rn(fmin(len * sc, 2147483648.0));
   const int dsz = stz, dsy = sty * g.nz, dsx = stx * g.nz * g.ny;
   int idx = iz + g.nz * (iy + g.ny * ix);
 
-  float4 n = __ldg(cells + idx);
   float p0 = 0.f, p1 = 0.f, p2 = 0.f;
   float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
-  const int cap = cx + cy + cz;  // every finite step crosses at least one face
-  const bool crx = cx != 0, cry = cy != 0, crz = cz != 0;  // axes with faces to cross
-  int it = 0;
-  // blocks of 16 steps (unrolled; the Kahan fold and the step bound are
-  // checked once per block, so only "faces left" is tested per step)
-  while ((cx | cy | cz) && it < cap) {
-    int k = 0;
+  if (kSlotStride) {
 #pragma unroll
-    for (; k < 16; k++) {
+    for (int q = 0; q < 6; q++) slot[q * kSlotStride] = 0.f;
+  }
+  uint32_t t = 0;  // path length of the latest crossing (units)
+  int it = 0;
+  // blocks of 16 steps (unrolled; the Kahan fold once per block, so only
+  // "faces left" is tested per step).  Every step crosses the face of at
+  // least one axis with faces left, so the walk ends.
+  while (cx | cy | cz) {
+    int kk = 0;
+#pragma unroll
+    for (; kk < 16; kk++) {
       if (!(cx | cy | cz)) break;
-      const float r = fminf(rx, fminf(ry, rz));
-      const bool hx = rx == r, hy = ry == r, hz = rz == r;
+      const uint32_t xh = (uint32_t)(tx >> 32), yh = (uint32_t)(ty >> 32), zh = (uint32_t)(tz >> 32);
+      const uint32_t m = min(xh, min(yh, zh));
+      const bool hx = xh == m, hy = yh == m, hz = zh == m;
+      const float4 n = __ldg(cells + idx);
       idx += (hx ? dsx : 0) + (hy ? dsy : 0) + (hz ? dsz : 0);
-      const float4 nn = __ldg(cells + idx);
-      p0 = fmaf(r, n.x, p0);
-      p1 = fmaf(r, n.y, p1);
-      p2 = fmaf(r, n.z, p2);
+      const float rf = __uint2float_rn(m - t);
+      t = m;
+      p0 = fmaf(rf, n.x, p0);
+      p1 = fmaf(rf, n.y, p1);
+      p2 = fmaf(rf, n.z, p2);
       cx -= hx; cy -= hy; cz -= hz;
-      rx = hx ? (cx ? tdx : kInf) : rx - r;
-      ry = hy ? (cy ? tdy : kInf) : ry - r;
-      rz = hz ? (cz ? tdz : kInf) : rz - r;
-      n = nn;
+      if (hx) tx = cx ? tx + Tx : kNone;
+      if (hy) ty = cy ? ty + Ty : kNone;
+      if (hz) tz = cz ? tz + Tz : kNone;
     }
-    it += k;
-    if (k == 16) {
-      kahan_add(s0, c0, p0);
-      kahan_add(s1, c1, p1);
-      kahan_add(s2, c2, p2);
+    it += kk;
+    if (kk == 16) {
+      if (kSlotStride) {
+        kahan_slot<kSlotStride>(slot, 0, p0);
+        kahan_slot<kSlotStride>(slot, 1, p1);
+        kahan_slot<kSlotStride>(slot, 2, p2);
+      } else {
+        kahan_add(s0, c0, p0);
+        kahan_add(s1, c1, p1);
+        kahan_add(s2, c2, p2);
+      }
       p0 = p1 = p2 = 0.f;
     }
   }
-  if (cx | cy | cz) *bad = true;  // only non-finite input leaves faces uncrossed
-  // the ray enters the end cell at its latest face crossing, so the last
-  // chord is the shortest distance from an axis's entry face of the end
-  // cell to the end point, over the axes that had faces to cross
-  float depth = len;
-  if (crx | cry | crz) {
-    depth = kInf;
-    if (crx) depth = fminf(depth, fabsf((xe - g.xminl) - g.dx * (float)(ixe + (stx < 0))) * iax);
-    if (cry) depth = fminf(depth, fabsf((ye - g.yminl) - g.dy * (float)(iye + (sty < 0))) * iay);
-    if (crz) depth = fminf(depth, fabsf((ze - g.zminl) - g.dz * (float)(ize + (stz < 0))) * iaz);
+  // the last chord: from the latest crossing to the end point
+  const float df = __int2float_rn(max((int)(lu - t), 0));
+  const float4 n = __ldg(cells + idx);
+  p0 = fmaf(df, n.x, p0);
+  p1 = fmaf(df, n.y, p1);
+  p2 = fmaf(df, n.z, p2);
+  if (kSlotStride) {
+    s0 = slot[0]; c0 = slot[3 * kSlotStride];
+    s1 = slot[kSlotStride]; c1 = slot[4 * kSlotStride];
+    s2 = slot[2 * kSlotStride]; c2 = slot[5 * kSlotStride];
   }
-  p0 = fmaf(depth, n.x, p0);
-  p1 = fmaf(depth, n.y, p1);
-  p2 = fmaf(depth, n.z, p2);
   kahan_add(s0, c0, p0);
   kahan_add(s1, c1, p1);
   kahan_add(s2, c2, p2);
+  const float unit = (float)(dmax * ldexp(1.0, -k));  // exact: dmax is a float
   *steps = it + 1;
-  return Tau3{s0, s1, s2};
+  return Tau3{s0 * unit, s1 * unit, s2 * unit};
 }
 
 // ---------------------------------------------------------------------------
@@ -220,22 +273,12 @@ __device__ __forceinline__ float cell_centre(float lo, int i, float d) {
   return __double2float_rn(__dadd_rn((double)lo, __dmul_rn(__dadd_rn((double)__int2float_rn(i), 0.5), (double)d)));
 }
 
-static __device__ __noinline__ void ray_start_outside(const GridDev &g, float sx, float sy, float sz,
-                                                      float xt, float yt, float zt, float *ox, float *oy,
-                                                      float *oz);
-
-__device__ __forceinline__ void ray_start(const GridDev &g, float sx, float sy, float sz, float xt,
-                                          float yt, float zt, float *ox, float *oy, float *oz) {
-  *ox = sx; *oy = sy; *oz = sz;
-  if (sx >= g.xmin && sx <= g.xmax && sy >= g.ymin && sy <= g.ymax && sz >= g.zmin && sz <= g.zmax)
-    return;
-  ray_start_outside(g, sx, sy, sz, xt, yt, zt, ox, oy, oz);
-}
-
-// emitters outside the box (rare: only sources placed outside it)
-static __device__ __noinline__ void ray_start_outside(const GridDev &g, float sx, float sy, float sz,
-                                                      float xt, float yt, float zt, float *ox, float *oy,
-                                                      float *oz) {
+// Emitters outside the box (rare: only sources placed outside it).  The box
+// bounds come by value and the point returns in registers, so that the
+// call does not make its callers keep the grid or the end points in memory.
+static __device__ __noinline__ float3 ray_start_outside(float xmin, float ymin, float zmin, float xmax,
+                                                        float ymax, float zmax, float sx, float sy,
+                                                        float sz, float xt, float yt, float zt) {
   const double tiny = 1.0e-30;
   const float dx = __fsub_rn(xt, sx), dy = __fsub_rn(yt, sy), dz = __fsub_rn(zt, sz);
   const float s3 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
@@ -251,17 +294,24 @@ static __device__ __noinline__ void ray_start_outside(const GridDev &g, float sx
   if (fabs((double)yo) < tiny) yo = (yo >= 0.f) ? (float)tiny : -(float)tiny;
   if (fabs((double)zo) < tiny) zo = (zo >= 0.f) ? (float)tiny : -(float)tiny;
   float out = 0.f;
-  if (sx < g.xmin) out = __fdiv_rn(__fsub_rn(g.xmin, sx), xo);
-  if (sx > g.xmax) out = __fdiv_rn(__fsub_rn(g.xmax, sx), xo);
-  if (sy < g.ymin) out = __fdiv_rn(__fsub_rn(g.ymin, sy), yo);
-  if (sy > g.ymax) out = __fdiv_rn(__fsub_rn(g.ymax, sy), yo);
-  if (sz < g.zmin) out = __fdiv_rn(__fsub_rn(g.zmin, sz), zo);
-  if (sz > g.zmax) out = __fdiv_rn(__fsub_rn(g.zmax, sz), zo);
-  if (out != 0.f) {
-    *ox = __fadd_rn(sx, __fmul_rn(out, xo));
-    *oy = __fadd_rn(sy, __fmul_rn(out, yo));
-    *oz = __fadd_rn(sz, __fmul_rn(out, zo));
-  }
+  if (sx < xmin) out = __fdiv_rn(__fsub_rn(xmin, sx), xo);
+  if (sx > xmax) out = __fdiv_rn(__fsub_rn(xmax, sx), xo);
+  if (sy < ymin) out = __fdiv_rn(__fsub_rn(ymin, sy), yo);
+  if (sy > ymax) out = __fdiv_rn(__fsub_rn(ymax, sy), yo);
+  if (sz < zmin) out = __fdiv_rn(__fsub_rn(zmin, sz), zo);
+  if (sz > zmax) out = __fdiv_rn(__fsub_rn(zmax, sz), zo);
+  if (out == 0.f) return make_float3(sx, sy, sz);
+  return make_float3(__fadd_rn(sx, __fmul_rn(out, xo)), __fadd_rn(sy, __fmul_rn(out, yo)),
+                     __fadd_rn(sz, __fmul_rn(out, zo)));
+}
+
+__device__ __forceinline__ void ray_start(const GridDev &g, float sx, float sy, float sz, float xt,
+                                          float yt, float zt, float *ox, float *oy, float *oz) {
+  *ox = sx; *oy = sy; *oz = sz;
+  if (sx >= g.xmin && sx <= g.xmax && sy >= g.ymin && sy <= g.ymax && sz >= g.zmin && sz <= g.zmax)
+    return;
+  const float3 o = ray_start_outside(g.xmin, g.ymin, g.zmin, g.xmax, g.ymax, g.zmax, sx, sy, sz, xt, yt, zt);
+  *ox = o.x; *oy = o.y; *oz = o.z;
 }
 
 // Target cell of lane `lane` in block b (local indices); false if the lane's
