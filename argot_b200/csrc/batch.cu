@@ -68,9 +68,9 @@ __global__ void __launch_bounds__(32 * kWarps, ARGOT_BATCH_MIN_WARPS / kWarps)
             uint32_t *__restrict__ next, unsigned long long *__restrict__ crossings, int *__restrict__ err) {
   __shared__ BinPair s_pairs[kBinPairs];
   __shared__ float s_nd[kWarps][32][6];
-  __shared__ double s_p[kWarps][32][3];
-  __shared__ double s_out[kWarps][32][6];
-  __shared__ int s_e[kWarps][32], s_t[kWarps][32];
+  __shared__ float s_p[kWarps][32][3];
+  __shared__ float s_out[kWarps][32][6];
+  __shared__ int s_e[kWarps][32], s_t[kWarps][32], s_cnt[kWarps][32], s_src[kWarps][32];
   load_bin_pairs(s_pairs);
   __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -98,7 +98,8 @@ __global__ void __launch_bounds__(32 * kWarps, ARGOT_BATCH_MIN_WARPS / kWarps)
       int ix, iy, iz;
       const bool own_valid = block_cell(g, b, lane, &ix, &iy, &iz);
       const uint64_t own = own_valid ? cell_index(g, ix, iy, iz) : 0;
-      double acc[6] = {0, 0, 0, 0, 0, 0};
+      CellSum6 acc;
+      acc.zero();
       int bix, biy, biz;
       block_cell(g, b, 0, &bix, &biy, &biz);
       const uint64_t r0 = P.blk_off[b], r1 = P.blk_off[b + 1];
@@ -121,10 +122,9 @@ __global__ void __launch_bounds__(32 * kWarps, ARGOT_BATCH_MIN_WARPS / kWarps)
           const Tau3 tt = march_kahan(g, cells, xs, ys, zs, xe, ye, ze, &steps, &bad);
           steps_total += (unsigned long long)steps;
           // the rate parameters (as argot_b200_photoion_rays)
-          const RayGeom geo = ray_geometry(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z);
           const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
-          const RayCols cols = ray_columns(g, tt.hi, tt.hei, tt.heii, rw, geo);
-          const RayParams p = ray_params(cols, __ldg(total + e));
+          const RayParams p = ray_params_f32(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z, tt.hi, tt.hei,
+                                             tt.heii, rw, __ldg(total + e));
 #pragma unroll
           for (int s = 0; s < 3; s++) {
             s_nd[wib][lane][s] = p.N[s];
@@ -142,38 +142,25 @@ __global__ void __launch_bounds__(32 * kWarps, ARGOT_BATCH_MIN_WARPS / kWarps)
           const float *sp = specn + (size_t)s_e[wib][q] * kNu;
           float part[6];
           ray_bins_packed(s_pairs, sp, j, N0, N1, N2, D0, D1, D2, part);
-          float g0 = part[0], g1 = part[1], g2 = part[2], h0 = part[3], h1 = part[4], h2 = part[5];
 #pragma unroll
           for (int o = 1; o < 8; o <<= 1) {
-            g0 += __shfl_xor_sync(gmask, g0, o);
-            g1 += __shfl_xor_sync(gmask, g1, o);
-            g2 += __shfl_xor_sync(gmask, g2, o);
-            h0 += __shfl_xor_sync(gmask, h0, o);
-            h1 += __shfl_xor_sync(gmask, h1, o);
-            h2 += __shfl_xor_sync(gmask, h2, o);
+#pragma unroll
+            for (int s = 0; s < 6; s++) part[s] += __shfl_xor_sync(gmask, part[s], o);
           }
           if (j == 0) {
-            const double p0 = s_p[wib][q][0], p1 = s_p[wib][q][1], p2 = s_p[wib][q][2];
-            s_out[wib][q][0] = p0 * g0;
-            s_out[wib][q][1] = p1 * g1;
-            s_out[wib][q][2] = p2 * g2;
-            s_out[wib][q][3] = p0 * h0 * kHNuL;
-            s_out[wib][q][4] = p1 * h1 * kHNuL;
-            s_out[wib][q][5] = p2 * h2 * kHNuL;
-          }
-        }
-        __syncwarp();
-        for (int k = 0; k < nk; k++) {
-          if (s_t[wib][k] == lane) {
+            const float Pq[3] = {s_p[wib][q][0], s_p[wib][q][1], s_p[wib][q][2]};
+            float out[6];
+            ray_rates6(Pq, part[0], part[1], part[2], part[3], part[4], part[5], out);
 #pragma unroll
-            for (int s = 0; s < 6; s++) acc[s] += s_out[wib][k][s];
+            for (int s = 0; s < 6; s++) s_out[wib][q][s] = out[s];
           }
         }
         __syncwarp();
+        add_chunk_in_order(acc, lane, t, s_out[wib], s_cnt[wib], s_src[wib]);
       }
       if (own_valid) {
 #pragma unroll
-        for (int s = 0; s < 6; s++) rates6[s * ncell + own] = (float)acc[s];
+        for (int s = 0; s < 6; s++) rates6[s * ncell + own] = acc.s[s];
       }
     }
   }

@@ -40,6 +40,11 @@ struct GridDev {
   float dx, dy, dz;
   double lunit, denstonh;
   int nbx, nby, nbz;  // blocks per axis
+  // FP32 forms of the unit conversions of the FP32 rate path: lunit *
+  // denstonh (code column -> cm^-2), and 1 / (4 pi lunit^2) = pcm * 2^pce
+  // (below the FP32 range, so its power of two is kept apart)
+  float cdf, pcm;
+  int pce;
 };
 
 GridDev make_grid(const argot_b200_grid &g);

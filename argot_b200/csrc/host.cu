@@ -37,6 +37,11 @@ GridDev make_grid(const argot_b200_grid &g) {
   d.nbx = (g.nx + kBlkX - 1) / kBlkX;
   d.nby = (g.ny + kBlkY - 1) / kBlkY;
   d.nbz = (g.nz + kBlkZ - 1) / kBlkZ;
+  d.cdf = (float)(g.lunit * g.denstonh);
+  int e = 0;
+  const double m = std::frexp(1.0 / (4.0 * kPi * g.lunit * g.lunit), &e);  // m in [0.5, 1)
+  d.pcm = (float)(2.0 * m);
+  d.pce = e - 1;
   return d;
 }
 

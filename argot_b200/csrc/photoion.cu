@@ -16,14 +16,12 @@ constexpr int kRateWarps = 4;  // warps per CTA in the block-rate kernel
 // One warp per target block.  Lanes compute the rates of 32 rays at a time
 // into shared memory; then lane j, which owns cell j of the block, adds the
 // contributions of the rays that end in its cell in ray order.  No atomics:
-// the result does not depend on scheduling.  EXACT_F64 adds to the existing
-// float value with the reference's float += double rounding per ray
-// (calc_photoion_rate.c:403-425); the other modes sum in double and store.
-template <int kMode>
+// the result does not depend on scheduling.  Each ray's rates are added to
+// the existing float value with the reference's float += double rounding
+// (calc_photoion_rate.c:403-425).
 __global__ void __launch_bounds__(32 * kRateWarps)
     k_rate_blocks(GridDev g, const float4 *__restrict__ raw, const float4 *__restrict__ emit_pos,
-                  const double *__restrict__ spec64, const float *__restrict__ specn,
-                  const double *__restrict__ total, uint64_t b0, uint64_t b1,
+                  const double *__restrict__ spec64, uint64_t b0, uint64_t b1,
                   const uint64_t *__restrict__ blk_off, uint64_t base, const uint32_t *__restrict__ rays,
                   uint64_t nray, const float *__restrict__ tau, float *__restrict__ rates6,
                   int *__restrict__ err) {
@@ -38,12 +36,8 @@ __global__ void __launch_bounds__(32 * kRateWarps)
     const bool own_valid = block_cell(g, b, lane, &ix, &iy, &iz);
     const uint64_t own = own_valid ? cell_index(g, ix, iy, iz) : 0;
     float accf[6];
-    double accd[6];
 #pragma unroll
-    for (int s = 0; s < 6; s++) {
-      accf[s] = (kMode == ARGOT_B200_RATE_EXACT_F64 && own_valid) ? rates6[s * ncell + own] : 0.f;
-      accd[s] = 0.0;
-    }
+    for (int s = 0; s < 6; s++) accf[s] = own_valid ? rates6[s * ncell + own] : 0.f;
     int bix, biy, biz;
     block_cell(g, b, 0, &bix, &biy, &biz);
     uint64_t r0, r1;
@@ -64,10 +58,7 @@ __global__ void __launch_bounds__(32 * kRateWarps)
         const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
         const RayCols cols = ray_columns(g, __ldg(tau + r), __ldg(tau + nray + r), __ldg(tau + 2 * nray + r), rw, geo);
         double out[6];
-        if (kMode == ARGOT_B200_RATE_EXACT_F64)
-          rate_bins_f64(cols, spec64 + (size_t)e * kNu, out);
-        else
-          rate_bins_f32(cols, specn + (size_t)e * kNu, __ldg(total + e), out);
+        rate_bins_f64(cols, spec64 + (size_t)e * kNu, out);
 #pragma unroll
         for (int s = 0; s < 6; s++) buf[wib][lane][s] = out[s];
       }
@@ -77,42 +68,37 @@ __global__ void __launch_bounds__(32 * kRateWarps)
       for (int k = 0; k < nk; k++) {
         if (tl[wib][k] == lane) {
 #pragma unroll
-          for (int s = 0; s < 6; s++) {
-            if (kMode == ARGOT_B200_RATE_EXACT_F64)
-              accf[s] = __double2float_rn(__dadd_rn((double)accf[s], buf[wib][k][s]));
-            else
-              accd[s] += buf[wib][k][s];
-          }
+          for (int s = 0; s < 6; s++) accf[s] = __double2float_rn(__dadd_rn((double)accf[s], buf[wib][k][s]));
         }
       }
       __syncwarp();
     }
     if (own_valid) {
 #pragma unroll
-      for (int s = 0; s < 6; s++)
-        rates6[s * ncell + own] = (kMode == ARGOT_B200_RATE_EXACT_F64) ? accf[s] : (float)accd[s];
+      for (int s = 0; s < 6; s++) rates6[s * ncell + own] = accf[s];
     }
   }
 }
 
 // ------------------------------------------------------------ FP32 rates
 // One warp per target block, rays in chunks of 32.  Phase A: lane i forms
-// the FP64 per-ray parameters of ray i of the chunk (geometry, columns,
-// prefactors).  Phase B: the warp splits into four groups of eight lanes;
-// a group takes one ray at a time and its lanes share the 256 frequency
-// bins (lane j: bins j, j+8, ..., two at a time with the packed f32x2
-// arithmetic, ray_bins_packed), reading the frequency tables from shared
-// memory; three butterfly steps sum the eight partial sums.  Phase C: lane
-// j adds the rays that end in cell j of the block, in ray order.
+// the FP32 per-ray parameters of ray i of the chunk (ray_params_f32).
+// Phase B: the warp splits into four groups of eight lanes; a group takes
+// one ray at a time and its lanes share the 256 frequency bins (lane j:
+// bins j, j+8, ..., two at a time with the packed f32x2 arithmetic,
+// ray_bins_packed), reading the bin-pair table from shared memory; three
+// butterfly steps sum the eight partial sums.  Phase C: every lane adds the
+// rays that end in its cell, in ray order (add_chunk_in_order).  The
+// kernel has no FP64 arithmetic.
 // Launch shape: ARGOT_RATE_WARPS warps per CTA, at least ARGOT_RATE_MIN_CTAS
 // CTAs resident per SM (which caps the registers per thread).  Measured on
-// B200 (192^3, 1024 sources): 8 warps x 4 CTAs (64 registers) is 19% faster
-// than 4 warps at 72 registers.
+// B200 (256^3, 4096 sources, 3.2e9 rays): 8 warps x 3 CTAs (80 registers,
+// no spills) 1.07 s, x 4 CTAs (64 registers) 1.08 s, x 5 CTAs 1.34 s.
 #ifndef ARGOT_RATE_WARPS
 #define ARGOT_RATE_WARPS 8
 #endif
 #ifndef ARGOT_RATE_MIN_CTAS
-#define ARGOT_RATE_MIN_CTAS 4
+#define ARGOT_RATE_MIN_CTAS 3
 #endif
 constexpr int kF32Warps = ARGOT_RATE_WARPS;
 
@@ -288,9 +274,8 @@ extern "C" int argot_b200_photoion_rays(const argot_b200_grid *gp, const void *p
   const int threads = 32 * kRateWarps;
   const int blocks = grid_blocks_for_rates((b1 - b0) * 32, threads);
   if (mode == ARGOT_B200_RATE_EXACT_F64)
-    k_rate_blocks<ARGOT_B200_RATE_EXACT_F64><<<blocks, threads, 0, st>>>(
-        g, raw, t->emit_pos, t->emit_spec64, t->emit_specn, t->emit_total, b0, b1, blk_off, base, rays, nray, tau,
-        rates6, err);
+    k_rate_blocks<<<blocks, threads, 0, st>>>(g, raw, t->emit_pos, t->emit_spec64, b0, b1, blk_off, base, rays,
+                                              nray, tau, rates6, err);
   else
     k_rate_f32<false><<<grid_blocks_for_rates((b1 - b0) * 32, 32 * kF32Warps), 32 * kF32Warps, 0, st>>>(
         g, raw, t->emit_pos, t->emit_specn, t->emit_total, b0, b1, blk_off, base, rays, nray, tau, rates6,

@@ -139,90 +139,101 @@ __device__ __forceinline__ float ex2_approx(float x) {
   return y;
 }
 
-// (1 - e^-x)/x.  Below x = 0.1 the difference 1 - e^-x cancels, so the
-// value is taken in FP64 from its Taylor series (error < x^6/5040 < 2e-10);
-// above, FP32 with the hardware exponential is accurate to ~3e-6.
-__device__ __forceinline__ float phi_pc(float x, float e_minus_x) {
-  if (x < 0.1f) {
-    const double d = (double)x;
-    double p = fma(d, -1.0 / 720.0, 1.0 / 120.0);
-    p = fma(d, p, -1.0 / 24.0);
-    p = fma(d, p, 1.0 / 6.0);
-    p = fma(d, p, -0.5);
-    p = fma(d, p, 1.0);
-    return (float)p;
-  }
-  return __fdividef(1.0f - e_minus_x, x);
-}
-
-// Per-ray parameters of the FP32 bin loop: columns to the cell's entry face
-// and of the cell [cm^-2] as floats, and the FP64 prefactors
-// total * dN_s / (n_s V_shell) of the three species.
+// ---------------------------------------------------------------------------
+// FP32 rates.  Per ray: the columns to the target cell's entry face N_s and
+// of the cell D_s [cm^-2] and the prefactor P_s = total dN_s / (n_s V_shell)
+// (calc_photoion_rate.c:159-246), all in FP32.  With dN_s = n_s delta lunit
+// and V_shell = 4 pi / 3 ((r + delta/2)^3 - (r - delta/2)^3) lunit^3 =
+// 4 pi (r^2 + delta^2 / 12) delta lunit^3 (the cube difference expanded,
+// which has no cancellation), the density cancels:
+// P_s = total / (4 pi lunit^2 (r^2 + delta^2 / 12)) for n_s > 0 and 0 for
+// n_s = 0 (the reference's TINY only keeps 0/0 away; its n_s V_shell is
+// above 1e40 whenever n_s is a positive float).  total (1e48-1e52 photons/s)
+// and 1/(4 pi lunit^2) (1e-46) are outside the FP32 range, so their powers
+// of two are added as integers and P_s (1e4-1e13) is formed in range.
 struct RayParams {
-  float N[3], D[3];
-  double P[3];
+  float N[3], D[3], P[3];
 };
 
-__device__ __forceinline__ RayParams ray_params(const RayCols &c, double total) {
+// v = m * 2^e for a positive double, m in [1, 2) from the leading 24
+// significant bits (integer operations on the bit pattern)
+__device__ __forceinline__ float mant_exp2(double v, int &e) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  e = (int)((b >> 52) & 0x7ffu) - 1023;
+  return __uint_as_float(0x3f800000u | (unsigned)((b >> 29) & 0x7fffffu));
+}
+
+constexpr float kHeliumFactF = (float)kHeliumFact;
+constexpr float kHNuLf = (float)kHNuL;
+
+// The FP32 parameters of a ray from emitter (sx, sy, sz) to the centre of
+// target cell (gix, giy, giz) (global indices) with code-unit columns t_s;
+// raw = {dens, fHI, fHeI, fHeII} of the target cell.  A ray that starts at
+// its target's centre (r = 0) contributes nothing, as in the reference,
+// whose shell volume then diverges.
+__device__ __forceinline__ RayParams ray_params_f32(const GridDev &g, int gix, int giy, int giz, float sx,
+                                                    float sy, float sz, float t0, float t1, float t2, float4 raw,
+                                                    double total) {
   RayParams p;
+  const float x = fmaf((float)gix + 0.5f, g.dx, g.xmin);
+  const float y = fmaf((float)giy + 0.5f, g.dy, g.ymin);
+  const float z = fmaf((float)giz + 0.5f, g.dz, g.zmin);
+  const float dx = x - sx, dy = y - sy, dz = z - sz;
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  // delta_length (calc_photoion_rate.c:52-90): the cell's chord along the
+  // ray, min over the axes of the cell side over |cosine|
+  const float delta = sqrtf(r2) * fminf(__fdividef(g.dx, fabsf(dx)),
+                                        fminf(__fdividef(g.dy, fabsf(dy)), __fdividef(g.dz, fabsf(dz))));
+  const float n[3] = {raw.x * raw.y, (raw.x * kHeliumFactF) * raw.z, (raw.x * kHeliumFactF) * raw.w};
+  const float tt[3] = {t0, t1, t2};
+  const float dc = delta * g.cdf;
+  int et;
+  const float mt = mant_exp2(total, et);
+  const float pv = ldexpf(__fdividef(mt * g.pcm, fmaf(delta * delta, 1.f / 12.f, r2)), et + g.pce);
+  const bool ok = r2 > 0.f;
 #pragma unroll
   for (int s = 0; s < 3; s++) {
-    p.N[s] = (float)c.N[s];
-    p.D[s] = (float)c.dN[s];
-    p.P[s] = total * c.dN[s] * c.rN[s];
+    p.D[s] = ok ? n[s] * dc : 0.f;
+    p.N[s] = ok ? fmaf(tt[s], g.cdf, -0.5f * p.D[s]) : 0.f;
+    p.P[s] = (ok && n[s] > 0.f) ? pv : 0.f;
   }
   return p;
 }
 
-// FP32 rates: the same integral with the spectrum normalised by its total
-// (FP32 cannot hold photon rates of 1e50 or rates of 1e-58) and the FP64
-// per-ray prefactor total * dN_s * rN_s applied once.  Sums run in FP32 over
-// 32 bins and are carried in FP64 across blocks of bins.
-static __device__ __noinline__ void rate_bins_f32(const RayCols &c, const float *__restrict__ specn, double total,
-                                           double out[6]) {
-  const float N0 = (float)c.N[0], N1 = (float)c.N[1], N2 = (float)c.N[2];
-  const float D0 = (float)c.dN[0], D1 = (float)c.dN[1], D2 = (float)c.dN[2];
-  const float ln2 = 0.69314718055994531f;
-  double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int k0 = 0; k0 < kNu; k0 += 32) {
-    float g0 = 0.f, g1 = 0.f, g2 = 0.f, h0 = 0.f, h1 = 0.f, h2 = 0.f;
-#pragma unroll 8
-    for (int k = k0; k < k0 + 32; k++) {
-      const float a0 = c_tab.cs_l2e[0][k], a1 = c_tab.cs_l2e[1][k], a2 = c_tab.cs_l2e[2][k];
-      const float tl2 = fmaf(N0, a0, fmaf(N1, a1, N2 * a2));
-      const float dl2 = fmaf(D0, a0, fmaf(D1, a1, D2 * a2));
-      const float e = ex2_approx(-tl2);
-      const float ed = ex2_approx(-dl2);
-      const float w = __ldg(specn + spec_pair_index(k)) * e * phi_pc(dl2 * ln2, ed);
-      g0 = fmaf(c_tab.cs[0][k], w, g0);
-      g1 = fmaf(c_tab.cs[1][k], w, g1);
-      g2 = fmaf(c_tab.cs[2][k], w, g2);
-      h0 = fmaf(c_tab.hw[0][k], w, h0);
-      h1 = fmaf(c_tab.hw[1][k], w, h1);
-      h2 = fmaf(c_tab.hw[2][k], w, h2);
-    }
-    acc[0] += g0; acc[1] += g1; acc[2] += g2;
-    acc[3] += h0; acc[4] += h1; acc[5] += h2;
-  }
+// The six rates of one ray from its quadrature sums a_s = sum (sigma_s
+// log2 e) w and b_s = sum (sigma_s log2 e) nu w (ray_bins_packed):
+// Gamma_s = P_s ln2 a_s, Heat_s = P_s ln2 (b_s - nu_s a_s) h nu_L.
+__device__ __forceinline__ void ray_rates6(const float (&P)[3], float a0, float a1, float a2, float b0, float b1,
+                                           float b2, float (&out)[6]) {
+  const float kLn2 = 0.69314718055994531f;
+  const float a[3] = {a0, a1, a2}, bb[3] = {b0, b1, b2};
+  const float thr[3] = {(float)kThrHI, (float)kThrHeI, (float)kThrHeII};
 #pragma unroll
   for (int s = 0; s < 3; s++) {
-    const double p = total * c.dN[s] * c.rN[s];
-    out[s] = p * acc[s];
-    out[3 + s] = p * acc[3 + s] * kHNuL;
+    out[s] = P[s] * (kLn2 * a[s]);
+    out[3 + s] = P[s] * (kLn2 * fmaf(-thr[s], a[s], bb[s])) * kHNuLf;
   }
 }
 
 // ---- packed FP32 bin loop: two bins per instruction with the f32x2 FMA
 // and multiply of sm_100.  An 8-lane group integrates one ray; lane j owns
 // the bin pairs (j + 16 i, j + 16 i + 8), i = 0..15 (the bins j + 8 m), and
-// keeps one partial sum per output and pair member.  Aligned to 16 bytes so
-// that a lane reads its pair with five 16-byte shared loads (measured: rates
-// 2% faster than with the 8-byte alignment of float2).
+// keeps one partial sum per output and pair member.
+// The pair table holds sigma_s log2(e) of the three species and nu of the
+// two bins, 32 bytes, two 16-byte shared loads per pair.  The sums run on
+// these entries: sum sigma_s w = ln2 sum (sigma_s log2 e) w, and, because
+// sigma_s vanishes below the species' threshold nu_s (the fits of
+// prim_chem/cross_section.c are 0 there), the heating sum
+// sum sigma_s (nu - nu_s)^+ w = ln2 (sum (sigma_s log2 e) nu w - nu_s
+// sum (sigma_s log2 e) w).  A 128-bit shared load is served in four
+// wavefronts whatever the broadcast, and the four groups of a warp read the
+// same entries, so the table's size sets the kernel's shared-memory
+// traffic: the earlier 80-byte entry (sigma log2 e, sigma and
+// sigma (nu - nu_s)^+ per species) kept the shared-memory pipe at 79% of
+// its peak (ncu, 256^3 / 16 sources).
 struct alignas(16) BinPair {
   float2 l2e[3];  // sigma_s log2(e) of the two bins
-  float2 cs[3];   // sigma_s
-  float2 hw[3];   // sigma_s ((float) nu - nu_s)^+
-  float2 pad;     // 80 B: the eight lanes of a group hit distinct banks
+  float2 nu;      // (float) nu of the two bins
 };
 constexpr int kBinPairs = kNu / 2;
 
@@ -234,28 +245,43 @@ __device__ __forceinline__ void load_bin_pairs(BinPair *tab) {
     const int k0 = j + 16 * i, k1 = k0 + 8;
     BinPair b;
 #pragma unroll
-    for (int s = 0; s < 3; s++) {
-      b.l2e[s] = make_float2(c_tab.cs_l2e[s][k0], c_tab.cs_l2e[s][k1]);
-      b.cs[s] = make_float2(c_tab.cs[s][k0], c_tab.cs[s][k1]);
-      b.hw[s] = make_float2(c_tab.hw[s][k0], c_tab.hw[s][k1]);
-    }
-    b.pad = make_float2(0.f, 0.f);
+    for (int s = 0; s < 3; s++) b.l2e[s] = make_float2(c_tab.cs_l2e[s][k0], c_tab.cs_l2e[s][k1]);
+    b.nu = make_float2(c_tab.nu_f[k0], c_tab.nu_f[k1]);
     tab[p] = b;
   }
 }
 
-// phi_pc of dl2 = dtau log2(e), with e^-dtau evaluated only where it is
-// used (dtau >= 0.1): same values as phi_pc, one exponential fewer in the
-// thin bins.
-__device__ __forceinline__ float phi_pc_lazy(float dl2) {
-  const float x = dl2 * 0.69314718055994531f;
-  if (x < 0.1f) return phi_pc(x, 0.f);
-  return phi_pc(x, ex2_approx(-dl2));
+// The photon-conserving cell factor phi(x) = (1 - e^-x)/x of the two bins
+// of a pair from dl2 = x log2(e).  Below x = 1 the difference 1 - e^-x
+// cancels, so phi comes from a degree-6 polynomial, a near-minimax fit of
+// relative error made by argot_b200/fits.py (8.8e-8 relative on [0, 1]
+// evaluated in FP32 with Horner's rule, checked by the CPU tests).  Above,
+// e^-x on the SFU: (1 - e^-x) / x to ~2e-7.  The SFU path is taken only
+// when a lane of the warp needs it.
+constexpr float kPhiXMax = 1.0f;
+__device__ __forceinline__ float2 phi_pc2(float2 dl2) {
+  constexpr float kPhiC[7] = {1.f, -0.499999762f, 0.166663095f, -0.041645579f, 0.00827309582f, -0.00129866367f,
+                              0.000128380707f};
+  const float kLn2 = 0.69314718055994531f;
+  const float2 x = __fmul2_rn(dl2, make_float2(kLn2, kLn2));
+  float2 p = make_float2(kPhiC[6], kPhiC[6]);
+#pragma unroll
+  for (int k = 5; k >= 0; k--) p = __ffma2_rn(x, p, make_float2(kPhiC[k], kPhiC[k]));
+  const bool t0 = x.x < kPhiXMax, t1 = x.y < kPhiXMax;
+  if (!(t0 && t1)) {
+    const float q0 = __fdividef(1.0f - ex2_approx(-dl2.x), x.x);
+    const float q1 = __fdividef(1.0f - ex2_approx(-dl2.y), x.y);
+    p.x = t0 ? p.x : q0;
+    p.y = t1 ? p.y : q1;
+  }
+  return p;
 }
 
-// The lane's six partial sums (Gamma then heating of HI, HeI, HeII) of one
-// ray with columns N (to the cell) and D (of the cell) in cm^-2; sp: the
-// emitter's normalised spectrum.  The caller adds the eight lanes.
+// The lane's six partial sums of one ray with columns N (to the cell) and
+// D (of the cell) in cm^-2; sp: the emitter's normalised spectrum:
+// out[s] = sum (sigma_s log2 e) w, out[3 + s] = sum (sigma_s log2 e) nu w
+// over the lane's bins, w = s_nu e^-tau phi(dtau).  The caller adds the
+// eight lanes and forms the rates (ray_rates6).
 __device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab, const float *__restrict__ sp,
                                                 int j, float N0, float N1, float N2, float D0, float D1, float D2,
                                                 float (&out)[6]) {
@@ -268,21 +294,20 @@ __device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab,
   for (int i = 0; i < kBinPairs / 8; i++) {
     const BinPair &b = tab[j + 8 * i];
     const float2 l0 = b.l2e[0], l1 = b.l2e[1], l2 = b.l2e[2];
-    const float2 c0 = b.cs[0], c1 = b.cs[1], c2 = b.cs[2];
-    const float2 w0 = b.hw[0], w1 = b.hw[1], w2 = b.hw[2];
     const float2 tl = __ffma2_rn(n0, l0, __ffma2_rn(n1, l1, __fmul2_rn(n2, l2)));
     const float2 dl = __ffma2_rn(d0, l0, __ffma2_rn(d1, l1, __fmul2_rn(d2, l2)));
     // the pair's two spectrum bins in one 8-byte load (pair order)
     const float2 s = __ldg(reinterpret_cast<const float2 *>(sp) + j + 8 * i);
     const float2 e = make_float2(ex2_approx(-tl.x), ex2_approx(-tl.y));
-    const float2 ph = make_float2(phi_pc_lazy(dl.x), phi_pc_lazy(dl.y));
+    const float2 ph = phi_pc2(dl);
     const float2 w = __fmul2_rn(__fmul2_rn(s, e), ph);
-    acc[0] = __ffma2_rn(c0, w, acc[0]);
-    acc[1] = __ffma2_rn(c1, w, acc[1]);
-    acc[2] = __ffma2_rn(c2, w, acc[2]);
-    acc[3] = __ffma2_rn(w0, w, acc[3]);
-    acc[4] = __ffma2_rn(w1, w, acc[4]);
-    acc[5] = __ffma2_rn(w2, w, acc[5]);
+    const float2 vw = __fmul2_rn(b.nu, w);
+    acc[0] = __ffma2_rn(l0, w, acc[0]);
+    acc[1] = __ffma2_rn(l1, w, acc[1]);
+    acc[2] = __ffma2_rn(l2, w, acc[2]);
+    acc[3] = __ffma2_rn(l0, vw, acc[3]);
+    acc[4] = __ffma2_rn(l1, vw, acc[4]);
+    acc[5] = __ffma2_rn(l2, vw, acc[5]);
   }
 #pragma unroll
   for (int q = 0; q < 6; q++) out[q] = acc[q].x + acc[q].y;
@@ -290,19 +315,58 @@ __device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab,
 
 // Per-warp scratch of rate_block_f32.
 struct RateWarpSmem {
-  float nd[32][6];    // N_s, dN_s of the chunk's rays (cm^-2)
-  double p[32][3];    // prefactors
-  double out[32][6];  // per-ray rates
-  int e[32], t[32];   // emitter, target lane
-  int q[32];          // lanes of the chunk's rays that take the quadrature
+  float nd[32][6];   // N_s, D_s of the chunk's rays (cm^-2)
+  float p[32][3];    // prefactors P_s
+  float out[32][6];  // per-ray rates
+  int e[32], t[32];  // emitter, target lane
+  int q[32];         // lanes of the chunk's rays that take the quadrature
+  int cnt[32], src[32];  // per target lane: rays of the chunk, ray of the round
 };
+
+// A cell's six rates summed over its rays in ray order, FP32 with Kahan
+// compensation (a cell receives up to a few hundred rays).
+struct CellSum6 {
+  float s[6], c[6];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int q = 0; q < 6; q++) s[q] = c[q] = 0.f;
+  }
+  __device__ __forceinline__ void add(const float *v) {
+#pragma unroll
+    for (int q = 0; q < 6; q++) kahan_add(s[q], c[q], v[q]);
+  }
+};
+
+// Phase C of the block-rate kernels: lane k holds ray k of a chunk (its six
+// values in out[k], its target lane t, -1 for none); every lane adds the
+// rays that end in its cell, in ray order.  __match_any_sync ranks each ray
+// among the chunk's rays with the same target; round r hands every cell
+// its rank-r ray through `src`, so a chunk whose rays end in distinct cells
+// takes one round (instead of every lane scanning the chunk's 32 rays).
+__device__ __forceinline__ void add_chunk_in_order(CellSum6 &acc, int lane, int t, const float (*out)[6],
+                                                   int *cnt, int *src) {
+  const unsigned same = __match_any_sync(0xffffffffu, t);
+  const int rank = __popc(same & ((1u << lane) - 1u));
+  cnt[lane] = 0;
+  __syncwarp();
+  if (t >= 0 && rank == 0) cnt[t] = __popc(same);
+  const int rounds = __reduce_max_sync(0xffffffffu, t >= 0 ? rank + 1 : 0);
+  __syncwarp();
+  const int mine = cnt[lane];
+  for (int r = 0; r < rounds; r++) {
+    if (t >= 0 && rank == r) src[t] = lane;
+    __syncwarp();
+    if (r < mine) acc.add(out[src[lane]]);
+    __syncwarp();
+  }
+}
 
 // The FP32 rates of one target block b whose rays are [r0, r1) of `rays`
 // (columns in three planes of nray), written to its cells in rates6; one
-// warp.  Phase A: per-ray parameters, one lane per ray, 32 rays at a time.
-// Phase B: four 8-lane groups, one ray each, over the bin pairs
-// (ray_bins_packed), three butterfly steps.  Phase C: lane j adds the rays
-// of cell j of the block in ray order.
+// warp.  Phase A: per-ray parameters (ray_params_f32), one lane per ray, 32
+// rays at a time.  Phase B: four 8-lane groups, one ray each, over the bin
+// pairs (ray_bins_packed), three butterfly steps.  Phase C: lane j adds the
+// rays of cell j of the block in ray order (add_chunk_in_order).
 // kServed: `pred` holds 7 planes of nray floats, six per-ray contributions
 // and a flag; a ray whose flag is non-zero contributes those six values
 // and skips the quadrature, which runs over the remaining rays of the
@@ -321,7 +385,8 @@ __device__ __forceinline__ void rate_block_f32(const GridDev &g, const float4 *_
   int ix, iy, iz;
   const bool own_valid = block_cell(g, b, lane, &ix, &iy, &iz);
   const uint64_t own = own_valid ? cell_index(g, ix, iy, iz) : 0;
-  double acc[6] = {0, 0, 0, 0, 0, 0};
+  CellSum6 acc;
+  acc.zero();
   int bix, biy, biz;
   block_cell(g, b, 0, &bix, &biy, &biz);
   for (uint64_t rc = r0; rc < r1; rc += 32) {
@@ -334,15 +399,14 @@ __device__ __forceinline__ void rate_block_f32(const GridDev &g, const float4 *_
       t = (int)(w & 31u);
       if (kServed && __ldg(pred + 6 * nray + r) != 0.f) {
 #pragma unroll
-        for (int s = 0; s < 6; s++) S.out[lane][s] = (double)__ldg(pred + s * nray + r);
+        for (int s = 0; s < 6; s++) S.out[lane][s] = __ldg(pred + s * nray + r);
       } else {
         quad = true;
         const int lx = bix + (t >> 4), ly = biy + ((t >> 2) & 3), lz = biz + (t & 3);
         const float4 ep = __ldg(emit_pos + e);
-        const RayGeom geo = ray_geometry(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z);
         const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
-        const RayCols cols = ray_columns(g, __ldg(tau + r), __ldg(tau + nray + r), __ldg(tau + 2 * nray + r), rw, geo);
-        const RayParams p = ray_params(cols, __ldg(total + e));
+        const RayParams p = ray_params_f32(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z, __ldg(tau + r),
+                                           __ldg(tau + nray + r), __ldg(tau + 2 * nray + r), rw, __ldg(total + e));
 #pragma unroll
         for (int s = 0; s < 3; s++) {
           S.nd[lane][s] = p.N[s];
@@ -366,38 +430,25 @@ __device__ __forceinline__ void rate_block_f32(const GridDev &g, const float4 *_
       float part[6];
       ray_bins_packed(pairs, specn + (size_t)S.e[q] * kNu, j, S.nd[q][0], S.nd[q][1], S.nd[q][2], S.nd[q][3],
                       S.nd[q][4], S.nd[q][5], part);
-      float g0 = part[0], g1 = part[1], g2 = part[2], h0 = part[3], h1 = part[4], h2 = part[5];
 #pragma unroll
       for (int o = 1; o < 8; o <<= 1) {
-        g0 += __shfl_xor_sync(gmask, g0, o);
-        g1 += __shfl_xor_sync(gmask, g1, o);
-        g2 += __shfl_xor_sync(gmask, g2, o);
-        h0 += __shfl_xor_sync(gmask, h0, o);
-        h1 += __shfl_xor_sync(gmask, h1, o);
-        h2 += __shfl_xor_sync(gmask, h2, o);
+#pragma unroll
+        for (int s = 0; s < 6; s++) part[s] += __shfl_xor_sync(gmask, part[s], o);
       }
       if (j == 0) {
-        const double p0 = S.p[q][0], p1 = S.p[q][1], p2 = S.p[q][2];
-        S.out[q][0] = p0 * g0;
-        S.out[q][1] = p1 * g1;
-        S.out[q][2] = p2 * g2;
-        S.out[q][3] = p0 * h0 * kHNuL;
-        S.out[q][4] = p1 * h1 * kHNuL;
-        S.out[q][5] = p2 * h2 * kHNuL;
-      }
-    }
-    __syncwarp();
-    for (int k = 0; k < nk; k++) {
-      if (S.t[k] == lane) {
+        const float P[3] = {S.p[q][0], S.p[q][1], S.p[q][2]};
+        float out[6];
+        ray_rates6(P, part[0], part[1], part[2], part[3], part[4], part[5], out);
 #pragma unroll
-        for (int s = 0; s < 6; s++) acc[s] += S.out[k][s];
+        for (int s = 0; s < 6; s++) S.out[q][s] = out[s];
       }
     }
     __syncwarp();
+    add_chunk_in_order(acc, lane, t, S.out, S.cnt, S.src);
   }
   if (own_valid) {
 #pragma unroll
-    for (int s = 0; s < 6; s++) rates6[s * ncell + own] = (float)acc[s];
+    for (int s = 0; s < 6; s++) rates6[s * ncell + own] = acc.s[s];
   }
 }
 

@@ -218,10 +218,9 @@ __device__ __forceinline__ RayTask ray_task(const GridDev &g, const float4 *__re
   t.tl = (int)(w & 31u);
   const int lx = bix + (t.tl >> 4), ly = biy + ((t.tl >> 2) & 3), lz = biz + (t.tl & 3);
   const float4 ep = __ldg(emit_pos + t.e);
-  const RayGeom geo = ray_geometry(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z);
   const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
-  const RayCols cols = ray_columns(g, __ldg(tau + r), __ldg(tau + nray + r), __ldg(tau + 2 * nray + r), rw, geo);
-  t.p = ray_params(cols, __ldg(total + t.e));
+  t.p = ray_params_f32(g, g.ix0 + lx, g.iy0 + ly, g.iz0 + lz, ep.x, ep.y, ep.z, __ldg(tau + r), __ldg(tau + nray + r),
+                       __ldg(tau + 2 * nray + r), rw, __ldg(total + t.e));
   return t;
 }
 
@@ -377,8 +376,8 @@ __global__ void __launch_bounds__(32 * kSurWarps, ARGOT_SUR_PREDICT_MIN_CTAS)
           eps += kGLErr;
 #pragma unroll
           for (int s = 0; s < 3; s++) {
-            cj[s] = (float)(p.P[s] * (double)G[s] * __ldg(emit_i0 + 6 * (size_t)e + s));
-            cj[3 + s] = (float)(p.P[s] * (double)G[3 + s] * __ldg(emit_i0 + 6 * (size_t)e + 3 + s) * kHNuL);
+            cj[s] = (float)((double)p.P[s] * (double)G[s] * __ldg(emit_i0 + 6 * (size_t)e + s));
+            cj[3 + s] = (float)((double)p.P[s] * (double)G[3 + s] * __ldg(emit_i0 + 6 * (size_t)e + 3 + s) * kHNuL);
           }
         }
         // the cell budget is taken from a lower bound of the true total:

@@ -97,6 +97,15 @@ def measured_peaks():
     return 6650.0, 1590.0, "fallback"
 
 
+def workload_config(wl, ws: int, sharded: bool) -> dict:
+    """The `config` of a bench line: what defines the workload, the same in
+    both arms (the run's own details go to `run`)."""
+    return {"workload": wl.name, "mesh": f"{wl.edge}^3", "sources": wl.nsrc, "theta": wl.theta,
+            "l2": "inputs larger than L2 (rays and fields of the whole problem); no flush",
+            "parallelism": (f"{ws} ranks, target x-slabs of one problem, rate slabs all-gathered"
+                            if sharded else f"{ws} independent problems (one per rank)")}
+
+
 # ------------------------------------------------------------ clocks
 class ClockSampler:
     """nvidia-smi samples during the timed region (clocks and throttle
@@ -335,10 +344,8 @@ def load_surrogate(pb):
 
 def compare_rate_modes(pb, rays, tau, prec, sur):
     """One pass of each rate kernel over every group after the same march:
-    device time of each (CUDA events around the rate launches only) and the
-    per-cell error of the FP32 and surrogate fields against the FP64
-    reference-order field (the same algorithm as the reference's FP64
-    arithmetic, itself held to the FP64 oracle by the GPU tests)."""
+    device time of each (CUDA events around the rate launches only).  Their
+    errors come from `sampled_parity` (against the FP64 CPU oracle)."""
     import torch
     from argot_b200 import _lib as L
     dev = pb.device
@@ -378,27 +385,47 @@ def compare_rate_modes(pb, rays, tau, prec, sur):
             e1.synchronize()
             t[m] += e0.elapsed_time(e1) / 1e3
     pb.check_device_error()
-    ref = fields["exact_f64"].view(6, -1).double()
     out = {}
-    names = ("gamma_HI", "gamma_HeI", "gamma_HeII", "heat_HI", "heat_HeI", "heat_HeII")
     for m, _ in modes:
-        d = {"s": t[m], "gamma_cells_per_s": pb.ncell / t[m], "rays_per_s": pb.nray / t[m],
-             "speedup_vs_exact_f64": t["exact_f64"] / t[m]}
-        if m != "exact_f64":
-            x = fields[m].view(6, -1).double()
-            err = {}
-            for j, nm in enumerate(names):
-                r = ref[j]
-                pos = r > 0
-                rel = ((x[j] - r).abs()[pos] / r[pos])
-                err[nm] = float(rel.max().item()) if rel.numel() else 0.0
-            d["max_rel_err_vs_f64"] = err
-        out[m] = d
+        out[m] = {"s": t[m], "gamma_cells_per_s": pb.ncell / t[m], "rays_per_s": pb.nray / t[m],
+                  "speedup_vs_exact_f64": t["exact_f64"] / t[m]}
     if sur is not None:
         c = counters.cpu().numpy()
         out["surrogate"]["rays_surrogate"] = int(c[0])
         out["surrogate"]["rays_exact_fallback"] = int(c[1])
         out["surrogate"]["fallback_frac"] = float(c[1] / max(1, c[0] + c[1]))
+    return out
+
+
+# ------------------------------------------------------------ parity check
+def sampled_parity(pb, wl, sur, runs: int = 16, length: int = 16, seed: int = 11):
+    """The checker on this workload: seeded runs of target cells computed by
+    the reference's own group loop (ARGOT's C, O1) and by the FP64 CPU
+    oracle pipeline (FP64 march + FP64 rates) on O1's rays, against the
+    device path on the target blocks holding them (oracle/sampled.py).
+    Reported per rate mode: the largest relative error per output field
+    over the sampled cells; for the reference-order path its ray lists and
+    columns against O1 and its FP64 rates against O1's."""
+    from argot_b200 import _lib as L
+    from oracle.sampled import SampledParity, z_runs
+    t0 = time.time()
+    sp = SampledParity(wl, z_runs(wl.edge, runs, length, seed))
+    ref, f64 = sp.reference(), sp.fp64()
+    r64, rays = sp.device(pb, L.PRECISION_REFERENCE, L.RATE_EXACT_F64, want_rays=True)
+    same_list, same_tau = sp.same_rays(rays)
+    r32, rays_k = sp.device(pb, L.PRECISION_KAHAN, L.RATE_EXACT_F32, want_rays=True)
+    out = {"sample": (f"{runs} seeded runs of {length} consecutive target cells along z "
+                      f"({len(sp.all_cells())} cells, {len(ref['tgt'])} rays)"),
+           "oracle": "O1 = ARGOT's C (reference order, FP32 march, FP64 rates); "
+                     "FP64 = orc_march_f64 + orc_photoion_f64 on O1's rays",
+           "reference_order": {"ray_lists_equal_O1": bool(same_list), "columns_bitwise_O1": bool(same_tau),
+                               "exact_f64_rates_vs_O1": sp.rate_errors(r64, ref["rates"])},
+           "kahan_columns_vs_fp64": sp.column_error_vs_f64(rays_k),
+           "exact_f32_vs_fp64": sp.rate_errors(r32, f64["rates"])}
+    if sur is not None:
+        rs, _ = sp.device(pb, L.PRECISION_KAHAN, surrogate=sur)
+        out["surrogate_vs_fp64"] = sp.rate_errors(rs, f64["rates"])
+    out["s"] = time.time() - t0
     return out
 
 
@@ -486,6 +513,14 @@ def run_ours(args):
     t_march = ev[0].elapsed_time(ev[1]) / 1e3
     t_rates = ev[1].elapsed_time(ev[2]) / 1e3
     rate_modes = None if args.no_rate_modes else compare_rate_modes(pb, rays, tau, prec, sur)
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = sampled_parity(pb, wl, sur)
+        if rate_modes is not None:
+            rate_modes["exact_f64"]["max_rel_err_vs_O1"] = parity["reference_order"]["exact_f64_rates_vs_O1"]
+            rate_modes["exact_f32"]["max_rel_err_vs_fp64_oracle"] = parity["exact_f32_vs_fp64"]
+            if "surrogate" in rate_modes and "surrogate_vs_fp64" in parity:
+                rate_modes["surrogate"]["max_rel_err_vs_fp64_oracle"] = parity["surrogate_vs_fp64"]
     # the next stage of an iteration: the 27-point smoothing of the rates
     # (smooth_photoion_rate.c), on the device
     smoothed = torch.empty_like(rates6)
@@ -540,13 +575,9 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
         "higher_is_better": True, "scaling": "strong" if sharded else "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded lognormal mesh + clustered sources)",
-        "config": {"workload": wl.name, "mesh": f"{wl.edge}^3", "sources": wl.nsrc,
-                   "theta": wl.theta, "rays": nray_mine, "crossings": n_cross,
-                   "march": args.precision, "rates": args.rate, "ray_groups": len(pb.groups),
-                   "overlap_parts": overlap,
-                   "l2": "inputs larger than L2 (13 GB rays, 268 MB field); no flush",
-                   "parallelism": (f"{ws} ranks, target x-slabs of one problem, rate slabs all-gathered"
-                                   if sharded else f"{ws} independent problems (one per GPU)")},
+        "config": workload_config(wl, ws, sharded),
+        "run": {"rays": nray_mine, "crossings": n_cross, "march": args.precision, "rates": args.rate,
+                "ray_groups": len(pb.groups), "overlap_parts": overlap},
         "gamma_cells_per_s": total_cells / t,
         "split": {"march_s": t_march, "rates_s": t_rates,
                   "march_crossings_per_s": n_cross / t_march,
@@ -567,6 +598,8 @@ def run_ours(args):
     }
     if rate_modes is not None:
         line["rate_modes"] = rate_modes
+    if parity is not None:
+        line["parity"] = parity
     if e2e is not None:
         line["e2e"] = e2e
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -935,8 +968,7 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "impl": "reference",
         "data": "synthetic (seeded lognormal mesh + clustered sources)",
-        "config": {"workload": wl.name, "mesh": f"{wl.edge}^3", "sources": wl.nsrc,
-                   "theta": wl.theta},
+        "config": workload_config(wl, ws, False),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"], "kind": "reference",
                          "sample": info["sample"] + " (per step; median over steps)"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -1012,6 +1044,8 @@ def main(argv=None):
                    help="cut the ray group into N parts and overlap the march of one part with the "
                         "rates of the previous one on two streams (0: one stream, kernels in sequence)")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-parity", action="store_true",
+                   help="skip the sampled parity check against the reference and the FP64 oracle")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-reference-gpu", action="store_true",
                    help="skip the sample of ARGOT's own GPU kernels built for sm_100a")

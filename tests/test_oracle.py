@@ -190,3 +190,19 @@ def test_reference_fast_math_spread(oracle):
     ts = oracle.march_f32ref(unit_box_grid(64, wl.lunit, wl.denstonh), wl.fields(), segs)
     rel = np.abs(tf - ts) / np.maximum(np.abs(ts), 1e-30)
     assert np.max(rel) < 1e-3
+
+
+def test_phi_polynomial_matches_fit_and_bound():
+    """The coefficients of the FP32 rate kernel's photon-conserving factor
+    (photoion.cuh kPhiC) are the ones argot_b200/fits.py makes, and their
+    FP32 Horner evaluation stays within 1e-7 of (1 - e^-x)/x on [0, 1]."""
+    import os
+    import re
+    from argot_b200 import fits
+    from conftest import ROOT
+    src = open(os.path.join(ROOT, "argot_b200", "csrc", "photoion.cuh")).read()
+    body = re.search(r"kPhiC\[7\]\s*=\s*\{([^}]*)\}", src).group(1)
+    c = np.array([float(v.strip().rstrip("f")) for v in body.split(",")], np.float32)
+    assert np.array_equal(c, fits.fit_phi())
+    assert float(re.search(r"kPhiXMax\s*=\s*([0-9.]+)f", src).group(1)) == fits.PHI_X_MAX
+    assert fits.phi_error(c) < 1e-7
