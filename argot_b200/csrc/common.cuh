@@ -9,7 +9,7 @@
 namespace argot {
 
 // Physical constants and flags exactly as the reference spells them
-// (constants.h, prim_chem/chemistry.h:25,286-314, calc_optical_depth.c:15).
+// (constants.h, prim_chem/chemistry.h:14,25, calc_optical_depth.c:15).
 constexpr double kTiny = 1.0e-31;
 constexpr double kHeliumFact = 0.0811258278;
 constexpr double kPi = 3.1415926535897932384626433;

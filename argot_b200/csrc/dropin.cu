@@ -1,5 +1,5 @@
-// dropin.cu -- the reference's own entry points (src/prototype.h:75,89,121,
-// 152-153) on one GPU, for argot_mpi / argot_hydro_mpi to link in place of
+// dropin.cu -- the reference's own entry points (src/prototype.h:47,89,93,
+// 124-125) on one GPU, for argot_mpi / argot_hydro_mpi to link in place of
 // calc_optical_depth_cuda.o, calc_photoion_rate_cuda.o,
 // accum_optical_depth.o and smooth_photoion_rate.o on a single rank.
 #include <algorithm>
@@ -20,7 +20,7 @@ int launch_pack_mesh(uint64_t n, const void *mesh, float4 *cells, float4 *raw, c
 int launch_rate_rayio(const GridDev &g, const float4 *raw, const void *rays_io, uint64_t nray, int rx, int ry,
                       int rz, double *per6, cudaStream_t st);
 int launch_accum_runs(const GridDev &g, const void *rays_io, uint64_t nray, int rx, int ry, int rz,
-                      const double *per6, void *mesh, cudaStream_t st);
+                      const double *per6, void *mesh, int *err, cudaStream_t st);
 int launch_zero_rates(uint64_t n, void *mesh, cudaStream_t st);
 int launch_smooth_mesh(int nx, int ny, int nz, void *mesh, float *work, int isolated, cudaStream_t st);
 int *err_flag(int dev);
@@ -204,6 +204,8 @@ int do_rates(cuda_mem_space *cm, light_ray *ray, light_ray_IO *ray_io, cuda_para
   if ((rc = ensure_tables(0))) return rc;
   fill_ray_io(ray, ray_io, nray);
   ARGOT_CUDA_TRY(s.cells.ensure(32 * ncell));
+  int *err = err_flag(0);
+  if (!err) return ARGOT_B200_ENOMEM;
   cudaStream_t caller = caller_stream(cp);
   float4 *cells = (float4 *)s.cells.ptr;
   if ((rc = launch_pack_mesh(ncell, cm[0].mesh_dev, cells, cells + ncell, caller))) return rc;
@@ -227,13 +229,14 @@ int do_rates(cuda_mem_space *cm, light_ray *ray, light_ray_IO *ray_io, cuda_para
       return rc;
     ARGOT_CUDA_TRY(cudaEventRecord(s.rate_done[bi], st));
     ARGOT_CUDA_TRY(cudaStreamWaitEvent(caller, s.rate_done[bi], 0));
-    if ((rc = launch_accum_runs(g, dbuf, n, run->rank_x, run->rank_y, run->rank_z, per, cm[0].mesh_dev, caller)))
+    if ((rc = launch_accum_runs(g, dbuf, n, run->rank_x, run->rank_y, run->rank_z, per, cm[0].mesh_dev, err,
+                                caller)))
       return rc;
     ARGOT_CUDA_TRY(cudaEventRecord(s.accum_done[bi], caller));
   }
   if ((rc = join_lanes(s, caller))) return rc;
   ARGOT_CUDA_TRY(cudaStreamSynchronize(caller));
-  return 0;
+  return check_err_flag(err, caller);
 }
 
 // smooth_photoion_rate with __USE_GPU__ on one rank

@@ -304,12 +304,16 @@ __global__ void k_zero3(uint64_t n, float *__restrict__ out) {
 }
 
 __global__ void k_stitch(uint64_t nseg, const uint64_t *__restrict__ ray_indx,
-                         const float *__restrict__ seg_tau3, uint64_t nray, float *__restrict__ ray_tau3) {
+                         const float *__restrict__ seg_tau3, uint64_t nray, float *__restrict__ ray_tau3,
+                         int *__restrict__ err) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nseg;
        i += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t r = ray_indx[i];
     if (i > 0 && ray_indx[i - 1] == r) continue;  // not the head of a run
-    if (r >= nray) continue;
+    if (r >= nray) {  // a segment of a ray the caller's array does not have: skipped, reported
+      atomicExch(err, 1);
+      continue;
+    }
     float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
     for (uint64_t j = i; j < nseg && ray_indx[j] == r; j++) {
       kahan_add(s0, c0, seg_tau3[3 * j + 0]);
@@ -320,6 +324,13 @@ __global__ void k_stitch(uint64_t nseg, const uint64_t *__restrict__ ray_indx,
     ray_tau3[3 * r + 1] = s1;
     ray_tau3[3 * r + 2] = s2;
   }
+}
+
+// adds base to the n offsets (the scan's shift), on the device
+__global__ void k_add_base(uint64_t n, uint64_t base, uint64_t *__restrict__ off) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    off[i] += base;
 }
 
 // per-device scratch: an error flag and a counter
@@ -425,18 +436,8 @@ int argot_b200_scan_blocks(const uint64_t *blk_count, uint64_t nb, uint64_t base
     cudaError_t e = cub::DeviceScan::InclusiveSum(tmp, tmp_bytes, blk_count, blk_off + 1, (int64_t)nb, st);
     cudaFreeAsync(tmp, st);
     ARGOT_CUDA_TRY(e);
-    if (base) {
-      // shift by base (rare: group offsets are usually rebased by the caller)
-      uint64_t *h = (uint64_t *)malloc(sizeof(uint64_t) * (nb + 1));
-      if (!h) { set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
-      ARGOT_CUDA_TRY(cudaMemcpyAsync(h, blk_off, sizeof(uint64_t) * (nb + 1), cudaMemcpyDeviceToHost, st));
-      ARGOT_CUDA_TRY(cudaStreamSynchronize(st));
-      for (uint64_t i = 1; i <= nb; i++) h[i] += base;
-      cudaError_t e2 = cudaMemcpyAsync(blk_off, h, sizeof(uint64_t) * (nb + 1), cudaMemcpyHostToDevice, st);
-      if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(st);
-      free(h);
-      ARGOT_CUDA_TRY(e2);
-    }
+    if (base) k_add_base<<<grid_blocks_for(nb, 256), 256, 0, st>>>(nb, base, blk_off + 1);
+    ARGOT_CUDA_TRY(cudaGetLastError());
   }
   if (total) {
     ARGOT_CUDA_TRY(cudaMemcpyAsync(total, blk_off + nb, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
@@ -547,9 +548,13 @@ int argot_b200_stitch(uint64_t nseg, const uint64_t *ray_indx, const float *seg_
     set_status(ARGOT_B200_EINVAL);
     return ARGOT_B200_EINVAL;
   }
+  int dev = 0;
+  ARGOT_CUDA_TRY(cudaGetDevice(&dev));
+  int *err = err_flag(dev);
+  if (!err) { set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
   cudaStream_t st = (cudaStream_t)stream;
   if (nray) k_zero3<<<grid_blocks_for(3 * nray, 256), 256, 0, st>>>(nray, ray_tau3);
-  if (nseg) k_stitch<<<grid_blocks_for(nseg, 256), 256, 0, st>>>(nseg, ray_indx, seg_tau3, nray, ray_tau3);
+  if (nseg) k_stitch<<<grid_blocks_for(nseg, 256), 256, 0, st>>>(nseg, ray_indx, seg_tau3, nray, ray_tau3, err);
   ARGOT_CUDA_TRY(cudaGetLastError());
   set_status(0);
   return 0;

@@ -165,7 +165,13 @@ __global__ void k_rate_rayio(GridDev g, const float4 *__restrict__ raw, const li
 // of consecutive rays with the same target (the reference emits the rays of
 // a cell consecutively); each field is updated with a compare-and-swap so
 // that a cell appearing in several runs still receives every contribution.
-__device__ __forceinline__ void add_run(float *field, const double *per6, int s, uint64_t i0, uint64_t i1) {
+// A CAS fails only when another run of the same cell has just landed, so the
+// loop ends after at most that many retries; past 2^20 of them (more than a
+// million runs of one cell in flight) the run's sum is added with one float
+// atomicAdd instead, its per-ray float rounding is lost, and the device
+// error flag reports it.
+__device__ __forceinline__ void add_run(float *field, const double *per6, int s, uint64_t i0, uint64_t i1,
+                                        int *err) {
   unsigned int *addr = (unsigned int *)field;
   unsigned int old = *((volatile unsigned int *)addr);
   for (int attempt = 0; attempt < 1 << 20; attempt++) {
@@ -175,10 +181,15 @@ __device__ __forceinline__ void add_run(float *field, const double *per6, int s,
     if (prev == old) return;
     old = prev;
   }
+  double sum = 0.0;
+  for (uint64_t i = i0; i < i1; i++) sum += per6[6 * i + s];
+  atomicAdd(field, (float)sum);
+  atomicExch(err, 1);
 }
 
 __global__ void k_accum_runs(GridDev g, const light_ray_IO *__restrict__ rays, uint64_t nray, int rank_x,
-                             int rank_y, int rank_z, const double *__restrict__ per6, fluid_mesh *__restrict__ mesh) {
+                             int rank_y, int rank_z, const double *__restrict__ per6, fluid_mesh *__restrict__ mesh,
+                             int *__restrict__ err) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nray;
        i += (uint64_t)gridDim.x * blockDim.x) {
     const int tx = rays[i].ix_target, ty = rays[i].iy_target, tz = rays[i].iz_target;
@@ -189,12 +200,12 @@ __global__ void k_accum_runs(GridDev g, const light_ray_IO *__restrict__ rays, u
     const int lx = tx - rank_x * g.nx, ly = ty - rank_y * g.ny, lz = tz - rank_z * g.nz;
     if ((unsigned)lx >= (unsigned)g.nx || (unsigned)ly >= (unsigned)g.ny || (unsigned)lz >= (unsigned)g.nz) continue;
     prim_chem &pc = mesh[cell_index(g, lx, ly, lz)].prev_chem;
-    add_run(&pc.GammaHI, per6, 0, i, j);
-    add_run(&pc.GammaHeI, per6, 1, i, j);
-    add_run(&pc.GammaHeII, per6, 2, i, j);
-    add_run(&pc.HeatHI, per6, 3, i, j);
-    add_run(&pc.HeatHeI, per6, 4, i, j);
-    add_run(&pc.HeatHeII, per6, 5, i, j);
+    add_run(&pc.GammaHI, per6, 0, i, j, err);
+    add_run(&pc.GammaHeI, per6, 1, i, j, err);
+    add_run(&pc.GammaHeII, per6, 2, i, j, err);
+    add_run(&pc.HeatHI, per6, 3, i, j, err);
+    add_run(&pc.HeatHeI, per6, 4, i, j, err);
+    add_run(&pc.HeatHeII, per6, 5, i, j, err);
   }
 }
 
@@ -218,10 +229,10 @@ int launch_rate_rayio(const GridDev &g, const float4 *raw, const void *rays_io, 
 }
 
 int launch_accum_runs(const GridDev &g, const void *rays_io, uint64_t nray, int rx, int ry, int rz,
-                      const double *per6, void *mesh, cudaStream_t st) {
+                      const double *per6, void *mesh, int *err, cudaStream_t st) {
   if (!nray) return 0;
   k_accum_runs<<<grid_blocks_for_rates(nray, 128), 128, 0, st>>>(g, (const light_ray_IO *)rays_io, nray, rx, ry,
-                                                                  rz, per6, (fluid_mesh *)mesh);
+                                                                  rz, per6, (fluid_mesh *)mesh, err);
   ARGOT_CUDA_TRY(cudaGetLastError());
   return 0;
 }

@@ -17,7 +17,7 @@ constexpr int kNGridNu = 256;
 constexpr int kNSegPerRay = 5;
 constexpr int kNMaxCudaDev = 4;
 
-// src/prim_chem/chemistry.h:317-339
+// src/prim_chem/chemistry.h:41-63
 struct prim_chem {
   float wmol, felec;
   float fHI, fHII;
@@ -27,7 +27,7 @@ struct prim_chem {
   float HeatHeI, HeatHeII;
 };
 
-// src/fluid.h:190-205
+// src/fluid.h:101-116
 struct fluid_mesh {
   float dens, eneg, momx, momy, momz;
   float uene, duene, durad, etrp, pot, dens_prev;
@@ -37,7 +37,7 @@ struct fluid_mesh {
   short under_shock, high_mach;
 };
 
-// src/source.h:229-239
+// src/source.h:6-16
 struct freq_param {
   double log_nu_min, log_nu_max, dlog_nu;
   double nu[kNGridNu];

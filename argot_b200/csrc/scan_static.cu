@@ -17,7 +17,11 @@
 //     caller;
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture.
+//     before any stream capture;
+//   * the total on the host (total != NULL) needs a copy and a stream
+//     synchronisation, which a stream capture cannot hold: while `stream`
+//     is capturing, total must be NULL (ARGOT_B200_EINVAL otherwise, nothing
+//     launched); the caller reads blk_offsets[nb] instead.
 #include <mutex>
 
 #include "common.cuh"
@@ -139,12 +143,20 @@ extern "C" int argot_b200_scan_blocks_static(const uint64_t *blk_count, uint64_t
     set_status(ARGOT_B200_EINVAL);
     return ARGOT_B200_EINVAL;
   }
+  cudaStream_t st = (cudaStream_t)stream;
+  if (total) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    ARGOT_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) {  // a synchronisation cannot be captured
+      set_status(ARGOT_B200_EINVAL);
+      return ARGOT_B200_EINVAL;
+    }
+  }
   int dev = 0;
   ARGOT_CUDA_TRY(cudaGetDevice(&dev));
   void *scratch = nullptr;
   int rc = scratch_address(dev, &scratch);
   if (rc) { set_status(rc); return rc; }
-  cudaStream_t st = (cudaStream_t)stream;
   unsigned long long *part = (unsigned long long *)scratch;
   const unsigned long long *cnt = (const unsigned long long *)blk_count;
   unsigned long long *out = (unsigned long long *)blk_off;

@@ -19,7 +19,7 @@ import numpy as np
 
 MPC = 3.086e24
 MPROTON = 1.672623e-24
-XHYDROGEN = 0.755  # helium build (prim_chem/chemistry.h:299)
+XHYDROGEN = 0.755  # helium build (prim_chem/chemistry.h:23)
 
 
 def units(nH: float = 1.0e-3, lunit_mpc: float = 6.6e-3):

@@ -79,25 +79,25 @@ struct omp_param;
 struct mpi_param;
 
 /* Replaces src/calc_optical_depth_cuda.cu:29-144 (declared at
- * src/prototype.h:152).  Overwrites seg[0..run->nseg).optical_depth_* in
+ * src/prototype.h:124).  Overwrites seg[0..run->nseg).optical_depth_* in
  * host memory before returning.  Reads the mesh from
  * cuda_mem[0].mesh_dev (device AoS struct fluid_mesh, filled by the caller's
  * send_mesh_data) and the domain geometry from *this_run (host copy). */
 ARGOT_B200_API void calc_optical_depth_cuda(struct ray_segment *seg, struct cuda_mem_space *cuda_mem,
                              struct cuda_param *this_cuda, struct run_param *this_run);
 
-/* Replaces src/calc_photoion_rate_cuda.cu:92-216 (src/prototype.h:153).
+/* Replaces src/calc_photoion_rate_cuda.cu:92-216 (src/prototype.h:125).
  * Fills ray_IO from ray as the reference does, and ADDS each ray's rates to
  * cuda_mem[0].mesh_dev[target].prev_chem.{Gamma,Heat}{HI,HeI,HeII}. */
 ARGOT_B200_API void calc_photoion_rate_cuda(struct cuda_mem_space *cuda_mem, struct light_ray *ray,
                              struct light_ray_IO *ray_IO, struct cuda_param *this_cuda,
                              struct run_param *this_run);
 
-/* Replaces src/calc_photoion_rate_cuda.cu:45-62 (src/prototype.h:121). */
+/* Replaces src/calc_photoion_rate_cuda.cu:45-62 (src/prototype.h:93). */
 ARGOT_B200_API void zero_out_photoion_rate_cuda(struct cuda_mem_space *cuda_mem,
                                  struct cuda_param *this_cuda, struct run_param *this_run);
 
-/* Replaces src/accum_optical_depth.c:14-167 (src/prototype.h:75) for a
+/* Replaces src/accum_optical_depth.c:14-167 (src/prototype.h:47) for a
  * single-rank run: every segment's columns go to ray[seg.ray_indx], rays
  * without a segment get zero.  A host routine (the columns are already in
  * host memory after calc_optical_depth_cuda).  An executable that still
@@ -225,7 +225,9 @@ ARGOT_B200_API int argot_b200_scan_blocks(const uint64_t *blk_count_dev, uint64_
  * 16 777 216 blocks (larger requests return ARGOT_B200_EINVAL and launch
  * nothing).  All calls on a device share that array, so calls that overlap
  * on the GPU race; serialise them.  The first call on a device looks up the
- * array's address: make it before any stream capture. */
+ * array's address: make it before any stream capture.  Under a stream
+ * capture total must be NULL (reading it back needs a synchronisation;
+ * ARGOT_B200_EINVAL otherwise): read blk_offsets[nb] from the device. */
 ARGOT_B200_API int argot_b200_scan_blocks_static(const uint64_t *blk_count_dev, uint64_t nb,
                                                  uint64_t base, uint64_t *blk_offsets_dev,
                                                  uint64_t *total, void *stream);
@@ -265,7 +267,9 @@ ARGOT_B200_API int argot_b200_march_segments(const argot_b200_grid *g, const voi
 /* Stitch: ray_tau[r] = sum of seg_tau over the segments with ray_indx == r
  * (segments sorted by ray index; Kahan-compensated segmented sums).  On one
  * rank, where each ray has one segment per domain, this is the reference's
- * accum_optical_depth. ray_tau3 is AoS (3 floats per ray) and overwritten. */
+ * accum_optical_depth. ray_tau3 is AoS (3 floats per ray) and overwritten.
+ * A segment whose ray index is >= nray is skipped and sets the device error
+ * flag (argot_b200_check_device_error). */
 ARGOT_B200_API int argot_b200_stitch(uint64_t nseg, const uint64_t *ray_indx_dev,
                       const float *seg_tau3_dev, uint64_t nray, float *ray_tau3_dev,
                       void *stream);
@@ -471,7 +475,7 @@ ARGOT_B200_API int argot_b200_art_rates(const argot_b200_art *a, const argot_b20
                                         int angles_per_pass, unsigned long long *crossings_dev, void *stream);
 
 /* Replaces src/diffuse_photon/calc_diffuse_photon_radiation.c:37-128 as built
- * with __USE_GPU__ (src/diffuse_photon/diffuse_prototype.h:27) on a single
+ * with __USE_GPU__ (src/diffuse_photon/diffuse_prototype.h:30) on a single
  * rank: the caller's angle table and step factors (hd_param, filled by its
  * setup_diffuse_photon), the mesh of cuda_mem[0].mesh_dev, whose
  * prev_chem.{Gamma,Heat}{HI,HeI,HeII} receive the diffuse rates (added).

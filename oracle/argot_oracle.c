@@ -25,7 +25,7 @@
  *
  * Conventions (all as in the reference): mesh index
  * MESH(ix,iy,iz) = f[iz + nz*(iy + ny*ix)] (calc_optical_depth.c:18); He
- * number density = HELIUM_FACT * n_H (prim_chem/chemistry.h:301); columns in
+ * number density = HELIUM_FACT * n_H (prim_chem/chemistry.h:25); columns in
  * code units (length x code density); TINY = 1e-31.
  */
 #include <math.h>

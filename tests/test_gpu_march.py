@@ -219,3 +219,26 @@ def test_stitch_segmented_sum(cuda_ok, oracle):
     L.check(lib.argot_b200_stitch(nray, one_d.data_ptr(), t1_d.data_ptr(), nray, out.data_ptr(), s),
             "stitch")
     assert np.array_equal(out.cpu().numpy(), oracle.accum(nray, one, t1))
+
+
+def test_stitch_flags_ray_index_past_the_rays(cuda_ok):
+    """A segment whose ray index is past the caller's ray count is skipped
+    and reported through the device error flag; the other rays are summed."""
+    import torch
+    from argot_b200 import _lib as L
+    lib = L.load()
+    nray = 100
+    ray_indx = np.concatenate([np.arange(nray, dtype=np.uint64), np.array([nray, nray + 7], np.uint64)])
+    seg_tau = np.ones((len(ray_indx), 3), np.float32)
+    ri = torch.from_numpy(ray_indx.view(np.int64)).cuda()
+    st = torch.from_numpy(seg_tau).cuda()
+    out = torch.zeros((nray + 8, 3), dtype=torch.float32, device="cuda")  # room past nray: nothing may land there
+    s = torch.cuda.current_stream().cuda_stream
+    L.check(lib.argot_b200_stitch(len(ray_indx), ri.data_ptr(), st.data_ptr(), nray, out.data_ptr(), s), "stitch")
+    torch.cuda.synchronize()
+    with pytest.raises(L.ArgotError):
+        L.check(lib.argot_b200_check_device_error(s), "device error flag")
+    L.check(lib.argot_b200_check_device_error(s), "device error flag")  # cleared
+    got = out.cpu().numpy()
+    assert np.array_equal(got[:nray], np.ones((nray, 3), np.float32))
+    assert not got[nray:].any()

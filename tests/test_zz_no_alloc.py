@@ -39,14 +39,67 @@ def test_static_scan_equals_allocating_scan(cuda_ok):
             assert tot1 == tot0 == base + int(counts.sum().item())
 
 
-def test_static_scan_rejects_oversize(cuda_ok):
+def test_static_scan_largest_size(cuda_ok):
+    """nb at the limit: the whole scratch array (8192 tiles) in use."""
     import torch
     from argot_b200 import _lib as L
     lib = L.load()
-    small = torch.zeros(4, dtype=torch.int64, device="cuda")
+    counts = torch.randint(0, 300, (MAX_BLOCKS,), dtype=torch.int64, device="cuda")
+    rc0, want, tot0 = _scan(lib, "argot_b200_scan_blocks", counts, 11)
+    rc1, got, tot1 = _scan(lib, "argot_b200_scan_blocks_static", counts, 11)
+    assert rc0 == 0 and rc1 == 0
+    assert np.array_equal(got, want)
+    assert tot1 == tot0 == 11 + int(counts.sum().item())
+
+
+def test_static_scan_rejects_oversize(cuda_ok):
+    """One block past the limit: rejected before any launch.  The buffers
+    are sized for the request, so even a launch would stay in bounds."""
+    import torch
+    from argot_b200 import _lib as L
+    lib = L.load()
+    nb = MAX_BLOCKS + 1
+    counts = torch.ones(nb, dtype=torch.int64, device="cuda")
+    off = torch.zeros(nb + 1, dtype=torch.int64, device="cuda")
     tot = C.c_uint64(99)
-    rc = lib.argot_b200_scan_blocks_static(small.data_ptr(), MAX_BLOCKS + 1, 0, small.data_ptr(),
+    rc = lib.argot_b200_scan_blocks_static(counts.data_ptr(), nb, 0, off.data_ptr(),
                                            C.byref(tot), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
     assert rc == L.EINVAL
     assert tot.value == 99  # nothing ran
-    assert int(small.abs().sum().item()) == 0
+    assert int(off.abs().sum().item()) == 0
+
+
+def test_static_scan_in_a_cuda_graph(cuda_ok):
+    """The use it exists for: captured into a CUDA graph (total = NULL, the
+    offsets read back from the device) and replayed; a host total under
+    capture is refused."""
+    import torch
+    from argot_b200 import _lib as L
+    lib = L.load()
+    rng = np.random.default_rng(5)
+    nb = 123_457
+    counts = torch.from_numpy(rng.integers(0, 1000, nb).astype(np.int64)).cuda()
+    _, want, _ = _scan(lib, "argot_b200_scan_blocks", counts, 42)
+    off = torch.full((nb + 1,), -1, dtype=torch.int64, device="cuda")
+    side = torch.cuda.Stream()
+    # the first call on the device (address look-up) comes before the capture
+    assert lib.argot_b200_scan_blocks_static(counts.data_ptr(), nb, 42, off.data_ptr(), None,
+                                             side.cuda_stream) == 0
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    refused = None
+    with torch.cuda.graph(g, stream=side):
+        rc = lib.argot_b200_scan_blocks_static(counts.data_ptr(), nb, 42, off.data_ptr(), None,
+                                               side.cuda_stream)
+        tot = C.c_uint64(0)
+        refused = lib.argot_b200_scan_blocks_static(counts.data_ptr(), nb, 42, off.data_ptr(), C.byref(tot),
+                                                    side.cuda_stream)
+    assert rc == 0
+    assert refused == L.EINVAL
+    for _ in range(2):
+        off.fill_(-1)
+        g.replay()
+        torch.cuda.synchronize()
+        assert np.array_equal(off.cpu().numpy(), want)
+    del g
