@@ -42,12 +42,12 @@ ART_UENETOK = 1.0e4
 METRIC = "ray-cell crossings/s (march+stitch+rates, 1 B200)"
 # DRAM bytes per ray-cell crossing of k_march_rays<Kahan> measured by ncu on
 # the 256^3 / 16-source case (dram__bytes_read.sum + dram__bytes_write.sum =
-# 148.7 + 21.3 GB over a 118.4 ms launch for 6.030e10 crossings); the
+# 142.3 + 19.9 GB over a 125.4 ms launch for 6.030e10 crossings); the
 # workloads here are too large to capture, so `traffic` scales this figure.
-MARCH_DRAM_BYTES_PER_CROSSING = 2.818
-# the same capture's L2 bytes (lts__t_bytes.sum, 701.4 GB over the launch's
-# 6.030e10 crossings): what the L2 serves per crossing
-MARCH_L2_BYTES_PER_CROSSING = 11.630
+MARCH_DRAM_BYTES_PER_CROSSING = 2.689
+# the same capture's L2 bytes (lts__t_sectors.sum x 32 B, 575.8 GB over the
+# launch's 6.030e10 crossings): what the L2 serves per crossing
+MARCH_L2_BYTES_PER_CROSSING = 9.548
 UNIT = "crossings/s"
 
 
