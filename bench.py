@@ -589,8 +589,14 @@ def run_ours(args):
                      "peak_kind": f"{peak_kind} hbm_gbs",
                      "traffic": MARCH_DRAM_BYTES_PER_CROSSING * n_cross,
                      "l2_traffic": MARCH_L2_BYTES_PER_CROSSING * n_cross,
-                     "traffic_source": "ncu DRAM bytes per crossing on 256^3 / 16 sources "
-                                       "(2.818 B; L2 11.630 B), scaled by this launch's crossings",
+                     "traffic_source": (f"ncu DRAM bytes per crossing on 256^3 / 16 sources "
+                                        f"({MARCH_DRAM_BYTES_PER_CROSSING} B; L2 {MARCH_L2_BYTES_PER_CROSSING} B), "
+                                        f"scaled by this launch's crossings"),
+                     "dram_gbs": MARCH_DRAM_BYTES_PER_CROSSING * n_cross / t_march / 1e9,
+                     "dram_frac": MARCH_DRAM_BYTES_PER_CROSSING * n_cross / t_march / 1e9 / hbm,
+                     "limiter": ("latency of the L1/L2-hit gathers (ncu: long-scoreboard stalls 11 per issue, "
+                                 "issue active 71%); DRAM moves 2.7 B and L2 serves 9.5 B of the 16 B per "
+                                 "crossing that the bytes model counts"),
                      "algorithmic_bytes": alg_bytes,
                      "bytes_model": "16 B per crossing + 36 B per ray"},
         "clocks": clk,
