@@ -1,8 +1,8 @@
 // scan_static.cu -- the ray-offset scan of argot_b200_scan_blocks in a form
 // that allocates no memory, for callers that cannot allocate device memory
-// while they run the path: code executing inside a stream capture whose
-// allocator must stay untouched, hosts that hand all device memory to their
-// own pool, or a drop-in used from code that forbids cudaMalloc after start-up.
+// while they run the path: hosts that hand all device memory to their own
+// pool allocator up front, or a drop-in used from code that forbids
+// cudaMalloc after start-up.
 //
 // The scan's scratch (one partial sum per tile of 2048 counts) lives in a
 // file-scope device array of fixed size instead of a temporary allocation.
@@ -19,9 +19,10 @@
 //     (cudaGetSymbolAddress) with that device current; make that first call
 //     before any stream capture;
 //   * the total on the host (total != NULL) needs a copy and a stream
-//     synchronisation, which a stream capture cannot hold: while `stream`
-//     is capturing, total must be NULL (ARGOT_B200_EINVAL otherwise, nothing
-//     launched); the caller reads blk_offsets[nb] instead.
+//     synchronisation; with total == NULL the call only enqueues work and
+//     the caller reads blk_offsets[nb] on the device.  A host total is
+//     refused (ARGOT_B200_EINVAL, nothing launched) while `stream` is
+//     capturing, where a synchronisation is not allowed.
 #include <mutex>
 
 #include "common.cuh"

@@ -217,17 +217,18 @@ ARGOT_B200_API int argot_b200_count_rays(const argot_b200_grid *g, const argot_b
 ARGOT_B200_API int argot_b200_scan_blocks(const uint64_t *blk_count_dev, uint64_t nb, uint64_t base,
                            uint64_t *blk_offsets_dev, uint64_t *total, void *stream);
 /* The same scan, allocating no memory: for callers that cannot allocate
- * device memory while the path runs (code inside a stream capture that must
- * not touch the allocator, hosts that give all device memory to their own
- * pool, drop-in callers that forbid cudaMalloc after start-up).  No
+ * device memory while the path runs (hosts that give all device memory to
+ * their own pool allocator up front, drop-in callers whose host code forbids
+ * cudaMalloc after start-up, loops that must not wait on the driver's
+ * allocator).  No
  * counterpart in the reference.  Its scratch is a fixed 64 KiB device array
  * that every GPU loading the library holds until exit: nb is limited to
  * 16 777 216 blocks (larger requests return ARGOT_B200_EINVAL and launch
  * nothing).  All calls on a device share that array, so calls that overlap
  * on the GPU race; serialise them.  The first call on a device looks up the
- * array's address: make it before any stream capture.  Under a stream
- * capture total must be NULL (reading it back needs a synchronisation;
- * ARGOT_B200_EINVAL otherwise): read blk_offsets[nb] from the device. */
+ * array's address: make it before any stream capture.  With total != NULL
+ * the call copies the total back and synchronises `stream`; with NULL it
+ * only enqueues work, and blk_offsets[nb] holds the total on the device. */
 ARGOT_B200_API int argot_b200_scan_blocks_static(const uint64_t *blk_count_dev, uint64_t nb,
                                                  uint64_t base, uint64_t *blk_offsets_dev,
                                                  uint64_t *total, void *stream);

@@ -59,7 +59,10 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_OUT = os.path.join(HERE, "_ref")
 ORC_OUT = os.path.join(HERE, "_build")
-DEFAULT_REF = os.environ.get("ARGOT_REFERENCE", "/root/reference")
+# ARGOT's source tree: $ARGOT_REFERENCE, else a checkout named ``reference``
+# beside this repository
+DEFAULT_REF = os.environ.get("ARGOT_REFERENCE",
+                             os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 
 SOURCES = [
     "calc_optical_depth.c",

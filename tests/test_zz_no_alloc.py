@@ -68,38 +68,3 @@ def test_static_scan_rejects_oversize(cuda_ok):
     assert rc == L.EINVAL
     assert tot.value == 99  # nothing ran
     assert int(off.abs().sum().item()) == 0
-
-
-def test_static_scan_in_a_cuda_graph(cuda_ok):
-    """The use it exists for: captured into a CUDA graph (total = NULL, the
-    offsets read back from the device) and replayed; a host total under
-    capture is refused."""
-    import torch
-    from argot_b200 import _lib as L
-    lib = L.load()
-    rng = np.random.default_rng(5)
-    nb = 123_457
-    counts = torch.from_numpy(rng.integers(0, 1000, nb).astype(np.int64)).cuda()
-    _, want, _ = _scan(lib, "argot_b200_scan_blocks", counts, 42)
-    off = torch.full((nb + 1,), -1, dtype=torch.int64, device="cuda")
-    side = torch.cuda.Stream()
-    # the first call on the device (address look-up) comes before the capture
-    assert lib.argot_b200_scan_blocks_static(counts.data_ptr(), nb, 42, off.data_ptr(), None,
-                                             side.cuda_stream) == 0
-    torch.cuda.synchronize()
-    g = torch.cuda.CUDAGraph()
-    refused = None
-    with torch.cuda.graph(g, stream=side):
-        rc = lib.argot_b200_scan_blocks_static(counts.data_ptr(), nb, 42, off.data_ptr(), None,
-                                               side.cuda_stream)
-        tot = C.c_uint64(0)
-        refused = lib.argot_b200_scan_blocks_static(counts.data_ptr(), nb, 42, off.data_ptr(), C.byref(tot),
-                                                    side.cuda_stream)
-    assert rc == 0
-    assert refused == L.EINVAL
-    for _ in range(2):
-        off.fill_(-1)
-        g.replay()
-        torch.cuda.synchronize()
-        assert np.array_equal(off.cpu().numpy(), want)
-    del g
