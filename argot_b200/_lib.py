@@ -59,6 +59,7 @@ SIGNATURES = {
     "argot_b200_last_error": (i32, []),
     "argot_b200_error_string": (C.c_char_p, [i32]),
     "argot_b200_version": (C.c_char_p, []),
+    "argot_b200_flagset": (C.c_char_p, []),
     "argot_b200_struct_sizes": (None, [vp]),
     "argot_b200_abi_check": (i32, [vp, i32]),
     "calc_optical_depth_cuda": (None, [vp, vp, vp, vp]),

@@ -143,3 +143,104 @@ def offsets():
             RunParam.xmin_local.offset, RunParam.nmesh_x_total.offset,
             RunParam.nmesh_x_local.offset, RunParam.delta_x.offset, RunParam.theta_crit.offset,
             RunParam.nmesh_per_loop.offset, RunParam.rank_x.offset, RunParam.anow.offset]
+
+
+# ---------------------------------------------------------------- flag sets
+def column_names(helium: bool, hydrogen_mol: bool):
+    """The optical_depth_* columns of a segment / ray in the reference's
+    order (src/radiation.h:23-83)."""
+    return (["HI"] + (["HeI", "HeII"] if helium else [])
+            + (["HM", "H2I", "H2II"] if hydrogen_mol else []))
+
+
+def rate_names(helium: bool, hydrogen_mol: bool):
+    """The Gamma / Heat fields of struct prim_chem from GammaHI on
+    (src/prim_chem/chemistry.h:41-63)."""
+    return (["GammaHI", "HeatHI"]
+            + (["GammaHeI", "GammaHeII", "HeatHeI", "HeatHeII"] if helium else [])
+            + (["GammaHM", "GammaH2I_I", "GammaH2I_II", "GammaH2II_I", "GammaH2II_II",
+                "HeatHM", "HeatH2I_I", "HeatH2I_II", "HeatH2II_I", "HeatH2II_II"] if hydrogen_mol else []))
+
+
+def channel_names(helium: bool, hydrogen_mol: bool):
+    """The csect_* fields of struct cross_section (src/cross_section.h:7-20)."""
+    return (["HI"] + (["HeI", "HeII"] if helium else [])
+            + (["HM", "H2I_I", "H2II_I", "H2II_II"] if hydrogen_mol else []))
+
+
+def make_layout(helium: bool = True, hydrogen_mol: bool = False):
+    """ctypes mirrors of the structs for another flag set of the reference:
+    the fields that -D__HELIUM__ and -D__HYDROGEN_MOL__ add sit where the
+    reference headers put them.  Returns a namespace with PrimChem,
+    FluidMesh, RaySegment, LightRay, LightRayIO, CrossSection, PhotoionRate,
+    RunParam, STRUCTS (the order of argot_b200_struct_sizes) and the column /
+    rate / channel names."""
+    import types
+    cols = column_names(helium, hydrogen_mol)
+    rates = rate_names(helium, hydrogen_mol)
+    chans = channel_names(helium, hydrogen_mol)
+    f = C.c_float
+
+    class PrimChemV(C.Structure):
+        _fields_ = ([(n, f) for n in ("wmol", "felec", "fHI", "fHII")]
+                    + ([(n, f) for n in ("fH2I", "fH2II", "fHM")] if hydrogen_mol else [])
+                    + ([(n, f) for n in ("fHeI", "fHeII", "fHeIII")] if helium else [])
+                    + [(n, f) for n in rates])
+
+    class FluidMeshV(C.Structure):
+        _fields_ = [(n, f) for n in
+                    ("dens", "eneg", "momx", "momy", "momz", "uene", "duene", "durad", "etrp", "pot",
+                     "dens_prev")] + [("chem", PrimChemV), ("prev_chem", PrimChemV),
+                                      ("prev_uene", f), ("under_shock", C.c_short),
+                                      ("high_mach", C.c_short)]
+
+    class RaySegmentV(C.Structure):
+        _fields_ = ([("ray_indx", C.c_uint64), ("local_rank", C.c_int), ("target_rank", C.c_int)]
+                    + [(n, f) for n in ("xpos_start", "ypos_start", "zpos_start",
+                                        "xpos_end", "ypos_end", "zpos_end")]
+                    + [("optical_depth_" + c, f) for c in cols])
+
+    class LightRayV(C.Structure):
+        _fields_ = ([("src", RadiationSrc), ("num_segment", C.c_int),
+                     ("segment", RaySegmentV * NSEG_PER_RAY),
+                     ("ix_target", C.c_int), ("iy_target", C.c_int), ("iz_target", C.c_int)]
+                    + [("optical_depth_" + c, f) for c in cols])
+
+    class LightRayIOV(C.Structure):
+        _fields_ = ([("src", RadiationSrc),
+                     ("ix_target", C.c_int), ("iy_target", C.c_int), ("iz_target", C.c_int)]
+                    + [("optical_depth_" + c, f) for c in cols])
+
+    class CrossSectionV(C.Structure):
+        _fields_ = [("csect_" + c, f) for c in chans]
+
+    class PhotoionRateV(C.Structure):
+        _fields_ = [(n, f) for n in rates]
+
+    run_fields = []
+    for name, typ in RunParam._fields_:
+        run_fields.append((name, CrossSectionV * NGRID_NU if name == "csect" else typ))
+
+    class RunParamV(C.Structure):
+        _fields_ = run_fields
+
+    ns = types.SimpleNamespace(
+        PrimChem=PrimChemV, FluidMesh=FluidMeshV, RaySegment=RaySegmentV, LightRay=LightRayV,
+        LightRayIO=LightRayIOV, CrossSection=CrossSectionV, PhotoionRate=PhotoionRateV,
+        RunParam=RunParamV, RadiationSrc=RadiationSrc, FreqParam=FreqParam,
+        columns=cols, rates=rates, channels=chans)
+    ns.STRUCTS = [RaySegmentV, LightRayV, LightRayIOV, RadiationSrc, FluidMeshV, PrimChemV, RunParamV,
+                  CrossSectionV, FreqParam, PhotoionRateV]
+    ns.sizes = lambda: [C.sizeof(s) for s in ns.STRUCTS]
+    return ns
+
+
+# the flag sets the library is also built for: tag -> (helium, H2, photon
+# conserving, cosmological); the default library is helium + photon conserving
+FLAGSETS = {
+    "h2_pc": (False, True, True, False),
+    "he_h2_pc": (True, True, True, False),
+    "he": (True, False, False, False),
+    "he_pc_cosmo": (True, False, True, True),
+    "hi": (False, False, False, False),
+}

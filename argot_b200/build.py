@@ -5,6 +5,15 @@ Every ``.cu`` file under ``argot_b200/csrc`` is compiled to an object in
 ``argot_b200/libargot_b200.so`` with the CUDA runtime linked statically, so
 the library does not depend on which libcudart a host process already
 loaded.
+
+ARGOT's struct layouts and rate formula follow its preprocessor flags, so
+the drop-in is also built for other flag sets: the sources that see the
+reference's structs (those that include ``ref_layout.h``) are compiled again
+with the set's flags and linked with the other objects into
+``libargot_b200_<tag>.so``.  FLAGSETS lists the sets built by default (the
+stock set of ARGOT's Makefile, -D__HYDROGEN_MOL__ -D__PHOTON_CONSERVING__,
+among them); ``python -m argot_b200.build --flags "-D__HELIUM__ ..."`` builds
+any other.
 """
 from __future__ import annotations
 
@@ -62,6 +71,72 @@ def _compile(src: str, verbose: bool, extra) -> str:
     return obj
 
 
+# tag -> the reference's flags (the default library is helium + photon
+# conserving)
+FLAGSETS = {
+    "h2_pc": ["-D__HYDROGEN_MOL__", "-D__PHOTON_CONSERVING__"],
+    "he_h2_pc": ["-D__HELIUM__", "-D__HYDROGEN_MOL__", "-D__PHOTON_CONSERVING__"],
+    "he": ["-D__HELIUM__"],
+    "he_pc_cosmo": ["-D__HELIUM__", "-D__PHOTON_CONSERVING__", "-D__COSMOLOGICAL__"],
+    "hi": [],
+}
+
+
+def flagset_tag(flags) -> str:
+    """libargot_b200_<tag>.so for a list of -D flags"""
+    f = set(flags)
+    parts = [t for t, m in (("he", "-D__HELIUM__"), ("h2", "-D__HYDROGEN_MOL__"),
+                            ("pc", "-D__PHOTON_CONSERVING__"), ("cosmo", "-D__COSMOLOGICAL__")) if m in f]
+    if not ("-D__HELIUM__" in f or "-D__HYDROGEN_MOL__" in f):
+        parts.insert(0, "hi")
+    return "_".join(parts)
+
+
+def flagset_lib(tag: str) -> str:
+    return os.path.join(HERE, f"libargot_b200_{tag}.so")
+
+
+def _layout_sources():
+    return [s for s in sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+            if '#include "ref_layout.h"' in open(s).read()]
+
+
+def build_flagset(flags, verbose: bool = False) -> str:
+    """libargot_b200_<tag>.so: the library with its drop-in compiled for the
+    reference flags `flags` (a list of -D options)."""
+    tag = flagset_tag(flags)
+    out = os.path.join(BUILD, "flags_" + tag)
+    os.makedirs(out, exist_ok=True)
+    layout = _layout_sources()
+    extra = ["-DARGOT_FLAGSET_EXPLICIT", *flags]
+
+    def comp(src):
+        obj = os.path.join(out, os.path.basename(src) + ".o")
+        if _stale(obj, _deps(src)):
+            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-c", src, "-o", obj]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, cmd)
+        return obj
+
+    with cf.ThreadPoolExecutor(max_workers=min(8, len(layout))) as ex:
+        objs = list(ex.map(comp, layout))
+    shared = [os.path.join(BUILD, os.path.basename(s) + ".o")
+              for s in sorted(glob.glob(os.path.join(CSRC, "*.cu"))) if s not in layout]
+    lib = flagset_lib(tag)
+    if _stale(lib, objs + shared):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", lib, *objs, *shared, "-cudart", "static",
+               "-Xlinker", "--no-undefined", "-Xlinker", "--exclude-libs,ALL",
+               "-Xlinker", "-Bsymbolic", "-lpthread", "-ldl", "-lrt"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return lib
+
+
 def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
@@ -77,6 +152,8 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
     build_legacy(verbose)
+    for flags in FLAGSETS.values():
+        build_flagset(flags, verbose)
     return LIB
 
 
@@ -100,4 +177,7 @@ def build_legacy(verbose: bool = False) -> str:
 
 
 if __name__ == "__main__":
-    print(build(verbose="-v" in sys.argv, ptxas_info="--ptxas" in sys.argv))
+    if "--flags" in sys.argv:
+        print(build_flagset(sys.argv[sys.argv.index("--flags") + 1].split(), verbose="-v" in sys.argv))
+    else:
+        print(build(verbose="-v" in sys.argv, ptxas_info="--ptxas" in sys.argv))

@@ -362,6 +362,7 @@ __global__ void __launch_bounds__(256) k_art_add(uint64_t n, const float *__rest
   }
 }
 
+#ifdef ARGOT_HELIUM_LAYOUT
 // fluid_mesh AoS <-> the planes of the ART kernels (the drop-in)
 __global__ void __launch_bounds__(256) k_art_from_mesh(uint64_t n, const fluid_mesh *__restrict__ mesh,
                                                       float *__restrict__ f8, float *__restrict__ rates6) {
@@ -395,6 +396,8 @@ __global__ void __launch_bounds__(256) k_art_to_mesh(uint64_t n, const float *__
     p.HeatHeII = rates6[5 * n + c];
   }
 }
+
+#endif  // ARGOT_HELIUM_LAYOUT
 
 int art_blocks(uint64_t n) {
   int dev = 0, sms = 148;
@@ -553,6 +556,7 @@ int *err_flag(int dev);
 int check_err_flag(int *flag, cudaStream_t st);
 }  // namespace argot
 
+#ifdef ARGOT_HELIUM_LAYOUT
 namespace argot {
 
 // Buffers of the drop-in, kept across calls.
@@ -646,6 +650,7 @@ int art_dropin(run_param *run, cuda_mem_space *cm, cuda_param *cp, host_diffuse_
 }
 
 }  // namespace argot
+#endif  // ARGOT_HELIUM_LAYOUT
 
 extern "C" {
 
@@ -736,6 +741,7 @@ void argot_b200_art_destroy(argot_b200_art *a) {
 
 int argot_b200_art_num_angles(const argot_b200_art *a) { return a ? a->nang : 0; }
 
+#ifdef ARGOT_HELIUM_LAYOUT
 // calc_diffuse_photon_radiation as built with __USE_GPU__
 // (calc_diffuse_photon_radiation.c:37-128) on one rank: the angle table and
 // step factors the caller's setup_diffuse_photon filled in hd_param, the
@@ -750,6 +756,7 @@ void calc_diffuse_photon_radiation(::fluid_mesh *mesh, ::run_param *this_run, ::
                        argot::art_dropin((argot::run_param *)this_run, (argot::cuda_mem_space *)cuda_mem,
                                          (argot::cuda_param *)this_cuda, (argot::host_diffuse_param *)hd_param));
 }
+#endif  // ARGOT_HELIUM_LAYOUT
 
 uint64_t argot_b200_art_workspace(const argot_b200_grid *g, int angles_per_pass) {
   if (!grid_valid(g) || angles_per_pass < 1) return 0;

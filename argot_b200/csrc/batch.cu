@@ -71,6 +71,7 @@ __global__ void __launch_bounds__(32 * kWarps, ARGOT_BATCH_MIN_WARPS / kWarps)
   __shared__ float s_p[kWarps][32][3];
   __shared__ float s_out[kWarps][32][6];
   __shared__ int s_e[kWarps][32], s_t[kWarps][32], s_cnt[kWarps][32], s_src[kWarps][32];
+  __shared__ int s_nsfu[kWarps][32];
   load_bin_pairs(s_pairs);
   __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -132,22 +133,28 @@ __global__ void __launch_bounds__(32 * kWarps, ARGOT_BATCH_MIN_WARPS / kWarps)
             s_p[wib][lane][s] = p.P[s];
           }
           s_e[wib][lane] = (int)e;
+          s_nsfu[wib][lane] = sfu_iters(p.D[0], p.D[1], p.D[2]);
         }
         s_t[wib][lane] = t;
         __syncwarp();
         const int nk = (int)min((uint64_t)32, r1 - rc);
-        for (int q = grp; q < nk; q += 4) {
+        // rounds of four rays with one SFU count, as in rate_block_f32
+        for (int q0 = 0; q0 < nk; q0 += 4) {
+          const int q = q0 + grp < nk ? q0 + grp : q0;
+          int nsfu = 0;
+#pragma unroll
+          for (int k = 0; k < 4; k++) nsfu = max(nsfu, q0 + k < nk ? s_nsfu[wib][q0 + k] : 0);
           const float N0 = s_nd[wib][q][0], N1 = s_nd[wib][q][1], N2 = s_nd[wib][q][2];
           const float D0 = s_nd[wib][q][3], D1 = s_nd[wib][q][4], D2 = s_nd[wib][q][5];
           const float *sp = specn + (size_t)s_e[wib][q] * kNu;
           float part[6];
-          ray_bins_packed(s_pairs, sp, j, N0, N1, N2, D0, D1, D2, part);
+          ray_bins_packed(s_pairs, sp, j, nsfu, N0, N1, N2, D0, D1, D2, part);
 #pragma unroll
           for (int o = 1; o < 8; o <<= 1) {
 #pragma unroll
             for (int s = 0; s < 6; s++) part[s] += __shfl_xor_sync(gmask, part[s], o);
           }
-          if (j == 0) {
+          if (j == 0 && q0 + grp < nk) {
             const float Pq[3] = {s_p[wib][q][0], s_p[wib][q][1], s_p[wib][q][2]};
             float out[6];
             ray_rates6(Pq, part[0], part[1], part[2], part[3], part[4], part[5], out);

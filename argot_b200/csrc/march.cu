@@ -4,7 +4,6 @@
 #include <cub/device/device_scan.cuh>
 
 #include "march.cuh"
-#include "ref_layout.h"
 
 namespace argot {
 
@@ -20,17 +19,6 @@ __global__ void k_pack_fields(uint64_t n, const float *__restrict__ dens, const 
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
     const float d = dens[i], a = fHI[i], b = fHeI[i], c = fHeII[i];
-    const float nhe = __double2float_rn(__dmul_rn((double)d, kHeliumFact));
-    cells[i] = make_float4(__fmul_rn(d, a), __fmul_rn(nhe, b), __fmul_rn(nhe, c), 0.f);
-    if (raw) raw[i] = make_float4(d, a, b, c);
-  }
-}
-
-__global__ void k_pack_mesh(uint64_t n, const fluid_mesh *__restrict__ mesh, float4 *__restrict__ cells,
-                            float4 *__restrict__ raw) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    const float d = mesh[i].dens, a = mesh[i].chem.fHI, b = mesh[i].chem.fHeI, c = mesh[i].chem.fHeII;
     const float nhe = __double2float_rn(__dmul_rn((double)d, kHeliumFact));
     cells[i] = make_float4(__fmul_rn(d, a), __fmul_rn(nhe, b), __fmul_rn(nhe, c), 0.f);
     if (raw) raw[i] = make_float4(d, a, b, c);
@@ -252,47 +240,6 @@ __global__ void k_march_segments(GridDev g, const float4 *__restrict__ cells, ui
   if (bad) atomicExch(err, 1);
 }
 
-// the reference's struct ray_segment array, in place (drop-in path)
-template <int kPrec>
-__global__ void k_march_aos(GridDev g, const float4 *__restrict__ cells, uint64_t nseg,
-                            ray_segment *__restrict__ seg, int *__restrict__ err) {
-  bool bad = false;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nseg;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    ray_segment &s = seg[i];
-    int steps;
-    const Tau3 t = (kPrec == ARGOT_B200_PRECISION_REFERENCE)
-                       ? march_reference(g, cells, s.xpos_start, s.ypos_start, s.zpos_start, s.xpos_end,
-                                         s.ypos_end, s.zpos_end, &steps, &bad)
-                       : march_kahan(g, cells, s.xpos_start, s.ypos_start, s.zpos_start, s.xpos_end,
-                                     s.ypos_end, s.zpos_end, &steps, &bad);
-    s.optical_depth_HI = t.hi;
-    s.optical_depth_HeI = t.hei;
-    s.optical_depth_HeII = t.heii;
-  }
-  if (bad) atomicExch(err, 1);
-}
-
-int launch_march_aos(const GridDev &g, const float4 *cells, uint64_t nseg, void *seg_dev, int prec,
-                     int *err_dev, cudaStream_t st) {
-  if (!nseg) return 0;
-  const int threads = 128;
-  const int blocks = grid_blocks_for(nseg, threads);
-  if (prec == ARGOT_B200_PRECISION_REFERENCE)
-    k_march_aos<ARGOT_B200_PRECISION_REFERENCE><<<blocks, threads, 0, st>>>(g, cells, nseg, (ray_segment *)seg_dev, err_dev);
-  else
-    k_march_aos<ARGOT_B200_PRECISION_KAHAN><<<blocks, threads, 0, st>>>(g, cells, nseg, (ray_segment *)seg_dev, err_dev);
-  ARGOT_CUDA_TRY(cudaGetLastError());
-  return 0;
-}
-
-int launch_pack_mesh(uint64_t n, const void *mesh, float4 *cells, float4 *raw, cudaStream_t st) {
-  if (!n) return 0;
-  k_pack_mesh<<<grid_blocks_for(n, 256), 256, 0, st>>>(n, (const fluid_mesh *)mesh, cells, raw);
-  ARGOT_CUDA_TRY(cudaGetLastError());
-  return 0;
-}
-
 // ---------------------------------------------------------------- stitching
 // Segments sorted by ray index: one thread per ray boundary run.  Each run
 // of equal ray_indx is summed with Kahan compensation and written to its
@@ -380,19 +327,6 @@ int argot_b200_pack_fields(const argot_b200_grid *gp, const float *dens, const f
   ARGOT_CUDA_TRY(cudaGetLastError());
   set_status(0);
   return 0;
-}
-
-int argot_b200_pack_fluid_mesh(const argot_b200_grid *gp, const void *mesh_dev, void *packed_dev,
-                               void *stream) {
-  if (!grid_valid(gp) || !mesh_dev || !packed_dev) {
-    set_status(ARGOT_B200_EINVAL);
-    return ARGOT_B200_EINVAL;
-  }
-  const uint64_t n = (uint64_t)gp->nx * gp->ny * gp->nz;
-  float4 *cells = (float4 *)packed_dev;
-  int rc = launch_pack_mesh(n, mesh_dev, cells, cells + n, (cudaStream_t)stream);
-  set_status(rc);
-  return rc;
 }
 
 int argot_b200_num_blocks(const argot_b200_grid *gp, uint64_t *nblocks) {

@@ -8,14 +8,31 @@ struct Tau3 {
   float hi, hei, heii;
 };
 
+// NC columns of a segment (the drop-in's flag sets carry 1 to 6 species).
+template <int NC>
+struct Cols {
+  float v[NC];
+};
+
+// Packed cells with NC species: (NC + 3) / 4 float4 per cell, species in
+// column order (one float4 {n_HI, n_HeI, n_HeII, 0} for the default set).
+template <int NC>
+__device__ __forceinline__ void ld_cols(const float4 *__restrict__ cells, size_t c, float (&n)[NC]) {
+  constexpr int NG = (NC + 3) / 4;
+#pragma unroll
+  for (int q = 0; q < NG; q++) {
+    const float4 f = __ldg(cells + c * NG + q);
+    if (4 * q + 0 < NC) n[(4 * q + 0) % NC] = f.x;
+    if (4 * q + 1 < NC) n[(4 * q + 1) % NC] = f.y;
+    if (4 * q + 2 < NC) n[(4 * q + 2) % NC] = f.z;
+    if (4 * q + 3 < NC) n[(4 * q + 3) % NC] = f.w;
+  }
+}
+
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 __device__ __forceinline__ size_t cell_index(const GridDev &g, int ix, int iy, int iz) {
   return (size_t)iz + (size_t)g.nz * ((size_t)iy + (size_t)g.ny * (size_t)ix);
-}
-
-__device__ __forceinline__ float4 ld_cell(const float4 *__restrict__ cells, size_t c) {
-  return __ldg(cells + c);
 }
 
 // Cell index of a coordinate along one axis, truncated toward zero and
@@ -38,9 +55,10 @@ __device__ __forceinline__ float cosine_guard(float c) {
 // build bit for bit.  `*steps` receives the number of cells visited (the
 // loop iterations plus the end cell); `*bad` is set when the walk exceeds
 // nx+ny+nz+2 steps (only possible for non-finite input).
-static __device__ __noinline__ Tau3 march_reference(const GridDev &g, const float4 *__restrict__ cells,
-                                             float xs, float ys, float zs, float xe, float ye,
-                                             float ze, int *steps, bool *bad) {
+template <int NC>
+static __device__ __noinline__ Cols<NC> march_reference_n(const GridDev &g, const float4 *__restrict__ cells,
+                                                          float xs, float ys, float zs, float xe, float ye,
+                                                          float ze, int *steps, bool *bad) {
   const int ixe = axis_cell(xe, g.xminl, g.dx, g.nx);
   const int iye = axis_cell(ye, g.yminl, g.dy, g.ny);
   const int ize = axis_cell(ze, g.zminl, g.dz, g.nz);
@@ -65,13 +83,16 @@ static __device__ __noinline__ Tau3 march_reference(const GridDev &g, const floa
   const int sz = zo > 0.f ? 1 : 0, nzs = zo > 0.f ? 1 : -1;
 
   float xc = __fsub_rn(xs, g.xminl), yc = __fsub_rn(ys, g.yminl), zc = __fsub_rn(zs, g.zminl);
-  Tau3 t = {0.f, 0.f, 0.f};
+  Cols<NC> t;
+#pragma unroll
+  for (int q = 0; q < NC; q++) t.v[q] = 0.f;
   int it = 0;
   const int cap = g.nx + g.ny + g.nz + 2;
   while ((ix != ixe || iy != iye || iz != ize) && (unsigned)ix < (unsigned)g.nx &&
          (unsigned)iy < (unsigned)g.ny && (unsigned)iz < (unsigned)g.nz) {
     if (++it > cap) { *bad = true; break; }
-    const float4 n = ld_cell(cells, cell_index(g, ix, iy, iz));
+    float n[NC];
+    ld_cols<NC>(cells, cell_index(g, ix, iy, iz), n);
     const float ddx = __fsub_rn(__fmul_rn(g.dx, __int2float_rn(sx + ix)), xc);
     const float ddy = __fsub_rn(__fmul_rn(g.dy, __int2float_rn(sy + iy)), yc);
     const float ddz = __fsub_rn(__fmul_rn(g.dz, __int2float_rn(sz + iz)), zc);
@@ -83,9 +104,8 @@ static __device__ __noinline__ Tau3 march_reference(const GridDev &g, const floa
     xc = __fadd_rn(xc, __fmul_rn(rmin, xo));
     yc = __fadd_rn(yc, __fmul_rn(rmin, yo));
     zc = __fadd_rn(zc, __fmul_rn(rmin, zo));
-    t.hi = __fadd_rn(t.hi, __fmul_rn(rmin, n.x));
-    t.hei = __fadd_rn(t.hei, __fmul_rn(rmin, n.y));
-    t.heii = __fadd_rn(t.heii, __fmul_rn(rmin, n.z));
+#pragma unroll
+    for (int q = 0; q < NC; q++) t.v[q] = __fadd_rn(t.v[q], __fmul_rn(rmin, n[q]));
   }
   xc = __fadd_rn(xc, g.xminl);
   yc = __fadd_rn(yc, g.yminl);
@@ -93,12 +113,20 @@ static __device__ __noinline__ Tau3 march_reference(const GridDev &g, const floa
   const float ex = __fsub_rn(xe, xc), ey = __fsub_rn(ye, yc), ez = __fsub_rn(ze, zc);
   const float e3 = __fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez));
   const float depth = __double2float_rn(__dsqrt_rn((double)e3));
-  const float4 ne = ld_cell(cells, cell_index(g, ixe, iye, ize));
-  t.hi = __fadd_rn(t.hi, __fmul_rn(depth, ne.x));
-  t.hei = __fadd_rn(t.hei, __fmul_rn(depth, ne.y));
-  t.heii = __fadd_rn(t.heii, __fmul_rn(depth, ne.z));
+  float ne[NC];
+  ld_cols<NC>(cells, cell_index(g, ixe, iye, ize), ne);
+#pragma unroll
+  for (int q = 0; q < NC; q++) t.v[q] = __fadd_rn(t.v[q], __fmul_rn(depth, ne[q]));
   *steps = it + 1;
   return t;
+}
+
+// The three-column march of the device path.
+__device__ __forceinline__ Tau3 march_reference(const GridDev &g, const float4 *__restrict__ cells, float xs,
+                                                float ys, float zs, float xe, float ye, float ze, int *steps,
+                                                bool *bad) {
+  const Cols<3> c = march_reference_n<3>(g, cells, xs, ys, zs, xe, ye, ze, steps, bad);
+  return Tau3{c.v[0], c.v[1], c.v[2]};
 }
 
 // Compensated (Kahan) summation step: s + c carries the running sum.
@@ -119,6 +147,9 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float v) {
 // cell, and the crossed axes advance to their following face by the face
 // spacing dX/|u_x|.  The walk always ends in the end cell after at most
 // sum|di| steps.  Columns are FP32 with compensated (Kahan) summation.
+// (Testing the next face against the position of each axis's last face
+// instead of keeping counts executes 9% fewer instructions but takes more
+// selects and spills at 32 registers: 4% slower, measured.)
 //
 // Path lengths are unsigned fixed-point integers.  Every chord is a
 // difference of two path lengths to faces, and the face spacing of a
@@ -146,23 +177,23 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float v) {
 // slots (`slot`, words kSlotStride apart), touched once per 16 steps, which
 // frees six registers for the walk.
 // Kahan step on a column kept in per-thread shared-memory slots: sum in
-// word q, compensation in word q + 3 (words kStride apart).
-template <int kStride>
+// word q, compensation in word q + NC (words kStride apart).
+template <int NC, int kStride>
 __device__ __forceinline__ void kahan_slot(float *slot, int q, float v) {
-  float s = slot[q * kStride], c = slot[(q + 3) * kStride];
+  float s = slot[q * kStride], c = slot[(q + NC) * kStride];
   kahan_add(s, c, v);
   slot[q * kStride] = s;
-  slot[(q + 3) * kStride] = c;
+  slot[(q + NC) * kStride] = c;
 }
 
 __device__ __forceinline__ uint64_t fixed_32_32(double units) {
   return (uint64_t)__double2ull_rz(units * 4294967296.0);
 }
 
-template <int kSlotStride = 0>
-static __device__ __forceinline__ Tau3 march_kahan(const GridDev &g, const float4 *__restrict__ cells,
-                                                   float xs, float ys, float zs, float xe, float ye,
-                                                   float ze, int *steps, bool *bad, float *slot = nullptr) {
+template <int NC, int kSlotStride = 0>
+static __device__ __forceinline__ Cols<NC> march_kahan_n(const GridDev &g, const float4 *__restrict__ cells,
+                                                         float xs, float ys, float zs, float xe, float ye,
+                                                         float ze, int *steps, bool *bad, float *slot = nullptr) {
   const int ixe = axis_cell(xe, g.xminl, g.dx, g.nx);
   const int iye = axis_cell(ye, g.yminl, g.dy, g.ny);
   const int ize = axis_cell(ze, g.zminl, g.dz, g.nz);
@@ -199,11 +230,12 @@ static __device__ __forceinline__ Tau3 march_kahan(const GridDev &g, const float
   const int dsz = stz, dsy = sty * g.nz, dsx = stx * g.nz * g.ny;
   int idx = iz + g.nz * (iy + g.ny * ix);
 
-  float p0 = 0.f, p1 = 0.f, p2 = 0.f;
-  float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
+  float p[NC], s[NC], c[NC];
+#pragma unroll
+  for (int q = 0; q < NC; q++) p[q] = s[q] = c[q] = 0.f;
   if (kSlotStride) {
 #pragma unroll
-    for (int q = 0; q < 6; q++) slot[q * kSlotStride] = 0.f;
+    for (int q = 0; q < 2 * NC; q++) slot[q * kSlotStride] = 0.f;
   }
   uint32_t t = 0;  // path length of the latest crossing (units)
   int it = 0;
@@ -218,13 +250,13 @@ static __device__ __forceinline__ Tau3 march_kahan(const GridDev &g, const float
       const uint32_t xh = (uint32_t)(tx >> 32), yh = (uint32_t)(ty >> 32), zh = (uint32_t)(tz >> 32);
       const uint32_t m = min(xh, min(yh, zh));
       const bool hx = xh == m, hy = yh == m, hz = zh == m;
-      const float4 n = __ldg(cells + idx);
+      float n[NC];
+      ld_cols<NC>(cells, (size_t)idx, n);
       idx += (hx ? dsx : 0) + (hy ? dsy : 0) + (hz ? dsz : 0);
       const float rf = __uint2float_rn(m - t);
       t = m;
-      p0 = fmaf(rf, n.x, p0);
-      p1 = fmaf(rf, n.y, p1);
-      p2 = fmaf(rf, n.z, p2);
+#pragma unroll
+      for (int q = 0; q < NC; q++) p[q] = fmaf(rf, n[q], p[q]);
       cx -= hx; cy -= hy; cz -= hz;
       if (hx) tx = cx ? tx + Tx : kNone;
       if (hy) ty = cy ? ty + Ty : kNone;
@@ -232,35 +264,74 @@ static __device__ __forceinline__ Tau3 march_kahan(const GridDev &g, const float
     }
     it += kk;
     if (kk == 16) {
-      if (kSlotStride) {
-        kahan_slot<kSlotStride>(slot, 0, p0);
-        kahan_slot<kSlotStride>(slot, 1, p1);
-        kahan_slot<kSlotStride>(slot, 2, p2);
-      } else {
-        kahan_add(s0, c0, p0);
-        kahan_add(s1, c1, p1);
-        kahan_add(s2, c2, p2);
+#pragma unroll
+      for (int q = 0; q < NC; q++) {
+        if (kSlotStride)
+          kahan_slot<NC, kSlotStride>(slot, q, p[q]);
+        else
+          kahan_add(s[q], c[q], p[q]);
+        p[q] = 0.f;
       }
-      p0 = p1 = p2 = 0.f;
     }
   }
   // the last chord: from the latest crossing to the end point
   const float df = __int2float_rn(max((int)(lu - t), 0));
-  const float4 n = __ldg(cells + idx);
-  p0 = fmaf(df, n.x, p0);
-  p1 = fmaf(df, n.y, p1);
-  p2 = fmaf(df, n.z, p2);
-  if (kSlotStride) {
-    s0 = slot[0]; c0 = slot[3 * kSlotStride];
-    s1 = slot[kSlotStride]; c1 = slot[4 * kSlotStride];
-    s2 = slot[2 * kSlotStride]; c2 = slot[5 * kSlotStride];
-  }
-  kahan_add(s0, c0, p0);
-  kahan_add(s1, c1, p1);
-  kahan_add(s2, c2, p2);
+  float n[NC];
+  ld_cols<NC>(cells, (size_t)idx, n);
   const float unit = (float)(dmax * ldexp(1.0, -k));  // exact: dmax is a float
+  Cols<NC> out;
+#pragma unroll
+  for (int q = 0; q < NC; q++) {
+    p[q] = fmaf(df, n[q], p[q]);
+    if (kSlotStride) {
+      s[q] = slot[q * kSlotStride];
+      c[q] = slot[(q + NC) * kSlotStride];
+    }
+    kahan_add(s[q], c[q], p[q]);
+    out.v[q] = s[q] * unit;
+  }
   *steps = it + 1;
-  return Tau3{s0 * unit, s1 * unit, s2 * unit};
+  return out;
+}
+
+// The three-column march of the device path.
+template <int kSlotStride = 0>
+__device__ __forceinline__ Tau3 march_kahan(const GridDev &g, const float4 *__restrict__ cells, float xs, float ys,
+                                            float zs, float xe, float ye, float ze, int *steps, bool *bad,
+                                            float *slot = nullptr) {
+  const Cols<3> c = march_kahan_n<3, kSlotStride>(g, cells, xs, ys, zs, xe, ye, ze, steps, bad, slot);
+  return Tau3{c.v[0], c.v[1], c.v[2]};
+}
+
+// Rate geometry shared by both precisions (calc_photoion_rate.c:176-246, FP32
+// where the reference uses float): target centre, squared distance and
+// distance, and the cell chord `delta` along the ray (delta_length, :52-90).
+struct RayGeom {
+  float dist2, dist, delta;
+};
+
+__device__ __forceinline__ RayGeom ray_geometry(const GridDev &g, int gix, int giy, int giz, float sx,
+                                                float sy, float sz) {
+  // x = delta_x*((float)ix + 0.5) + xmin, in double, stored as float
+  const float x = __double2float_rn(__dadd_rn(__dmul_rn((double)g.dx, __dadd_rn((double)__int2float_rn(gix), 0.5)), (double)g.xmin));
+  const float y = __double2float_rn(__dadd_rn(__dmul_rn((double)g.dy, __dadd_rn((double)__int2float_rn(giy), 0.5)), (double)g.ymin));
+  const float z = __double2float_rn(__dadd_rn(__dmul_rn((double)g.dz, __dadd_rn((double)__int2float_rn(giz), 0.5)), (double)g.zmin));
+  const float dx = __fsub_rn(x, sx), dy = __fsub_rn(y, sy), dz = __fsub_rn(z, sz);
+  const float sxy = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+  const float s3 = __fadd_rn(sxy, __fmul_rn(dz, dz));
+  const float dl = __double2float_rn(__dsqrt_rn(__dadd_rn((double)s3, kTiny)));
+  const float dxy = __double2float_rn(__dsqrt_rn(__dadd_rn((double)sxy, kTiny)));
+  const float ct = __fdiv_rn(dz, dl), st = __fdiv_rn(dxy, dl);
+  const float cp = __fdiv_rn(dx, dxy), sp = __fdiv_rn(dy, dxy);
+  const float xo = cosine_guard(__fmul_rn(cp, st));
+  const float yo = cosine_guard(__fmul_rn(sp, st));
+  const float zo = cosine_guard(ct);
+  const float rx = fabsf(__fdiv_rn(g.dx, xo)), ry = fabsf(__fdiv_rn(g.dy, yo)), rz = fabsf(__fdiv_rn(g.dz, zo));
+  RayGeom r;
+  r.delta = fminf(rx, fminf(ry, rz));
+  r.dist2 = s3;
+  r.dist = __double2float_rn(__dsqrt_rn((double)s3));
+  return r;
 }
 
 // ---------------------------------------------------------------------------

@@ -1,7 +1,6 @@
 // photoion.cu -- per-cell photo-ionisation and heating rates from the rays
 // of each target block (calc_photoion_rate on the device-resident layout).
 #include "photoion.cuh"
-#include "ref_layout.h"
 
 namespace argot {
 
@@ -137,109 +136,6 @@ int launch_rate_f32_served(const GridDev &g, const float4 *raw, const float4 *em
   if (b0 >= b1) return 0;
   k_rate_f32<true><<<grid_blocks_for_rates((b1 - b0) * 32, 32 * kF32Warps), 32 * kF32Warps, 0, st>>>(
       g, raw, emit_pos, specn, total, b0, b1, blk_off, base, rays, nray, tau, rates6, pred, err);
-  ARGOT_CUDA_TRY(cudaGetLastError());
-  return 0;
-}
-
-// ------------------------------------------------------------- drop-in rays
-// Per-ray rates of the reference's light_ray_IO array (one thread per ray).
-__global__ void k_rate_rayio(GridDev g, const float4 *__restrict__ raw, const light_ray_IO *__restrict__ rays,
-                             uint64_t nray, int rank_x, int rank_y, int rank_z, double *__restrict__ per6) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nray;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    const light_ray_IO &r = rays[i];
-    const int lx = r.ix_target - rank_x * g.nx, ly = r.iy_target - rank_y * g.ny, lz = r.iz_target - rank_z * g.nz;
-    double out[6] = {0, 0, 0, 0, 0, 0};
-    if ((unsigned)lx < (unsigned)g.nx && (unsigned)ly < (unsigned)g.ny && (unsigned)lz < (unsigned)g.nz) {
-      const RayGeom geo = ray_geometry(g, r.ix_target, r.iy_target, r.iz_target, r.src.xpos, r.src.ypos, r.src.zpos);
-      const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
-      const RayCols cols = ray_columns(g, r.optical_depth_HI, r.optical_depth_HeI, r.optical_depth_HeII, rw, geo);
-      rate_bins_f64(cols, r.src.photon_rate, out);
-    }
-#pragma unroll
-    for (int s = 0; s < 6; s++) per6[6 * i + s] = out[s];
-  }
-}
-
-// Adds per-ray rates into mesh[].prev_chem in ray order.  One thread per run
-// of consecutive rays with the same target (the reference emits the rays of
-// a cell consecutively); each field is updated with a compare-and-swap so
-// that a cell appearing in several runs still receives every contribution.
-// A CAS fails only when another run of the same cell has just landed, so the
-// loop ends after at most that many retries; past 2^20 of them (more than a
-// million runs of one cell in flight) the run's sum is added with one float
-// atomicAdd instead, its per-ray float rounding is lost, and the device
-// error flag reports it.
-__device__ __forceinline__ void add_run(float *field, const double *per6, int s, uint64_t i0, uint64_t i1,
-                                        int *err) {
-  unsigned int *addr = (unsigned int *)field;
-  unsigned int old = *((volatile unsigned int *)addr);
-  for (int attempt = 0; attempt < 1 << 20; attempt++) {
-    float v = __uint_as_float(old);
-    for (uint64_t i = i0; i < i1; i++) v = __double2float_rn(__dadd_rn((double)v, per6[6 * i + s]));
-    const unsigned int prev = atomicCAS(addr, old, __float_as_uint(v));
-    if (prev == old) return;
-    old = prev;
-  }
-  double sum = 0.0;
-  for (uint64_t i = i0; i < i1; i++) sum += per6[6 * i + s];
-  atomicAdd(field, (float)sum);
-  atomicExch(err, 1);
-}
-
-__global__ void k_accum_runs(GridDev g, const light_ray_IO *__restrict__ rays, uint64_t nray, int rank_x,
-                             int rank_y, int rank_z, const double *__restrict__ per6, fluid_mesh *__restrict__ mesh,
-                             int *__restrict__ err) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nray;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    const int tx = rays[i].ix_target, ty = rays[i].iy_target, tz = rays[i].iz_target;
-    if (i > 0 && rays[i - 1].ix_target == tx && rays[i - 1].iy_target == ty && rays[i - 1].iz_target == tz)
-      continue;
-    uint64_t j = i + 1;
-    while (j < nray && rays[j].ix_target == tx && rays[j].iy_target == ty && rays[j].iz_target == tz) j++;
-    const int lx = tx - rank_x * g.nx, ly = ty - rank_y * g.ny, lz = tz - rank_z * g.nz;
-    if ((unsigned)lx >= (unsigned)g.nx || (unsigned)ly >= (unsigned)g.ny || (unsigned)lz >= (unsigned)g.nz) continue;
-    prim_chem &pc = mesh[cell_index(g, lx, ly, lz)].prev_chem;
-    add_run(&pc.GammaHI, per6, 0, i, j, err);
-    add_run(&pc.GammaHeI, per6, 1, i, j, err);
-    add_run(&pc.GammaHeII, per6, 2, i, j, err);
-    add_run(&pc.HeatHI, per6, 3, i, j, err);
-    add_run(&pc.HeatHeI, per6, 4, i, j, err);
-    add_run(&pc.HeatHeII, per6, 5, i, j, err);
-  }
-}
-
-__global__ void k_zero_rates(uint64_t n, fluid_mesh *__restrict__ mesh) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    prim_chem &pc = mesh[i].prev_chem;
-    pc.GammaHI = 0.f; pc.HeatHI = 0.f;
-    pc.GammaHeI = 0.f; pc.GammaHeII = 0.f;
-    pc.HeatHeI = 0.f; pc.HeatHeII = 0.f;
-  }
-}
-
-int launch_rate_rayio(const GridDev &g, const float4 *raw, const void *rays_io, uint64_t nray, int rx, int ry,
-                      int rz, double *per6, cudaStream_t st) {
-  if (!nray) return 0;
-  k_rate_rayio<<<grid_blocks_for_rates(nray, 128), 128, 0, st>>>(g, raw, (const light_ray_IO *)rays_io, nray, rx,
-                                                                  ry, rz, per6);
-  ARGOT_CUDA_TRY(cudaGetLastError());
-  return 0;
-}
-
-int launch_accum_runs(const GridDev &g, const void *rays_io, uint64_t nray, int rx, int ry, int rz,
-                      const double *per6, void *mesh, int *err, cudaStream_t st) {
-  if (!nray) return 0;
-  k_accum_runs<<<grid_blocks_for_rates(nray, 128), 128, 0, st>>>(g, (const light_ray_IO *)rays_io, nray, rx, ry,
-                                                                  rz, per6, (fluid_mesh *)mesh, err);
-  ARGOT_CUDA_TRY(cudaGetLastError());
-  return 0;
-}
-
-int launch_zero_rates(uint64_t n, void *mesh, cudaStream_t st) {
-  if (!n) return 0;
-  k_zero_rates<<<grid_blocks_for_rates(n, 256), 256, 0, st>>>(n, (fluid_mesh *)mesh);
   ARGOT_CUDA_TRY(cudaGetLastError());
   return 0;
 }

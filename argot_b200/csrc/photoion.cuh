@@ -37,39 +37,16 @@ static int ensure_rate_tables(int device) {
       t.hw[s][i] = (float)((double)c * w);
     }
   }
+  for (int s = 0; s < 3; s++) {
+    float m = 0.f;
+    for (int k = kNu - 1; k >= 0; k--) {
+      m = fmaxf(m, t.cs[s][k]);
+      if (k % 16 == 0) t.smax16[s][k / 16] = m;
+    }
+  }
   ARGOT_CUDA_TRY(cudaMemcpyToSymbol(c_tab, &t, sizeof(t)));
   done[device] = true;
   return 0;
-}
-
-// Geometry shared by both precisions (calc_photoion_rate.c:176-246, FP32
-// where the reference uses float): target centre, distance, and the cell
-// chord `delta` along the ray (delta_length, :52-90).
-struct RayGeom {
-  float dist, delta;
-};
-
-__device__ __forceinline__ RayGeom ray_geometry(const GridDev &g, int gix, int giy, int giz, float sx,
-                                                float sy, float sz) {
-  // x = delta_x*((float)ix + 0.5) + xmin, in double, stored as float
-  const float x = __double2float_rn(__dadd_rn(__dmul_rn((double)g.dx, __dadd_rn((double)__int2float_rn(gix), 0.5)), (double)g.xmin));
-  const float y = __double2float_rn(__dadd_rn(__dmul_rn((double)g.dy, __dadd_rn((double)__int2float_rn(giy), 0.5)), (double)g.ymin));
-  const float z = __double2float_rn(__dadd_rn(__dmul_rn((double)g.dz, __dadd_rn((double)__int2float_rn(giz), 0.5)), (double)g.zmin));
-  const float dx = __fsub_rn(x, sx), dy = __fsub_rn(y, sy), dz = __fsub_rn(z, sz);
-  const float sxy = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-  const float s3 = __fadd_rn(sxy, __fmul_rn(dz, dz));
-  const float dl = __double2float_rn(__dsqrt_rn(__dadd_rn((double)s3, kTiny)));
-  const float dxy = __double2float_rn(__dsqrt_rn(__dadd_rn((double)sxy, kTiny)));
-  const float ct = __fdiv_rn(dz, dl), st = __fdiv_rn(dxy, dl);
-  const float cp = __fdiv_rn(dx, dxy), sp = __fdiv_rn(dy, dxy);
-  const float xo = cosine_guard(__fmul_rn(cp, st));
-  const float yo = cosine_guard(__fmul_rn(sp, st));
-  const float zo = cosine_guard(ct);
-  const float rx = fabsf(__fdiv_rn(g.dx, xo)), ry = fabsf(__fdiv_rn(g.dy, yo)), rz = fabsf(__fdiv_rn(g.dz, zo));
-  RayGeom r;
-  r.delta = fminf(rx, fminf(ry, rz));
-  r.dist = __double2float_rn(__dsqrt_rn((double)s3));
-  return r;
 }
 
 // Per-species quantities of the target cell for one ray (double):
@@ -256,9 +233,14 @@ __device__ __forceinline__ void load_bin_pairs(BinPair *tab) {
 // cancels, so phi comes from a degree-6 polynomial, a near-minimax fit of
 // relative error made by argot_b200/fits.py (8.8e-8 relative on [0, 1]
 // evaluated in FP32 with Horner's rule, checked by the CPU tests).  Above,
-// e^-x on the SFU: (1 - e^-x) / x to ~2e-7.  The SFU path is taken only
-// when a lane of the warp needs it.
+// e^-x on the SFU: (1 - e^-x) / x to ~2e-7.  kSfu = false: the polynomial
+// alone, for the iterations whose bins are known to lie below x = 1
+// (sfu_iters): the SFU path is predicated, not branched, so where it is
+// compiled in every pair pays its two exponentials, two reciprocals and
+// their range handling (ncu, 256^3 / 16 sources: three MUFU operations per
+// bin instead of one, 60 warp instructions per iteration instead of ~40).
 constexpr float kPhiXMax = 1.0f;
+template <bool kSfu = true>
 __device__ __forceinline__ float2 phi_pc2(float2 dl2) {
   constexpr float kPhiC[7] = {1.f, -0.499999762f, 0.166663095f, -0.041645579f, 0.00827309582f, -0.00129866367f,
                               0.000128380707f};
@@ -267,6 +249,7 @@ __device__ __forceinline__ float2 phi_pc2(float2 dl2) {
   float2 p = make_float2(kPhiC[6], kPhiC[6]);
 #pragma unroll
   for (int k = 5; k >= 0; k--) p = __ffma2_rn(x, p, make_float2(kPhiC[k], kPhiC[k]));
+  if (!kSfu) return p;
   const bool t0 = x.x < kPhiXMax, t1 = x.y < kPhiXMax;
   if (!(t0 && t1)) {
     const float q0 = __fdividef(1.0f - ex2_approx(-dl2.x), x.x);
@@ -277,38 +260,62 @@ __device__ __forceinline__ float2 phi_pc2(float2 dl2) {
   return p;
 }
 
+// Iterations of ray_bins_packed that may hold a bin with x = sum_s D_s
+// sigma_s(nu) >= kPhiXMax: iteration i covers the bins 16 i .. 16 i + 15,
+// whose x is at most sum_s D_s max_{k >= 16 i} sigma_s (smax16).  That bound
+// does not grow with i, so the iterations that need the SFU path are the
+// leading ones; the rest take the polynomial alone.  (A bin whose x lies
+// within rounding of 1 may take the polynomial, 1e-7 accurate there.)
+__device__ __forceinline__ int sfu_iters(float D0, float D1, float D2) {
+  int n = 0;
+#pragma unroll
+  for (int i = 0; i < kNu / 16; i++)
+    n += fmaf(D0, c_tab.smax16[0][i], fmaf(D1, c_tab.smax16[1][i], D2 * c_tab.smax16[2][i])) >= kPhiXMax;
+  return n;
+}
+
+// One iteration of ray_bins_packed: the bin pair p of the lane.
+template <bool kSfu>
+__device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, float2 n0, float2 n1, float2 n2, float2 d0,
+                                         float2 d1, float2 d2, float2 (&acc)[6]) {
+  const float2 l0 = b.l2e[0], l1 = b.l2e[1], l2 = b.l2e[2];
+  const float2 tl = __ffma2_rn(n0, l0, __ffma2_rn(n1, l1, __fmul2_rn(n2, l2)));
+  const float2 dl = __ffma2_rn(d0, l0, __ffma2_rn(d1, l1, __fmul2_rn(d2, l2)));
+  const float2 e = make_float2(ex2_approx(-tl.x), ex2_approx(-tl.y));
+  const float2 ph = phi_pc2<kSfu>(dl);
+  const float2 w = __fmul2_rn(__fmul2_rn(s, e), ph);
+  const float2 vw = __fmul2_rn(b.nu, w);
+  acc[0] = __ffma2_rn(l0, w, acc[0]);
+  acc[1] = __ffma2_rn(l1, w, acc[1]);
+  acc[2] = __ffma2_rn(l2, w, acc[2]);
+  acc[3] = __ffma2_rn(l0, vw, acc[3]);
+  acc[4] = __ffma2_rn(l1, vw, acc[4]);
+  acc[5] = __ffma2_rn(l2, vw, acc[5]);
+}
+
 // The lane's six partial sums of one ray with columns N (to the cell) and
-// D (of the cell) in cm^-2; sp: the emitter's normalised spectrum:
+// D (of the cell) in cm^-2; sp: the emitter's normalised spectrum; j: the
+// lane in the ray's 8-lane group; the first nsfu iterations may need the
+// SFU path of phi (sfu_iters; the caller passes the same count to the four
+// groups of the warp, so that their loops stay converged):
 // out[s] = sum (sigma_s log2 e) w, out[3 + s] = sum (sigma_s log2 e) nu w
 // over the lane's bins, w = s_nu e^-tau phi(dtau).  The caller adds the
 // eight lanes and forms the rates (ray_rates6).
 __device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab, const float *__restrict__ sp,
-                                                int j, float N0, float N1, float N2, float D0, float D1, float D2,
-                                                float (&out)[6]) {
+                                                int j, int nsfu, float N0, float N1, float N2, float D0, float D1,
+                                                float D2, float (&out)[6]) {
   const float2 n0 = make_float2(N0, N0), n1 = make_float2(N1, N1), n2 = make_float2(N2, N2);
   const float2 d0 = make_float2(D0, D0), d1 = make_float2(D1, D1), d2 = make_float2(D2, D2);
+  // the pair's two spectrum bins in one 8-byte load (pair order)
+  const float2 *__restrict__ sp2 = reinterpret_cast<const float2 *>(sp) + j;
   float2 acc[6];
 #pragma unroll
   for (int q = 0; q < 6; q++) acc[q] = make_float2(0.f, 0.f);
+  int i = 0;
+#pragma unroll 2
+  for (; i < nsfu; i++) bin_pair<true>(tab[j + 8 * i], __ldg(sp2 + 8 * i), n0, n1, n2, d0, d1, d2, acc);
 #pragma unroll 4
-  for (int i = 0; i < kBinPairs / 8; i++) {
-    const BinPair &b = tab[j + 8 * i];
-    const float2 l0 = b.l2e[0], l1 = b.l2e[1], l2 = b.l2e[2];
-    const float2 tl = __ffma2_rn(n0, l0, __ffma2_rn(n1, l1, __fmul2_rn(n2, l2)));
-    const float2 dl = __ffma2_rn(d0, l0, __ffma2_rn(d1, l1, __fmul2_rn(d2, l2)));
-    // the pair's two spectrum bins in one 8-byte load (pair order)
-    const float2 s = __ldg(reinterpret_cast<const float2 *>(sp) + j + 8 * i);
-    const float2 e = make_float2(ex2_approx(-tl.x), ex2_approx(-tl.y));
-    const float2 ph = phi_pc2(dl);
-    const float2 w = __fmul2_rn(__fmul2_rn(s, e), ph);
-    const float2 vw = __fmul2_rn(b.nu, w);
-    acc[0] = __ffma2_rn(l0, w, acc[0]);
-    acc[1] = __ffma2_rn(l1, w, acc[1]);
-    acc[2] = __ffma2_rn(l2, w, acc[2]);
-    acc[3] = __ffma2_rn(l0, vw, acc[3]);
-    acc[4] = __ffma2_rn(l1, vw, acc[4]);
-    acc[5] = __ffma2_rn(l2, vw, acc[5]);
-  }
+  for (; i < kBinPairs / 8; i++) bin_pair<false>(tab[j + 8 * i], __ldg(sp2 + 8 * i), n0, n1, n2, d0, d1, d2, acc);
 #pragma unroll
   for (int q = 0; q < 6; q++) out[q] = acc[q].x + acc[q].y;
 }
@@ -319,6 +326,7 @@ struct RateWarpSmem {
   float p[32][3];    // prefactors P_s
   float out[32][6];  // per-ray rates
   int e[32], t[32];  // emitter, target lane
+  int nsfu[32];      // iterations of the bin loop that may need the SFU path (sfu_iters)
   int q[32];         // lanes of the chunk's rays that take the quadrature
   int cnt[32], src[32];  // per target lane: rays of the chunk, ray of the round
 };
@@ -414,6 +422,7 @@ __device__ __forceinline__ void rate_block_f32(const GridDev &g, const float4 *_
           S.p[lane][s] = p.P[s];
         }
         S.e[lane] = (int)e;
+        S.nsfu[lane] = sfu_iters(p.D[0], p.D[1], p.D[2]);
       }
     }
     S.t[lane] = t;
@@ -425,17 +434,25 @@ __device__ __forceinline__ void rate_block_f32(const GridDev &g, const float4 *_
       nq = __popc(m);
     }
     __syncwarp();
-    for (int i = grp; i < nq; i += 4) {
+    // rounds of four rays, one per group; the groups of a round run the
+    // same bin loop (the largest SFU count of the four), so that the warp
+    // stays converged; a group without a ray in the last round repeats the
+    // round's first ray and discards it
+    for (int i0 = 0; i0 < nq; i0 += 4) {
+      const int i = i0 + grp < nq ? i0 + grp : i0;
       const int q = kServed ? S.q[i] : i;
+      int nsfu = 0;
+#pragma unroll
+      for (int k = 0; k < 4; k++) nsfu = max(nsfu, i0 + k < nq ? S.nsfu[kServed ? S.q[i0 + k] : i0 + k] : 0);
       float part[6];
-      ray_bins_packed(pairs, specn + (size_t)S.e[q] * kNu, j, S.nd[q][0], S.nd[q][1], S.nd[q][2], S.nd[q][3],
+      ray_bins_packed(pairs, specn + (size_t)S.e[q] * kNu, j, nsfu, S.nd[q][0], S.nd[q][1], S.nd[q][2], S.nd[q][3],
                       S.nd[q][4], S.nd[q][5], part);
 #pragma unroll
       for (int o = 1; o < 8; o <<= 1) {
 #pragma unroll
         for (int s = 0; s < 6; s++) part[s] += __shfl_xor_sync(gmask, part[s], o);
       }
-      if (j == 0) {
+      if (j == 0 && i0 + grp < nq) {
         const float P[3] = {S.p[q][0], S.p[q][1], S.p[q][2]};
         float out[6];
         ray_rates6(P, part[0], part[1], part[2], part[3], part[4], part[5], out);

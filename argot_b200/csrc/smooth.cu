@@ -11,12 +11,11 @@
 // (the reference's default build, `isolated = yes`, with no neighbour rank)
 // or the periodic image.  Bit-identical to the reference.
 #include "march.cuh"
-#include "ref_layout.h"
 
 namespace argot {
 
 __global__ void __launch_bounds__(256) k_smooth(int nx, int ny, int nz, const float *__restrict__ in,
-                                               float *__restrict__ out, int isolated) {
+                                               float *__restrict__ out, int nplanes, int isolated) {
   const uint64_t ncell = (uint64_t)nx * ny * nz;
   const double kNormal = 1.0 / (30.0 + 26.0);
   for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < ncell;
@@ -40,7 +39,7 @@ __global__ void __launch_bounds__(256) k_smooth(int nx, int ny, int nz, const fl
 #pragma unroll
         for (int d = 0; d < 3; d++) off[9 * a + 3 * b + d] = (uint32_t)((jx[a] * ny + jy[b]) * nz + jz[d]);
 #pragma unroll 1
-    for (int s = 0; s < 6; s++) {
+    for (int s = 0; s < nplanes; s++) {
       const float *__restrict__ f = in + s * ncell;
       float acc = __ldg(f + off[0]);
 #pragma unroll
@@ -53,37 +52,6 @@ __global__ void __launch_bounds__(256) k_smooth(int nx, int ny, int nz, const fl
   }
 }
 
-// The six rate fields of prev_chem (AoS struct fluid_mesh, 156 B per cell)
-// to and from the plane layout of k_smooth (Γ HI, HeI, HeII, heat HI, HeI,
-// HeII; one plane of ncell floats each).
-__global__ void __launch_bounds__(256) k_rates_from_mesh(uint64_t n, const fluid_mesh *__restrict__ mesh,
-                                                        float *__restrict__ planes) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    const prim_chem &pc = mesh[i].prev_chem;
-    planes[0 * n + i] = pc.GammaHI;
-    planes[1 * n + i] = pc.GammaHeI;
-    planes[2 * n + i] = pc.GammaHeII;
-    planes[3 * n + i] = pc.HeatHI;
-    planes[4 * n + i] = pc.HeatHeI;
-    planes[5 * n + i] = pc.HeatHeII;
-  }
-}
-
-__global__ void __launch_bounds__(256) k_rates_to_mesh(uint64_t n, const float *__restrict__ planes,
-                                                      fluid_mesh *__restrict__ mesh) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    prim_chem &pc = mesh[i].prev_chem;
-    pc.GammaHI = planes[0 * n + i];
-    pc.GammaHeI = planes[1 * n + i];
-    pc.GammaHeII = planes[2 * n + i];
-    pc.HeatHI = planes[3 * n + i];
-    pc.HeatHeI = planes[4 * n + i];
-    pc.HeatHeII = planes[5 * n + i];
-  }
-}
-
 int smooth_blocks(uint64_t ncell) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -91,18 +59,12 @@ int smooth_blocks(uint64_t ncell) {
   return (int)(want < (uint64_t)sms * 8 ? (want ? want : 1) : (uint64_t)sms * 8);
 }
 
-// Smooths the rate fields of a device mesh in place: mesh -> planes (work),
-// smoothed planes (work + 6 ncell), planes -> mesh.  work holds 12 ncell
-// floats; afterwards its second half holds the smoothed planes.
-int launch_smooth_mesh(int nx, int ny, int nz, void *mesh, float *work, int isolated, cudaStream_t st) {
+// Smooths nplanes planes of ncell floats (in -> out).
+int launch_smooth_planes(int nx, int ny, int nz, const float *in, float *out, int nplanes, int isolated,
+                         cudaStream_t st) {
   const uint64_t ncell = (uint64_t)nx * ny * nz;
-  if (!ncell) return 0;
-  const int blocks = smooth_blocks(ncell);
-  k_rates_from_mesh<<<blocks, 256, 0, st>>>(ncell, (const fluid_mesh *)mesh, work);
-  ARGOT_CUDA_TRY(cudaGetLastError());
-  k_smooth<<<blocks, 256, 0, st>>>(nx, ny, nz, work, work + 6 * ncell, isolated);
-  ARGOT_CUDA_TRY(cudaGetLastError());
-  k_rates_to_mesh<<<blocks, 256, 0, st>>>(ncell, work + 6 * ncell, (fluid_mesh *)mesh);
+  if (!ncell || nplanes <= 0) return 0;
+  k_smooth<<<smooth_blocks(ncell), 256, 0, st>>>(nx, ny, nz, in, out, nplanes, isolated);
   ARGOT_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -121,7 +83,7 @@ int argot_b200_smooth_rates(const argot_b200_grid *gp, const float *in6, float *
   const uint64_t ncell = (uint64_t)gp->nx * gp->ny * gp->nz;
   if (ncell >= (1ull << 32)) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
   const int blocks = smooth_blocks(ncell);
-  k_smooth<<<blocks, 256, 0, (cudaStream_t)stream>>>(gp->nx, gp->ny, gp->nz, in6, out6, isolated);
+  k_smooth<<<blocks, 256, 0, (cudaStream_t)stream>>>(gp->nx, gp->ny, gp->nz, in6, out6, 6, isolated);
   ARGOT_CUDA_TRY(cudaGetLastError());
   set_status(0);
   return 0;

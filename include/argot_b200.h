@@ -11,11 +11,19 @@
  * 1. Drop-in entry points with the reference's exact names and signatures
  *    (ARGOT src/prototype.h).  The reference's structs are only
  *    forward-declared here, so a C host that includes ARGOT's own headers can
- *    include this file too; the library was compiled against byte-identical
- *    mirrors of those structs for the reference's default flag set
- *    (-D__HELIUM__ -D__PHOTON_CONSERVING__, no __HYDROGEN_MOL__, no
- *    __COSMOLOGICAL__, NGRID_NU=256, NSEG_PER_RAY=5, NMAX_CUDA_DEV=4), and
- *    argot_b200_abi_check() verifies a caller's struct sizes at run time.
+ *    include this file too.  ARGOT fixes its struct layouts and its rate
+ *    formula with preprocessor flags (src/Makefile:149-196), so the library
+ *    is built once per flag set, against byte-identical mirrors of the
+ *    structs for that set (NGRID_NU=256, NSEG_PER_RAY=5, NMAX_CUDA_DEV=4):
+ *      libargot_b200.so          -D__HELIUM__ -D__PHOTON_CONSERVING__ (the
+ *                                default; also carries the device API of 2.)
+ *      libargot_b200_h2_pc.so    -D__HYDROGEN_MOL__ -D__PHOTON_CONSERVING__
+ *                                (the set ARGOT's own Makefile compiles)
+ *      libargot_b200_he_h2_pc.so, libargot_b200_he.so (no photon
+ *      conservation), libargot_b200_he_pc_cosmo.so (-D__COSMOLOGICAL__), ...
+ *    (argot_b200/build.py builds any other combination on request).  A host
+ *    links the one its own flags select; argot_b200_flagset() names it and
+ *    argot_b200_abi_check() verifies the caller's struct sizes at run time.
  *    Mesh dimensions are read from run_param at run time, so one library
  *    serves every NMESH_* build.  These entry points use GPU 0 of the
  *    caller's cuda_param (one rank, one GPU).
@@ -60,6 +68,9 @@ ARGOT_B200_API const char *argot_b200_error_string(int code);
 
 /* library / ABI identification */
 ARGOT_B200_API const char *argot_b200_version(void);
+/* the flag set this build's drop-in follows, e.g. "helium, photon
+ * conserving" or "h2, photon conserving" */
+ARGOT_B200_API const char *argot_b200_flagset(void);
 /* sizes[10]: ray_segment, light_ray, light_ray_IO, radiation_src,
  * fluid_mesh, prim_chem, run_param, cross_section, freq_param,
  * photoion_rate as the library was compiled */
@@ -79,8 +90,9 @@ struct omp_param;
 struct mpi_param;
 
 /* Replaces src/calc_optical_depth_cuda.cu:29-144 (declared at
- * src/prototype.h:124).  Overwrites seg[0..run->nseg).optical_depth_* in
- * host memory before returning.  Reads the mesh from
+ * src/prototype.h:124).  Overwrites seg[0..run->nseg).optical_depth_* (every
+ * column of the build's flag set: HI, HeI, HeII, HM, H2I, H2II as present)
+ * in host memory before returning.  Reads the mesh from
  * cuda_mem[0].mesh_dev (device AoS struct fluid_mesh, filled by the caller's
  * send_mesh_data) and the domain geometry from *this_run (host copy). */
 ARGOT_B200_API void calc_optical_depth_cuda(struct ray_segment *seg, struct cuda_mem_space *cuda_mem,
@@ -88,12 +100,17 @@ ARGOT_B200_API void calc_optical_depth_cuda(struct ray_segment *seg, struct cuda
 
 /* Replaces src/calc_photoion_rate_cuda.cu:92-216 (src/prototype.h:125).
  * Fills ray_IO from ray as the reference does, and ADDS each ray's rates to
- * cuda_mem[0].mesh_dev[target].prev_chem.{Gamma,Heat}{HI,HeI,HeII}. */
+ * cuda_mem[0].mesh_dev[target].prev_chem: every Gamma and Heat field of the
+ * build's flag set, by the photon-conserving or the plain formula and with
+ * the scale-factor terms as the flags select (calc_photoion_rate.c:93-439,
+ * the H2 Lyman-Werner term included), in FP64.  The frequency grid and the
+ * cross sections are the caller's (this_run->freq, this_run->csect). */
 ARGOT_B200_API void calc_photoion_rate_cuda(struct cuda_mem_space *cuda_mem, struct light_ray *ray,
                              struct light_ray_IO *ray_IO, struct cuda_param *this_cuda,
                              struct run_param *this_run);
 
-/* Replaces src/calc_photoion_rate_cuda.cu:45-62 (src/prototype.h:93). */
+/* Replaces src/calc_photoion_rate_cuda.cu:45-62 (src/prototype.h:93):
+ * zeroes every rate field of prev_chem in cuda_mem[0].mesh_dev. */
 ARGOT_B200_API void zero_out_photoion_rate_cuda(struct cuda_mem_space *cuda_mem,
                                  struct cuda_param *this_cuda, struct run_param *this_run);
 
@@ -115,8 +132,8 @@ ARGOT_B200_API void accum_optical_depth(struct light_ray *ray, struct ray_segmen
 ARGOT_B200_API int argot_b200_set_dropin_march_mode(int mode);
 
 /* Replaces src/smooth_photoion_rate.c:27-1588 as built with __USE_GPU__
- * (src/prototype.h:89) on a single rank.  Smooths
- * cuda_mem[0].mesh_dev[].prev_chem.{Gamma,Heat}{HI,HeI,HeII} in place on the
+ * (src/prototype.h:89) on a single rank.  Smooths every rate field of
+ * cuda_mem[0].mesh_dev[].prev_chem in place on the
  * device, bit-identical to the reference's host smoothing (27 cells, centre
  * weighted by 30, times 1/56), so the rates stay in HBM for the GPU
  * chemistry (src/chemistry.cu) that reads mesh_dev next; then, when mesh is
@@ -160,7 +177,9 @@ typedef struct argot_b200_grid {
 ARGOT_B200_API int argot_b200_pack_fields(const argot_b200_grid *g, const float *dens, const float *fHI,
                            const float *fHeI, const float *fHeII, void *packed_dev,
                            void *stream);
-/* from a device array of the reference's struct fluid_mesh (156 B/cell) */
+/* from a device array of the reference's struct fluid_mesh (156 B/cell);
+ * ARGOT_B200_ENOTSUP in a build for a flag set without helium or with H2 or
+ * the scale factor (the device path carries HI, HeI and HeII only) */
 ARGOT_B200_API int argot_b200_pack_fluid_mesh(const argot_b200_grid *g, const void *mesh_dev,
                                void *packed_dev, void *stream);
 
@@ -480,7 +499,8 @@ ARGOT_B200_API int argot_b200_art_rates(const argot_b200_art *a, const argot_b20
  * rank: the caller's angle table and step factors (hd_param, filled by its
  * setup_diffuse_photon), the mesh of cuda_mem[0].mesh_dev, whose
  * prev_chem.{Gamma,Heat}{HI,HeI,HeII} receive the diffuse rates (added).
- * mesh, cd_param and this_omp are not used. */
+ * mesh, cd_param and this_omp are not used.  Exported by the builds for
+ * helium without H2 or the scale factor only. */
 struct host_diffuse_param;
 struct cuda_diffuse_param;
 ARGOT_B200_API void calc_diffuse_photon_radiation(struct fluid_mesh *mesh, struct run_param *this_run,

@@ -8,6 +8,11 @@
    reference-GPU baseline of the benchmark.
 3. The restatement (``oracle/argot_oracle.c``, ref-order FP32/FP64 functions and
    the FP64 precision oracle) into ``oracle/_build/libargot_oracle.so``.
+4. O1 for ARGOT's other flag sets (``build_ref_flags``: the hot-path sources
+   with the stock ``-D__HYDROGEN_MOL__`` set, helium + H2, no photon
+   conservation, the scale factor, hydrogen only; driver
+   ``oracle/ref_flags_driver.c``) into
+   ``oracle/_ref/libargot_ref_flags_<tag>_n16.so``.
 
 Both directories are git-ignored; the built libraries travel with the working
 tree.  Nothing in the product path (the ``argot_b200`` package) loads them.
@@ -168,6 +173,57 @@ def build_ref(edge: int, ref: str = DEFAULT_REF, fast_math: bool = False,
     return out
 
 
+# the hot-path sources a flag-set build needs (the rays are made by the test)
+FLAG_SOURCES = ["calc_optical_depth.c", "calc_photoion_rate.c", "source.c", "cross_section.c",
+                "prim_chem/cross_section.c", "mpi_rank.c", "timing.c", "smooth_photoion_rate.c"]
+# tag -> the reference flags of the flag sets the library is also built for
+# (argot_b200/build.py FLAGSETS); every build is -D__ISOLATED__, as the
+# reference Makefile's default
+REF_FLAGSETS = {
+    "h2_pc": ["-D__HYDROGEN_MOL__", "-D__PHOTON_CONSERVING__"],
+    "he_h2_pc": ["-D__HELIUM__", "-D__HYDROGEN_MOL__", "-D__PHOTON_CONSERVING__"],
+    "he": ["-D__HELIUM__"],
+    "he_pc_cosmo": ["-D__HELIUM__", "-D__PHOTON_CONSERVING__", "-D__COSMOLOGICAL__"],
+    "hi": [],
+}
+
+
+def ref_flags_lib_path(tag: str, edge: int) -> str:
+    return os.path.join(REF_OUT, f"libargot_ref_flags_{tag}_n{edge}.so")
+
+
+def build_ref_flags(tag: str, edge: int = 16, ref: str = DEFAULT_REF, verbose: bool = False) -> str:
+    """ARGOT's own calc_optical_depth.c / calc_photoion_rate.c /
+    smooth_photoion_rate.c and their tables, compiled unmodified with the
+    flag set REF_FLAGSETS[tag] (plus -D__RADIATION_TRANSFER__
+    -D__ARGOT_PROFILE__ -D__ISOLATED__) and ref_flags_driver.c into
+    oracle/_ref/libargot_ref_flags_<tag>_n<EDGE>.so."""
+    src_dir = os.path.join(ref, "src")
+    if not os.path.isdir(src_dir):
+        raise FileNotFoundError(f"reference sources not found at {src_dir}")
+    inc = os.path.join(REF_OUT, f"inc_{edge}")
+    os.makedirs(inc, exist_ok=True)
+    with open(os.path.join(src_dir, "run_param.h")) as f:
+        text = patched_run_param(f.read(), edge)
+    with open(os.path.join(inc, "run_param.h"), "w") as f:
+        f.write(text)
+    out = ref_flags_lib_path(tag, edge)
+    cmd = [_cc(), "-O2", "-std=gnu99", "-fgnu89-inline", "-fopenmp", "-fPIC", "-shared", "-w",
+           "-fno-strict-aliasing", "-ffp-contract=off", *REF_FLAGSETS[tag],
+           "-D__RADIATION_TRANSFER__", "-D__ARGOT_PROFILE__", "-D__HEATCOOL__", "-D__ISOLATED__",
+           "-I" + inc, "-I-", "-I" + os.path.join(HERE, "shim"),
+           "-I" + src_dir, "-I" + os.path.join(src_dir, "prim_chem")]
+    cmd += [os.path.join(src_dir, s) for s in FLAG_SOURCES]
+    cmd += [os.path.join(HERE, "ref_flags_driver.c"), "-o", out, "-lm", "-Wl,--no-undefined"]
+    if verbose:
+        print(" ".join(cmd))
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stderr)
+        raise subprocess.CalledProcessError(r.returncode, cmd)
+    return out
+
+
 def refgpu_lib_path(edge: int) -> str:
     return os.path.join(REF_OUT, f"libargot_refgpu_n{edge}.so")
 
@@ -264,6 +320,8 @@ def build_all(edges=EDGES, ref: str = DEFAULT_REF, verbose: bool = False):
         built.append(build_ref(64, ref, True, verbose))
         built.append(build_ref(16, ref, False, verbose, isolated=True))
         built.append(build_ref(32, ref, False, verbose, isolated=True))
+        for tag in REF_FLAGSETS:
+            built.append(build_ref_flags(tag, 16, ref, verbose))
         import concurrent.futures as cf
         with cf.ThreadPoolExecutor(max_workers=min(len(GPU_EDGES), os.cpu_count() or 1)) as ex:
             built += list(ex.map(lambda e: build_ref_gpu(e, ref, verbose), GPU_EDGES))

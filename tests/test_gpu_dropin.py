@@ -30,6 +30,16 @@ def _run_param(edge, lunit, denstonh, nseg=0, nray=0):
         setattr(r, f"delta_{a}", float(np.float32(1.0) / np.float32(edge)))
     r.nseg, r.nray = nseg, nray
     r.theta_crit = 0.5
+    # the tables the caller's setup_freq_param / setup_cross_section fill
+    # (source.c:38-53, cross_section.c:5-22); the drop-in reads them
+    from argot_b200 import _lib as L
+    nu = np.zeros(256)
+    cs3 = np.zeros(3 * 256, np.float32)
+    L.load().argot_b200_tables(nu.ctypes.data, cs3.ctypes.data)
+    r.freq.log_nu_min, r.freq.log_nu_max, r.freq.dlog_nu = 0.0, 1.5, 1.5 / 256.0
+    for i in range(256):
+        r.freq.nu[i] = nu[i]
+        r.csect[i].csect_HI, r.csect[i].csect_HeI, r.csect[i].csect_HeII = cs3[3 * i:3 * i + 3]
     return r
 
 
