@@ -327,12 +327,34 @@ struct RateWarpSmem {
   float out[32][6];  // per-ray rates
   int e[32], t[32];  // emitter, target lane
   int nsfu[32];      // iterations of the bin loop that may need the SFU path (sfu_iters)
+  float acc[12][32]; // per target lane: Kahan sums and compensations (CellSum6Smem)
   int q[32];         // lanes of the chunk's rays that take the quadrature
   int cnt[32], src[32];  // per target lane: rays of the chunk, ray of the round
 };
 
 // A cell's six rates summed over its rays in ray order, FP32 with Kahan
-// compensation (a cell receives up to a few hundred rays).
+// compensation (a cell receives up to a few hundred rays).  CellSum6 keeps
+// the sums in registers; CellSum6Smem in the warp's shared memory (word
+// [q][lane], conflict-free), which frees twelve registers across the bin
+// loop of the rate kernel.
+struct CellSum6Smem {
+  float (*a)[32];
+  int lane;
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int q = 0; q < 12; q++) a[q][lane] = 0.f;
+  }
+  __device__ __forceinline__ void add(const float *v) {
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      float s = a[q][lane], c = a[6 + q][lane];
+      kahan_add(s, c, v[q]);
+      a[q][lane] = s;
+      a[6 + q][lane] = c;
+    }
+  }
+  __device__ __forceinline__ float sum(int q) const { return a[q][lane]; }
+};
 struct CellSum6 {
   float s[6], c[6];
   __device__ __forceinline__ void zero() {
@@ -343,6 +365,7 @@ struct CellSum6 {
 #pragma unroll
     for (int q = 0; q < 6; q++) kahan_add(s[q], c[q], v[q]);
   }
+  __device__ __forceinline__ float sum(int q) const { return s[q]; }
 };
 
 // Phase C of the block-rate kernels: lane k holds ray k of a chunk (its six
@@ -351,8 +374,9 @@ struct CellSum6 {
 // among the chunk's rays with the same target; round r hands every cell
 // its rank-r ray through `src`, so a chunk whose rays end in distinct cells
 // takes one round (instead of every lane scanning the chunk's 32 rays).
-__device__ __forceinline__ void add_chunk_in_order(CellSum6 &acc, int lane, int t, const float (*out)[6],
-                                                   int *cnt, int *src) {
+template <class Acc>
+__device__ __forceinline__ void add_chunk_in_order(Acc &acc, int lane, int t, const float (*out)[6], int *cnt,
+                                                   int *src) {
   const unsigned same = __match_any_sync(0xffffffffu, t);
   const int rank = __popc(same & ((1u << lane) - 1u));
   cnt[lane] = 0;
@@ -393,7 +417,7 @@ __device__ __forceinline__ void rate_block_f32(const GridDev &g, const float4 *_
   int ix, iy, iz;
   const bool own_valid = block_cell(g, b, lane, &ix, &iy, &iz);
   const uint64_t own = own_valid ? cell_index(g, ix, iy, iz) : 0;
-  CellSum6 acc;
+  CellSum6Smem acc{S.acc, lane};
   acc.zero();
   int bix, biy, biz;
   block_cell(g, b, 0, &bix, &biy, &biz);
@@ -465,7 +489,7 @@ __device__ __forceinline__ void rate_block_f32(const GridDev &g, const float4 *_
   }
   if (own_valid) {
 #pragma unroll
-    for (int s = 0; s < 6; s++) rates6[s * ncell + own] = acc.s[s];
+    for (int s = 0; s < 6; s++) rates6[s * ncell + own] = acc.sum(s);
   }
 }
 
