@@ -1,6 +1,7 @@
 // surrogate.cu -- per-cell rates with the BF16 MLP surrogate of the
-// frequency integral, evaluated on the tensor cores, and the exact FP32
-// quadrature as fallback.
+// frequency integral, evaluated on the fifth-generation tensor cores
+// (tcgen05: operands in shared memory, fp32 accumulators in TMEM), and the
+// exact FP32 quadrature as fallback.
 //
 // Photon-conserving cell factor.  For every frequency
 //   e^{-tau} (1 - e^{-dtau}) / dtau = int_0^1 e^{-(tau + u dtau)} du,
@@ -35,6 +36,7 @@
 
 #include "mlp.cuh"
 #include "photoion.cuh"
+#include "umma.cuh"
 
 namespace argot {
 
@@ -50,147 +52,213 @@ constexpr float kEnvQLo = -7.0f;     // ... in [-7, 0]
 constexpr int kHistBins = 64;        // half-octave bins of a ray's budget share
 constexpr float kGLErr = 4e-5f;      // relative error of the Gauss-Legendre cell factor
 constexpr int kWorkPlanes = 7;       // c_0..c_5, eps per ray
-constexpr int kSurWarps = 4;
-constexpr int kMaxEval = 96;  // 32 rays x 3 quadrature nodes
+constexpr int kSurWarps = 8;   // warps of the predict kernel: a tile's 128 rows x two column halves
+constexpr int kSelWarps = 4;   // warps of the select kernel
+constexpr int kMaxEval = 96;   // 32 rays x 3 quadrature nodes
+constexpr int kTile = 128;     // network evaluations per tensor-core tile (MMA M)
 
-// B-fragments of the four layers (mma.m16n8k16, BF16), biases, envelope.
-struct SurWeights {
-  uint2 f1[8][32];        // layer 1: 8 N-tiles x 1 K-step (input hi|lo in k 0..7)
-  uint2 f2[8][4][32];     // layer 2: 8 N-tiles x 4 K-steps
-  uint2 f3[8][4][32];     // layer 3
-  uint2 f4[8][32];        // layer 4: 1 N-tile x 8 K-steps (hidden hi | lo)
-  float b1[64], b2[64], b3[64], b4[8];
-  float env[6][kEnvBins]; // e^dq - 1, dq the bound of |error of q| per output and bin of q^
+// The network in the operand layout of the tensor cores (umma.cuh: BF16,
+// K-major, no swizzle), built on the host, copied to shared memory as it is:
+//   layer 1: N = 64, K = 16 (k 0..3 the inputs' BF16 high parts, 4..7 their
+//            low parts, both against W1, 8..15 zero);
+//   layers 2, 3: N = 64, K = 64 (the activations enter as a BF16 pair
+//            hi + lo: two MMA chains against the same weights);
+//   layer 4: N = 16 (outputs 0..5, the rest zero), K = 64, hi and lo.
+// Every activation therefore carries 16 mantissa bits into the tensor
+// cores; the weights are single BF16 values (the network is trained with
+// them rounded).
+struct TcNet {
+  uint16_t b1[64 * 16];
+  uint16_t b2[64 * 64];
+  uint16_t b3[64 * 64];
+  uint16_t b4[16 * 64];
+  float bias1[64], bias2[64], bias3[64], bias4[16];
+  float env[6][kEnvBins];  // e^dq - 1, dq the bound of |error of q| per output and bin of q^
   float sig0[3];
-  float tol;              // per-cell relative error budget
+  float tol;               // per-cell relative error budget
+};
+static_assert(sizeof(TcNet) % 16 == 0, "TcNet copies in 16-byte words");
+
+// Operand tiles of one 128-row tile and the tensor-core bookkeeping.
+struct TcTile {
+  uint16_t a1[kTile * 16];   // layer-1 inputs
+  uint16_t ahi[kTile * 64];  // activations, BF16 high parts
+  uint16_t alo[kTile * 64];  // ... and low parts
+  uint64_t bar;              // MMA completion
+  uint32_t tmem;             // TMEM base of the fp32 accumulator (64 columns)
+  uint32_t phase;            // parity of the next completion of bar
 };
 
-struct PredSmem {
-  SurWeights w;
-  // per warp
-  float x[kSurWarps][kMaxEval][4];     // normalised network inputs
-  float tout[kSurWarps][kMaxEval][6];  // network outputs q_j
-  float c[kSurWarps][32][6];           // predicted per-ray contributions
-  int t[kSurWarps][32];
-};
-
-struct SelSmem {
-  // per warp
-  float Sc[kSurWarps][32][6];                // lower bounds of the cell totals
-  unsigned hist[kSurWarps][32][kHistBins];   // budget-share histogram per cell
-  int thr[kSurWarps][32];                    // last accepted bin per cell
-};
+constexpr uint32_t kWaitPolls = 1u << 22;  // bound of one MMA wait (far above a microsecond MMA)
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
   const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<const uint32_t *>(&v);
 }
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint2 b) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b.x), "r"(b.y));
-}
-
-// x -> BF16 pair (hi, lo) with hi + lo = x to 16 mantissa bits, packed two
-// values per register as the mma fragments want them.
-__device__ __forceinline__ void split_bf16x2(float x0, float x1, uint32_t *hi, uint32_t *lo) {
-  const float h0 = bf16_round(x0), h1 = bf16_round(x1);
-  *hi = pack_bf16x2(h0, h1);
-  *lo = pack_bf16x2(x0 - h0, x1 - h1);
-}
-
-// SiLU of the 8 accumulator values of two N-tiles, in fragment order (the
-// single-precision hardware tanh: a packed half-precision tanh was measured
-// no faster here and less accurate).
-__device__ __forceinline__ void silu8(const float (&a)[4], const float (&b)[4], float (&s)[8]) {
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-    s[i] = silu_acc(a[i]);
-    s[4 + i] = silu_acc(b[i]);
-  }
-}
-
-// The network on 16 evaluations (rows r0..r0+15 of the warp's list).  The
-// m16n8 accumulator of one layer is, register for register, the A fragment
-// of the next (N-tiles 2kk, 2kk+1 -> K-step kk), so activations never leave
-// the registers.
-__device__ __forceinline__ void mlp_tile16(const SurWeights &W, const float (*x)[4], float (*tout)[6],
-                                           int r0, int lane) {
-  const int g = lane >> 2, tq = lane & 3;
-  // layer 1: A = [hi(x) | lo(x) | 0] (k = 0..3 | 4..7 | 8..15)
-  uint32_t a[4];
-  {
-    const int c0 = (2 * tq) & 3;  // columns 2tq, 2tq+1 of the 8 used
-    const bool lo = tq >= 2;
-    float v[4];
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const float *xr = x[r0 + g + 8 * h];
-      const float x0 = xr[c0], x1 = xr[c0 + 1];
-      const float h0 = bf16_round(x0), h1 = bf16_round(x1);
-      v[2 * h + 0] = lo ? x0 - h0 : h0;
-      v[2 * h + 1] = lo ? x1 - h1 : h1;
+// The tensor-core thread of the CTA issues one layer and everyone waits for
+// it: A rows from `a` (row stride of a K-major tile of 128 rows), `ksteps`
+// K-steps of 16 over `a`, then (if `a2`) the same over `a2`, against B with
+// its own LBO; fp32 result in TMEM columns [0, n).  Returns false (for the
+// whole CTA) when the completion did not arrive in time; then nothing more
+// is issued.
+__device__ __forceinline__ bool tc_layer(TcTile &T, const uint16_t *a, const uint16_t *a2, const uint16_t *b,
+                                         int ksteps, uint32_t b_lbo, int n, bool ok) {
+  if (ok && threadIdx.x == 0) {
+    umma::fence_after_sync();
+    const uint32_t id = umma::idesc_bf16(kTile, n);
+    const uint32_t a_lbo = (kTile / 8) * 128;
+    int step = 0;
+    for (int pass = 0; pass < (a2 ? 2 : 1); pass++) {
+      const uint32_t ab = umma::smem_addr(pass ? a2 : a), bb = umma::smem_addr(b);
+      for (int s = 0; s < ksteps; s++, step++)
+        umma::mma_bf16(T.tmem, umma::smem_desc(ab + 2 * s * a_lbo, a_lbo, 128),
+                       umma::smem_desc(bb + 2 * s * b_lbo, b_lbo, 128), id, step > 0);
     }
-    a[0] = pack_bf16x2(v[0], v[1]);
-    a[1] = pack_bf16x2(v[2], v[3]);
-    a[2] = 0u;
-    a[3] = 0u;
+    umma::commit(&T.bar);
   }
-  float acc[8][4];
-#pragma unroll
-  for (int j = 0; j < 8; j++) {
-    const float bb0 = W.b1[8 * j + 2 * tq], bb1 = W.b1[8 * j + 2 * tq + 1];
-    acc[j][0] = bb0; acc[j][1] = bb1; acc[j][2] = bb0; acc[j][3] = bb1;
-    mma_bf16(acc[j], a, W.f1[j][lane]);
+  bool done = true;
+  if (ok) {
+    done = umma::mbar_wait(&T.bar, T.phase, kWaitPolls);
+    umma::fence_after_sync();
   }
-  // layers 2 and 3: each activation as a BF16 pair hi + lo, both against
-  // the same weight fragment
+  ok = __syncthreads_and(ok && done);
+  if (threadIdx.x == 0) T.phase ^= 1u;
+  return ok;
+}
+
+// Epilogue of a hidden layer: thread (warp w, lane) takes row 32 (w % 4) +
+// lane and columns [32 h, 32 h + 32), h = w / 4: the accumulator plus
+// bias, SiLU, split into BF16 hi + lo, stored as the next layer's A.
+__device__ __forceinline__ void tc_hidden_epilogue(TcTile &T, const float *__restrict__ bias, bool ok) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = 32 * (w & 3) + lane, h = w >> 2;
+  if (ok) {
 #pragma unroll
-  for (int layer = 0; layer < 2; layer++) {
-    uint32_t Ah[4][4], Al[4][4];
+    for (int cc = 0; cc < 2; cc++) {
+      const int k0 = 32 * h + 16 * cc;
+      float v[16];
+      umma::tmem_ld16(T.tmem + ((uint32_t)(32 * (w & 3)) << 16) + (uint32_t)k0, v);
+      uint32_t hi[8], lo[8];
 #pragma unroll
-    for (int kk = 0; kk < 4; kk++) {
-      float s[8];
-      silu8(acc[2 * kk], acc[2 * kk + 1], s);
-#pragma unroll
-      for (int q = 0; q < 4; q++) split_bf16x2(s[2 * q], s[2 * q + 1], &Ah[kk][q], &Al[kk][q]);
-    }
-    const float *bias = layer == 0 ? W.b2 : W.b3;
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const float bb0 = bias[8 * j + 2 * tq], bb1 = bias[8 * j + 2 * tq + 1];
-      acc[j][0] = bb0; acc[j][1] = bb1; acc[j][2] = bb0; acc[j][3] = bb1;
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) {
-        const uint2 bf = layer == 0 ? W.f2[j][kk][lane] : W.f3[j][kk][lane];
-        mma_bf16(acc[j], Ah[kk], bf);
-        mma_bf16(acc[j], Al[kk], bf);
+      for (int i = 0; i < 8; i++) {
+        const float s0 = silu_acc(v[2 * i] + bias[k0 + 2 * i]);
+        const float s1 = silu_acc(v[2 * i + 1] + bias[k0 + 2 * i + 1]);
+        const float h0 = bf16_round(s0), h1 = bf16_round(s1);
+        hi[i] = pack_bf16x2(h0, h1);
+        lo[i] = pack_bf16x2(s0 - h0, s1 - h1);
       }
+      // two 8-element K chunks per 16 columns
+      *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(T.ahi) + umma::kmajor_offset(kTile, row, k0)) =
+          make_uint4(hi[0], hi[1], hi[2], hi[3]);
+      *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(T.ahi) + umma::kmajor_offset(kTile, row, k0 + 8)) =
+          make_uint4(hi[4], hi[5], hi[6], hi[7]);
+      *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(T.alo) + umma::kmajor_offset(kTile, row, k0)) =
+          make_uint4(lo[0], lo[1], lo[2], lo[3]);
+      *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(T.alo) + umma::kmajor_offset(kTile, row, k0 + 8)) =
+          make_uint4(lo[4], lo[5], lo[6], lo[7]);
     }
   }
-  // layer 4 on the last hidden layer split as hi | lo
-  float o[4] = {W.b4[2 * tq], W.b4[2 * tq + 1], W.b4[2 * tq], W.b4[2 * tq + 1]};
-#pragma unroll
-  for (int kk = 0; kk < 4; kk++) {
-    float s[8];
-    silu8(acc[2 * kk], acc[2 * kk + 1], s);
-    uint32_t hi[4], lo[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) split_bf16x2(s[2 * q], s[2 * q + 1], &hi[q], &lo[q]);
-    mma_bf16(o, hi, W.f4[kk][lane]);
-    mma_bf16(o, lo, W.f4[4 + kk][lane]);
-  }
-  if (tq < 3) {
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      tout[r0 + g + 8 * h][2 * tq] = fmaf(o[2 * h], kOutScale, kOutShift);
-      tout[r0 + g + 8 * h][2 * tq + 1] = fmaf(o[2 * h + 1], kOutScale, kOutShift);
-    }
-  }
+  // the TMEM reads complete before the next MMA overwrites the columns,
+  // the shared-memory writes are visible to the tensor cores
+  umma::fence_before_sync();
+  umma::fence_smem_to_async();
+  __syncthreads();
 }
+
+// The network on one tile of up to 128 evaluations.  load(row, x[4]) gives
+// the normalised inputs of tile row `row` (called for row < nrows by the
+// threads of warps 0..3, thread = row); put(row, q[6]) receives the outputs
+// q_j (same threads).  All threads of the CTA call it; `ok` is CTA-uniform.
+template <class Load, class Put>
+__device__ __forceinline__ bool mlp_tile_tc(const TcNet &W, TcTile &T, int nrows, Load load, Put put, bool ok) {
+  const int tid = threadIdx.x, w = tid >> 5;
+  if (w < 4) {
+    const int row = tid;
+    float x[4] = {0.f, 0.f, 0.f, 0.f};
+    if (row < nrows) load(row, x);
+    float h[4], l[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      h[c] = bf16_round(x[c]);
+      l[c] = x[c] - h[c];
+    }
+    // K chunk 0: hi | lo; chunk 1 stays zero (written once)
+    *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(T.a1) + umma::kmajor_offset(kTile, row, 0)) =
+        make_uint4(pack_bf16x2(h[0], h[1]), pack_bf16x2(h[2], h[3]), pack_bf16x2(l[0], l[1]),
+                   pack_bf16x2(l[2], l[3]));
+  }
+  umma::fence_before_sync();
+  umma::fence_smem_to_async();
+  __syncthreads();
+  ok = tc_layer(T, T.a1, nullptr, W.b1, 1, (64 / 8) * 128, 64, ok);
+  tc_hidden_epilogue(T, W.bias1, ok);
+  ok = tc_layer(T, T.ahi, T.alo, W.b2, 4, (64 / 8) * 128, 64, ok);
+  tc_hidden_epilogue(T, W.bias2, ok);
+  ok = tc_layer(T, T.ahi, T.alo, W.b3, 4, (64 / 8) * 128, 64, ok);
+  tc_hidden_epilogue(T, W.bias3, ok);
+  ok = tc_layer(T, T.ahi, T.alo, W.b4, 4, (16 / 8) * 128, 16, ok);
+  if (ok && w < 4) {
+    float v[16];
+    umma::tmem_ld16(T.tmem + ((uint32_t)(32 * w) << 16), v);
+    if (tid < nrows) {
+      float q[6];
+#pragma unroll
+      for (int j = 0; j < 6; j++) q[j] = fmaf(v[j] + W.bias4[j], kOutScale, kOutShift);
+      put(tid, q);
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  return ok;
+}
+
+// Set-up of the tensor-core state of a CTA: the network image into shared
+// memory, TMEM (warp 0), the mbarrier, the constant zero chunk of layer 1.
+__device__ __forceinline__ void tc_setup(const TcNet *__restrict__ g_net, TcNet &W, TcTile &T) {
+  {
+    const uint4 *src = reinterpret_cast<const uint4 *>(g_net);
+    uint4 *dst = reinterpret_cast<uint4 *>(&W);
+    for (int i = threadIdx.x; i < (int)(sizeof(TcNet) / 16); i += blockDim.x) dst[i] = src[i];
+  }
+  for (int r = threadIdx.x; r < kTile; r += blockDim.x)
+    *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(T.a1) + umma::kmajor_offset(kTile, r, 8)) =
+        make_uint4(0u, 0u, 0u, 0u);
+  if (threadIdx.x < 32) umma::tmem_alloc(&T.tmem, 64);
+  if (threadIdx.x == 0) {
+    umma::mbar_init(&T.bar, 1);
+    T.phase = 0;
+  }
+  umma::fence_before_sync();
+  umma::fence_smem_to_async();
+  __syncthreads();
+  umma::fence_after_sync();
+}
+
+__device__ __forceinline__ void tc_teardown(TcTile &T) {
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  if (threadIdx.x < 32) umma::tmem_dealloc(T.tmem, 64);
+}
+
+struct PredSmem {
+  TcNet w;
+  TcTile tile;
+  // per warp
+  float x[kSurWarps][kMaxEval][4];     // normalised network inputs
+  float tout[kSurWarps][kMaxEval][6];  // network outputs q_j
+  float c[kSurWarps][32][6];           // predicted per-ray contributions
+  int t[kSurWarps][32];
+  int nev[kSurWarps];                  // evaluations of the warp's chunk this round
+};
+
+struct SelSmem {
+  // per warp
+  float Sc[kSelWarps][32][6];                // lower bounds of the cell totals
+  unsigned hist[kSelWarps][32][kHistBins];   // budget-share histogram per cell
+  int thr[kSelWarps][32];                    // last accepted bin per cell
+};
 
 // Gauss-Legendre nodes and weights on [0, 1]
 __device__ __forceinline__ void gl_node(int n, int i, float *u, float *w) {
@@ -236,54 +304,74 @@ __device__ __forceinline__ RayTask ray_task(const GridDev &g, const float4 *__re
 // bins of predicted q, times a safety factor), so with y^ = ylin e^q^,
 // |y - y^| <= |y^| (e^dq - 1) = x and |I - I^| <= I^ (e^x - 1) <= I^ x e^x;
 // the node bounds add up over the nodes.
-// Launch shapes: kSurWarps warps per CTA, at least ARGOT_SUR_PREDICT_MIN_CTAS
-// and ARGOT_SUR_FINISH_MIN_CTAS CTAs resident per SM (register caps).
+// The kernel runs in rounds: in each round every warp of the CTA takes the
+// next chunk of 32 rays of its target blocks (blocks b0 + warp, + nwarp,
+// ...), forms their quadrature nodes' network inputs, and the CTA's tensor
+// cores evaluate all the round's evaluations in tiles of 128 (the 8 warps'
+// lists concatenated); then every warp turns its outputs into contributions,
+// bounds and per-cell lower bounds.  A warp without work left takes part in
+// the CTA's barriers only.
+// Launch shape: kSurWarps warps per CTA, at least ARGOT_SUR_PREDICT_MIN_CTAS
+// CTAs resident per SM.
 #ifndef ARGOT_SUR_PREDICT_MIN_CTAS
-#define ARGOT_SUR_PREDICT_MIN_CTAS 4
-#endif
-#ifndef ARGOT_SUR_FINISH_MIN_CTAS
-#define ARGOT_SUR_FINISH_MIN_CTAS 1
+#define ARGOT_SUR_PREDICT_MIN_CTAS 2
 #endif
 __global__ void __launch_bounds__(32 * kSurWarps, ARGOT_SUR_PREDICT_MIN_CTAS)
     k_sur_predict(GridDev g, const float4 *__restrict__ raw, const float4 *__restrict__ emit_pos,
                   const double *__restrict__ total, const float *__restrict__ emit_logT,
                   const double *__restrict__ emit_i0, const float *__restrict__ emit_m,
-                  const SurWeights *__restrict__ wts, uint64_t b0, uint64_t b1, const uint64_t *__restrict__ blk_off,
+                  const TcNet *__restrict__ net, uint64_t b0, uint64_t b1, const uint64_t *__restrict__ blk_off,
                   uint64_t base, const uint32_t *__restrict__ rays, uint64_t nray, const float *__restrict__ tau,
                   float *__restrict__ rates6, float *__restrict__ work, int *__restrict__ err) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
   PredSmem &S = *reinterpret_cast<PredSmem *>(smem_raw);
-  {
-    const uint32_t *src = reinterpret_cast<const uint32_t *>(wts);
-    uint32_t *dst = reinterpret_cast<uint32_t *>(&S.w);
-    for (int i = threadIdx.x; i < (int)(sizeof(SurWeights) / 4); i += blockDim.x) dst[i] = src[i];
-  }
-  __syncthreads();
+  tc_setup(net, S.w, S.tile);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const float s00 = c_tab.cs[0][0];
   const float s0a = c_tab.cs[0][44], s1a = c_tab.cs[1][44];
   const float s0b = c_tab.cs[0][103], s1b = c_tab.cs[1][103], s2b = c_tab.cs[2][103];
-  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarp = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t nwarp = (uint64_t)gridDim.x * kSurWarps;
   const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
   const float kInf = __int_as_float(0x7f800000);
-  for (uint64_t b = b0 + warp; b < b1; b += nwarp) {
-    int ix, iy, iz;
-    const bool own_valid = block_cell(g, b, lane, &ix, &iy, &iz);
-    const uint64_t own = own_valid ? cell_index(g, ix, iy, iz) : 0;
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    int bix, biy, biz;
-    block_cell(g, b, 0, &bix, &biy, &biz);
-    uint64_t r0, r1;
-    if (!block_rays(blk_off, b, base, nray, &r0, &r1)) {
-      if (lane == 0) atomicExch(err, 1);
-      continue;
+  // this warp's position: block b, chunk start rc in [r0, r1)
+  uint64_t b = b0 + (uint64_t)blockIdx.x * kSurWarps + wib;
+  uint64_t r0 = 0, r1 = 0, rc = 0;
+  int bix = 0, biy = 0, biz = 0;
+  bool own_valid = false;
+  uint64_t own = 0;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  // the first block with rays at or after b (blocks with bad offsets are
+  // reported and skipped; blocks without rays get a zero lower bound)
+  auto open_block = [&]() {
+    for (; b < b1; b += nwarp) {
+      int ix, iy, iz;
+      own_valid = block_cell(g, b, lane, &ix, &iy, &iz);
+      own = own_valid ? cell_index(g, ix, iy, iz) : 0;
+      block_cell(g, b, 0, &bix, &biy, &biz);
+      if (!block_rays(blk_off, b, base, nray, &r0, &r1)) {
+        if (lane == 0) atomicExch(err, 1);
+        continue;
+      }
+      if (r0 < r1) break;
+      if (own_valid) {
+#pragma unroll
+        for (int s = 0; s < 6; s++) rates6[s * ncell + own] = 0.f;
+      }
     }
-    for (uint64_t rc = r0; rc < r1; rc += 32) {
-      // ---- phase A: per-ray parameters and quadrature nodes
-      const uint64_t r = rc + lane;
-      int tl = -1, nq = 0, e = 0;
-      RayParams p;
+    rc = r0;
+#pragma unroll
+    for (int s = 0; s < 6; s++) acc[s] = 0.0;
+  };
+  open_block();
+  bool ok = true;
+  for (;;) {
+    const bool active = b < b1;
+    if (!__syncthreads_or(active)) break;
+    // ---- phase A: per-ray parameters and quadrature nodes of the chunk
+    const uint64_t r = rc + lane;
+    int tl = -1, nq = 0, e = 0, pos = 0;
+    RayParams p;
+    if (active) {
       float xin[3][4];
       if (r < r1) {
         const RayTask t = ray_task(g, raw, emit_pos, total, rays, tau, nray, r, bix, biy, biz);
@@ -312,8 +400,8 @@ __global__ void __launch_bounds__(32 * kSurWarps, ARGOT_SUR_PREDICT_MIN_CTAS)
           xin[i][3] = (lT - 0.5f * (kTLo + kTHi)) * (2.f / (kTHi - kTLo));
         }
       }
-      // exclusive scan of the node counts -> positions in the evaluation list
-      int pos = nq;
+      // exclusive scan of the node counts -> positions in the warp's list
+      pos = nq;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
         const int v = __shfl_up_sync(0xffffffffu, pos, o);
@@ -325,20 +413,50 @@ __global__ void __launch_bounds__(32 * kSurWarps, ARGOT_SUR_PREDICT_MIN_CTAS)
 #pragma unroll
         for (int c = 0; c < 4; c++) S.x[wib][pos + i][c] = xin[i][c];
       S.t[wib][lane] = tl;
-      // pad the last tile with valid inputs
-      for (int q = nev + lane; q < ((nev + 15) & ~15); q += 32)
+      if (lane == 0) S.nev[wib] = nev;
+    } else if (lane == 0) {
+      S.nev[wib] = 0;
+    }
+    __syncthreads();
+    // ---- phase B: the round's evaluations on the tensor cores
+    int start[kSurWarps + 1];
+    start[0] = 0;
 #pragma unroll
-        for (int c = 0; c < 4; c++) S.x[wib][q][c] = 0.f;
-      __syncwarp();
-      // ---- phase B: the network on the tensor cores
-      for (int r16 = 0; r16 < nev; r16 += 16) mlp_tile16(S.w, S.x[wib], S.tout[wib], r16, lane);
-      __syncwarp();
+    for (int k = 0; k < kSurWarps; k++) start[k + 1] = start[k] + S.nev[k];
+    const int total_ev = start[kSurWarps];
+    for (int t0 = 0; t0 < total_ev; t0 += kTile) {
+      // tile row -> (warp, index in its list)
+      auto where = [&](int row, int &wk, int &ik) {
+        const int gi = t0 + row;
+        wk = 0;
+#pragma unroll
+        for (int k = 1; k < kSurWarps; k++) wk += gi >= start[k];
+        ik = gi - start[wk];
+      };
+      ok = mlp_tile_tc(
+          S.w, S.tile, min(kTile, total_ev - t0),
+          [&](int row, float(&x)[4]) {
+            int wk, ik;
+            where(row, wk, ik);
+#pragma unroll
+            for (int c = 0; c < 4; c++) x[c] = S.x[wk][ik][c];
+          },
+          [&](int row, const float(&q)[6]) {
+            int wk, ik;
+            where(row, wk, ik);
+#pragma unroll
+            for (int j = 0; j < 6; j++) S.tout[wk][ik][j] = q[j];
+          },
+          ok);
+    }
+    // (the tile's last barrier orders the outputs before their readers)
+    if (active) {
       // ---- phase C: predicted contributions and their error bound
       if (tl >= 0) {
         float cj[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         float low[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // lower-bound factor of each c_j
         float eps = kInf;
-        if (nq > 0) {
+        if (nq > 0 && ok) {
           float mj[18];
 #pragma unroll
           for (int k = 0; k < 18; k++) mj[k] = __ldg(emit_m + 18 * (size_t)e + k);
@@ -399,12 +517,20 @@ __global__ void __launch_bounds__(32 * kSurWarps, ARGOT_SUR_PREDICT_MIN_CTAS)
         }
       }
       __syncwarp();
-    }
-    if (own_valid) {
+      // next chunk, or the block's lower bounds and the next block
+      rc += 32;
+      if (rc >= r1) {
+        if (own_valid) {
 #pragma unroll
-      for (int s = 0; s < 6; s++) rates6[s * ncell + own] = (float)acc[s];
+          for (int s = 0; s < 6; s++) rates6[s * ncell + own] = (float)acc[s];
+        }
+        b += nwarp;
+        open_block();
+      }
     }
   }
+  if (!ok && threadIdx.x == 0) atomicExch(err, 1);
+  tc_teardown(S.tile);
 }
 
 // Histogram bin of a ray's share of its cell's error budget,
@@ -440,7 +566,7 @@ __device__ __forceinline__ double beta_edge(int b) { return exp2(0.5 * (double)(
 // to 1, every other ray's to 0.  Kernel 3, the FP32 rate kernel
 // (rate_block_f32<true>), then runs the exact quadrature for the flagged-0
 // rays only, at its own occupancy, and sums every cell in ray order.
-__global__ void __launch_bounds__(32 * kSurWarps)
+__global__ void __launch_bounds__(32 * kSelWarps)
     k_sur_select(GridDev g, float tol, uint64_t b0, uint64_t b1, const uint64_t *__restrict__ blk_off, uint64_t base,
                  const uint32_t *__restrict__ rays, uint64_t nray, const float *__restrict__ rates6,
                  float *__restrict__ work, unsigned long long *__restrict__ counters, int *__restrict__ err) {
@@ -513,45 +639,46 @@ __global__ void __launch_bounds__(32 * kSurWarps)
   }
 }
 
-// The network on a list of raw inputs (log10 tau x3, log10 T), one warp per
-// 16 evaluations, with the inference numerics of k_rate_sur.
-__global__ void __launch_bounds__(128) k_sur_eval(const SurWeights *__restrict__ wts, const float *__restrict__ X,
-                                                  int n, float *__restrict__ T) {
-  __shared__ SurWeights W;
-  __shared__ float xs[4][16][4];
-  __shared__ float ts[4][16][6];
-  {
-    const uint32_t *src = reinterpret_cast<const uint32_t *>(wts);
-    uint32_t *dst = reinterpret_cast<uint32_t *>(&W);
-    for (int i = threadIdx.x; i < (int)(sizeof(SurWeights) / 4); i += blockDim.x) dst[i] = src[i];
-  }
-  __syncthreads();
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int nt = (n + 15) / 16;
-  for (int tile = blockIdx.x * 4 + wib; tile < nt; tile += gridDim.x * 4) {
-    if (lane < 16) {
-      const int i = tile * 16 + lane;
+// The network on a list of raw inputs (log10 tau x3, log10 T) with the
+// inference numerics of k_sur_predict: one CTA of 8 warps per tile of 128
+// evaluations on the tensor cores (the inputs normalised as there).
+struct EvalSmem {
+  TcNet w;
+  TcTile tile;
+};
+__global__ void __launch_bounds__(32 * kSurWarps) k_sur_eval(const TcNet *__restrict__ net,
+                                                           const float *__restrict__ X, int n,
+                                                           float *__restrict__ T, int *__restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  EvalSmem &S = *reinterpret_cast<EvalSmem *>(smem_raw);
+  tc_setup(net, S.w, S.tile);
+  bool ok = true;
+  for (int t0 = blockIdx.x * kTile; t0 < n; t0 += gridDim.x * kTile) {
+    ok = mlp_tile_tc(
+        S.w, S.tile, min(kTile, n - t0),
+        [&](int row, float(&x)[4]) {
+          const size_t i = (size_t)(t0 + row);
 #pragma unroll
-      for (int c = 0; c < 4; c++) {
-        float v = i < n ? X[4 * (size_t)i + c] : 0.f;
-        if (c < 3) {
-          v = fminf(fmaxf(v, kTauLo), kTauHi);
-          v = (v - 0.5f * (kTauLo + kTauHi)) * (2.f / (kTauHi - kTauLo));
-        } else {
-          v = (v - 0.5f * (kTLo + kTHi)) * (2.f / (kTHi - kTLo));
-        }
-        xs[wib][lane][c] = v;
-      }
-    }
-    __syncwarp();
-    mlp_tile16(W, xs[wib], ts[wib], 0, lane);
-    __syncwarp();
-    for (int q = lane; q < 16 * 6; q += 32) {
-      const int i = tile * 16 + q / 6;
-      if (i < n) T[6 * (size_t)i + q % 6] = ts[wib][q / 6][q % 6];
-    }
-    __syncwarp();
+          for (int c = 0; c < 4; c++) {
+            float v = X[4 * i + c];
+            if (c < 3) {
+              v = fminf(fmaxf(v, kTauLo), kTauHi);
+              v = (v - 0.5f * (kTauLo + kTauHi)) * (2.f / (kTauHi - kTauLo));
+            } else {
+              v = (v - 0.5f * (kTLo + kTHi)) * (2.f / (kTHi - kTLo));
+            }
+            x[c] = v;
+          }
+        },
+        [&](int row, const float(&q)[6]) {
+          const size_t i = (size_t)(t0 + row);
+#pragma unroll
+          for (int j = 0; j < 6; j++) T[6 * i + j] = q[j];
+        },
+        ok);
   }
+  if (!ok && threadIdx.x == 0) atomicExch(err, 1);
+  tc_teardown(S.tile);
 }
 
 }  // namespace argot
@@ -561,7 +688,7 @@ using namespace argot;
 // ------------------------------------------------------------- host side
 struct argot_b200_surrogate {
   int device;
-  SurWeights *dev;
+  TcNet *dev;
   float tol;  // host copy of the per-cell budget (kernel 2 argument)
 };
 
@@ -573,17 +700,29 @@ uint16_t bf16_bits(float f) {
   const uint32_t r = u + 0x7FFFu + ((u >> 16) & 1u);
   return (uint16_t)(r >> 16);
 }
-uint32_t pack2(float lo, float hi) { return (uint32_t)bf16_bits(lo) | ((uint32_t)bf16_bits(hi) << 16); }
 
-// B fragment of N-tile j, K-step kk for W[n][k] (rows n, cols k, getter)
+// W[n][k] (getter) into a K-major tile of R rows (umma.cuh layout)
 template <class F>
-uint2 frag(F w, int j, int kk, int lane) {
-  const int gq = lane >> 2, tq = lane & 3;
-  const int n = 8 * j + gq, k = 16 * kk + 2 * tq;
-  uint2 r;
-  r.x = pack2(w(n, k), w(n, k + 1));
-  r.y = pack2(w(n, k + 8), w(n, k + 9));
-  return r;
+void put_kmajor(uint16_t *tile, int R, int K, F w) {
+  for (int n = 0; n < R; n++)
+    for (int k = 0; k < K; k++) tile[umma::kmajor_offset(R, n, k) / 2] = bf16_bits(w(n, k));
+}
+
+// shared-memory bytes of the predict / eval kernels
+size_t pred_smem() { return sizeof(PredSmem); }
+size_t eval_smem() { return sizeof(EvalSmem); }
+
+int kernel_attrs(int dev) {
+  static std::mutex mu;
+  static bool done[64] = {false};
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev < 0 || dev >= 64) return ARGOT_B200_EINVAL;
+  if (!done[dev]) {
+    ARGOT_CUDA_TRY(cudaFuncSetAttribute(k_sur_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pred_smem()));
+    ARGOT_CUDA_TRY(cudaFuncSetAttribute(k_sur_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eval_smem()));
+    done[dev] = true;
+  }
+  return 0;
 }
 
 }  // namespace
@@ -595,24 +734,18 @@ extern "C" {
 // relative error budget of the surrogate's contributions.
 int argot_b200_surrogate_create(const float *params, const float *env, float tol, argot_b200_surrogate **out) {
   if (!params || !env || !out || !(tol > 0.f)) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
-  auto *h = new (std::nothrow) SurWeights();
+  auto *h = new (std::nothrow) TcNet();
   if (!h) { set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
   const float *W1 = params + kOffW1, *W2 = params + kOffW2, *W3 = params + kOffW3, *W4 = params + kOffW4;
-  for (int j = 0; j < 8; j++)
-    for (int l = 0; l < 32; l++) {
-      h->f1[j][l] = frag([&](int n, int k) { return k < 8 ? W1[n * kMlpIn + (k & 3)] : 0.f; }, j, 0, l);
-      for (int kk = 0; kk < 4; kk++) {
-        h->f2[j][kk][l] = frag([&](int n, int k) { return W2[n * kMlpH + k]; }, j, kk, l);
-        h->f3[j][kk][l] = frag([&](int n, int k) { return W3[n * kMlpH + k]; }, j, kk, l);
-      }
-    }
-  for (int kk = 0; kk < 8; kk++)
-    for (int l = 0; l < 32; l++)
-      h->f4[kk][l] = frag([&](int n, int k) { return n < kMlpOut ? W4[n * kMlpH + (k & 63)] : 0.f; }, 0, kk, l);
-  std::memcpy(h->b1, params + kOffB1, sizeof(float) * 64);
-  std::memcpy(h->b2, params + kOffB2, sizeof(float) * 64);
-  std::memcpy(h->b3, params + kOffB3, sizeof(float) * 64);
-  for (int j = 0; j < 8; j++) h->b4[j] = j < kMlpOut ? params[kOffB4 + j] : 0.f;
+  // layer 1: k 0..3 against the inputs' high parts, 4..7 against their low parts
+  put_kmajor(h->b1, 64, 16, [&](int n, int k) { return k < 8 ? W1[n * kMlpIn + (k & 3)] : 0.f; });
+  put_kmajor(h->b2, 64, 64, [&](int n, int k) { return W2[n * kMlpH + k]; });
+  put_kmajor(h->b3, 64, 64, [&](int n, int k) { return W3[n * kMlpH + k]; });
+  put_kmajor(h->b4, 16, 64, [&](int n, int k) { return n < kMlpOut ? W4[n * kMlpH + k] : 0.f; });
+  std::memcpy(h->bias1, params + kOffB1, sizeof(float) * 64);
+  std::memcpy(h->bias2, params + kOffB2, sizeof(float) * 64);
+  std::memcpy(h->bias3, params + kOffB3, sizeof(float) * 64);
+  for (int j = 0; j < 16; j++) h->bias4[j] = j < kMlpOut ? params[kOffB4 + j] : 0.f;
   // kernel 1 uses e^dq - 1: |q - q^| <= dq gives |y - y^| <= |y^| (e^dq - 1)
   for (int j = 0; j < 6; j++)
     for (int b = 0; b < kEnvBins; b++) h->env[j][b] = (float)std::expm1((double)env[j * kEnvBins + b]);
@@ -627,8 +760,8 @@ int argot_b200_surrogate_create(const float *params, const float *env, float tol
   if (!s) { delete h; set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
   s->tol = tol;
   cudaError_t e = cudaGetDevice(&s->device);
-  if (e == cudaSuccess) e = cudaMalloc(&s->dev, sizeof(SurWeights));
-  if (e == cudaSuccess) e = cudaMemcpy(s->dev, h, sizeof(SurWeights), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&s->dev, sizeof(TcNet));
+  if (e == cudaSuccess) e = cudaMemcpy(s->dev, h, sizeof(TcNet), cudaMemcpyHostToDevice);
   delete h;
   if (e != cudaSuccess) { delete s; return status_from_cuda(e); }
   *out = s;
@@ -645,11 +778,17 @@ void argot_b200_surrogate_free(argot_b200_surrogate *s) {
 // q_j predictions (n x 6) for raw inputs X (n x 4: log10 tau_HI, tau_HeI,
 // tau_HeII, log10 T) with the tensor-core inference numerics.
 int argot_b200_surrogate_eval(const argot_b200_surrogate *s, const float *X, int n, float *T, void *stream) {
-  if (!s || (n && (!X || !T))) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
+  if (!s || n < 0 || (n && (!X || !T))) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
   if (n) {
-    const int tiles = (n + 15) / 16;
-    const int blocks = (tiles + 3) / 4 < 4096 ? (tiles + 3) / 4 : 4096;
-    k_sur_eval<<<blocks, 128, 0, (cudaStream_t)stream>>>(s->dev, X, n, T);
+    int dev = 0;
+    ARGOT_CUDA_TRY(cudaGetDevice(&dev));
+    int rc = kernel_attrs(dev);
+    if (rc) { set_status(rc); return rc; }
+    int *err = err_flag(dev);
+    if (!err) { set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
+    const int tiles = (n + kTile - 1) / kTile;
+    const int blocks = tiles < 592 ? tiles : 592;
+    k_sur_eval<<<blocks, 32 * kSurWarps, eval_smem(), (cudaStream_t)stream>>>(s->dev, X, n, T, err);
     ARGOT_CUDA_TRY(cudaGetLastError());
   }
   set_status(0);
@@ -680,29 +819,19 @@ int argot_b200_photoion_rays_surrogate(const argot_b200_grid *gp, const void *pa
   if (rc) return rc;
   int *err = err_flag(dev);
   if (!err) { set_status(ARGOT_B200_ENOMEM); return ARGOT_B200_ENOMEM; }
-  static std::mutex mu;
-  static bool attr[64] = {false};
-  {
-    std::lock_guard<std::mutex> lock(mu);
-    if (dev < 0 || dev >= 64) { set_status(ARGOT_B200_EINVAL); return ARGOT_B200_EINVAL; }
-    if (!attr[dev]) {
-      ARGOT_CUDA_TRY(cudaFuncSetAttribute(k_sur_predict, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)sizeof(PredSmem)));
-      attr[dev] = true;
-    }
-  }
+  if ((rc = kernel_attrs(dev))) { set_status(rc); return rc; }
   GridDev g = make_grid(*gp);
   const uint64_t ncell = (uint64_t)gp->nx * gp->ny * gp->nz;
   const float4 *raw = (const float4 *)packed + ncell;
-  const int threads = 32 * kSurWarps;
-  const int blocks = grid_blocks_for_rates((b1 - b0) * 32, threads);
   cudaStream_t st = (cudaStream_t)stream;
-  k_sur_predict<<<blocks, threads, sizeof(PredSmem), st>>>(g, raw, t->emit_pos, t->emit_total, t->emit_logT,
-                                                            t->emit_i0, t->emit_m, sur->dev, b0, b1, blk_off,
-                                                            base, rays, nray, tau, rates6, work, err);
+  const int pthreads = 32 * kSurWarps;
+  k_sur_predict<<<grid_blocks_for_rates((b1 - b0) * 32, pthreads), pthreads, pred_smem(), st>>>(
+      g, raw, t->emit_pos, t->emit_total, t->emit_logT, t->emit_i0, t->emit_m, sur->dev, b0, b1, blk_off, base, rays,
+      nray, tau, rates6, work, err);
   ARGOT_CUDA_TRY(cudaGetLastError());
-  k_sur_select<<<blocks, threads, 0, st>>>(g, sur->tol, b0, b1, blk_off, base, rays, nray, rates6, work,
-                                            counters, err);
+  const int sthreads = 32 * kSelWarps;
+  k_sur_select<<<grid_blocks_for_rates((b1 - b0) * 32, sthreads), sthreads, 0, st>>>(
+      g, sur->tol, b0, b1, blk_off, base, rays, nray, rates6, work, counters, err);
   ARGOT_CUDA_TRY(cudaGetLastError());
   rc = launch_rate_f32_served(g, raw, t->emit_pos, t->emit_specn, t->emit_total, b0, b1, blk_off, base, rays, nray,
                               tau, rates6, work, err, st);
