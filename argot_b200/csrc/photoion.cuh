@@ -229,31 +229,32 @@ __device__ __forceinline__ void load_bin_pairs(BinPair *tab) {
 }
 
 // The photon-conserving cell factor phi(x) = (1 - e^-x)/x of the two bins
-// of a pair from dl2 = x log2(e).  Below x = 1 the difference 1 - e^-x
-// cancels, so phi comes from a degree-6 polynomial, a near-minimax fit of
-// relative error made by argot_b200/fits.py (8.8e-8 relative on [0, 1]
-// evaluated in FP32 with Horner's rule, checked by the CPU tests).  Above,
-// e^-x on the SFU: (1 - e^-x) / x to ~2e-7.  kSfu = false: the polynomial
-// alone, for the iterations whose bins are known to lie below x = 1
-// (sfu_iters): the SFU path is predicated, not branched, so where it is
-// compiled in every pair pays its two exponentials, two reciprocals and
-// their range handling (ncu, 256^3 / 16 sources: three MUFU operations per
-// bin instead of one, 60 warp instructions per iteration instead of ~40).
+// of a pair from u = x / ln 2 (the log2-scaled cell optical depth the loop
+// forms).  Below x = 1 the difference 1 - e^-x cancels, so phi comes from a
+// degree-6 polynomial in u, a near-minimax fit of relative error made by
+// argot_b200/fits.py (1.1e-7 relative on [0, 1 / ln 2) evaluated in FP32
+// with Horner's rule, checked by the CPU tests).  Above, e^-x on the SFU:
+// (1 - e^-x) / x to ~2e-7.  kSfu = false: the polynomial alone, for the
+// iterations whose bins are known to lie below x = 1 (sfu_iters): the SFU
+// path is predicated, not branched, so where it is compiled in every pair
+// pays its two exponentials, two reciprocals and their range handling
+// (ncu, 256^3 / 16 sources: three MUFU operations per bin instead of one,
+// 60 warp instructions per iteration instead of ~40).
 constexpr float kPhiXMax = 1.0f;
+constexpr float kPhiUMax = 1.44269504088896341f;  // kPhiXMax / ln 2
 template <bool kSfu = true>
-__device__ __forceinline__ float2 phi_pc2(float2 dl2) {
-  constexpr float kPhiC[7] = {1.f, -0.499999762f, 0.166663095f, -0.041645579f, 0.00827309582f, -0.00129866367f,
-                              0.000128380707f};
-  const float kLn2 = 0.69314718055994531f;
-  const float2 x = __fmul2_rn(dl2, make_float2(kLn2, kLn2));
+__device__ __forceinline__ float2 phi_pc2(float2 u) {
+  constexpr float kPhiC[7] = {1.f, -0.346573442f, 0.0800737888f, -0.0138690043f, 0.00190972083f, -0.000207789693f,
+                              1.42381168e-05f};
   float2 p = make_float2(kPhiC[6], kPhiC[6]);
 #pragma unroll
-  for (int k = 5; k >= 0; k--) p = __ffma2_rn(x, p, make_float2(kPhiC[k], kPhiC[k]));
+  for (int k = 5; k >= 0; k--) p = __ffma2_rn(u, p, make_float2(kPhiC[k], kPhiC[k]));
   if (!kSfu) return p;
-  const bool t0 = x.x < kPhiXMax, t1 = x.y < kPhiXMax;
+  const bool t0 = u.x < kPhiUMax, t1 = u.y < kPhiUMax;
   if (!(t0 && t1)) {
-    const float q0 = __fdividef(1.0f - ex2_approx(-dl2.x), x.x);
-    const float q1 = __fdividef(1.0f - ex2_approx(-dl2.y), x.y);
+    const float kLn2 = 0.69314718055994531f;
+    const float q0 = __fdividef(1.0f - ex2_approx(-u.x), u.x * kLn2);
+    const float q1 = __fdividef(1.0f - ex2_approx(-u.y), u.y * kLn2);
     p.x = t0 ? p.x : q0;
     p.y = t1 ? p.y : q1;
   }
@@ -279,9 +280,10 @@ template <bool kSfu>
 __device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, float2 n0, float2 n1, float2 n2, float2 d0,
                                          float2 d1, float2 d2, float2 (&acc)[6]) {
   const float2 l0 = b.l2e[0], l1 = b.l2e[1], l2 = b.l2e[2];
-  const float2 tl = __ffma2_rn(n0, l0, __ffma2_rn(n1, l1, __fmul2_rn(n2, l2)));
+  // n0..n2 hold the negated columns: ntl = -tau log2(e)
+  const float2 ntl = __ffma2_rn(n0, l0, __ffma2_rn(n1, l1, __fmul2_rn(n2, l2)));
   const float2 dl = __ffma2_rn(d0, l0, __ffma2_rn(d1, l1, __fmul2_rn(d2, l2)));
-  const float2 e = make_float2(ex2_approx(-tl.x), ex2_approx(-tl.y));
+  const float2 e = make_float2(ex2_approx(ntl.x), ex2_approx(ntl.y));
   const float2 ph = phi_pc2<kSfu>(dl);
   const float2 w = __fmul2_rn(__fmul2_rn(s, e), ph);
   const float2 vw = __fmul2_rn(b.nu, w);
@@ -304,7 +306,7 @@ __device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, float2 n0, 
 __device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab, const float *__restrict__ sp,
                                                 int j, int nsfu, float N0, float N1, float N2, float D0, float D1,
                                                 float D2, float (&out)[6]) {
-  const float2 n0 = make_float2(N0, N0), n1 = make_float2(N1, N1), n2 = make_float2(N2, N2);
+  const float2 n0 = make_float2(-N0, -N0), n1 = make_float2(-N1, -N1), n2 = make_float2(-N2, -N2);
   const float2 d0 = make_float2(D0, D0), d1 = make_float2(D1, D1), d2 = make_float2(D2, D2);
   // the pair's two spectrum bins in one 8-byte load (pair order)
   const float2 *__restrict__ sp2 = reinterpret_cast<const float2 *>(sp) + j;

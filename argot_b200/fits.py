@@ -16,6 +16,9 @@ import numpy as np
 
 PHI_X_MAX = 1.0
 PHI_DEGREE = 6
+# the kernel evaluates the polynomial in u = x / ln 2 (the log2-scaled
+# cell optical depth it forms anyway), on [0, PHI_X_MAX / ln 2)
+LN2 = 0.69314718055994531
 
 
 def phi(x):
@@ -26,12 +29,14 @@ def phi(x):
     return np.where(small, 1 - x / 2 + x * x / 6 - x ** 3 / 24 + x ** 4 / 120, -np.expm1(-xs) / xs)
 
 
-def fit_phi(x_max: float = PHI_X_MAX, degree: int = PHI_DEGREE, points: int = 4000, iters: int = 200):
-    """Power-basis coefficients c[0..degree] (FP32) of the fit on [0, x_max]."""
+def fit_phi(x_max: float = PHI_X_MAX, degree: int = PHI_DEGREE, points: int = 4000, iters: int = 200,
+            scale: float = 1.0):
+    """Power-basis coefficients c[0..degree] (FP32) of the fit of
+    u -> phi(scale u) on [0, x_max / scale]."""
     t = np.cos(np.pi * (np.arange(points) + 0.5) / points) * 0.5 + 0.5
-    x = t * x_max
+    x = t * (x_max / scale)
     V = np.vander(x, degree + 1, increasing=True)
-    f = phi(x)
+    f = phi(scale * x)
     w = 1.0 / f
     wt = np.full_like(x, 1.0 / points)
     c = None
@@ -53,14 +58,16 @@ def horner_f32(c, x):
     return p
 
 
-def phi_error(c, x_max: float = PHI_X_MAX, n: int = 200001):
-    """Largest relative error of the FP32 evaluation on [0, x_max]."""
-    x = np.linspace(0.0, x_max, n).astype(np.float32)
-    return float(np.max(np.abs(horner_f32(c, x).astype(np.float64) - phi(x.astype(np.float64)))
-                        / phi(x.astype(np.float64))))
+def phi_error(c, x_max: float = PHI_X_MAX, n: int = 200001, scale: float = 1.0):
+    """Largest relative error of the FP32 evaluation of u -> phi(scale u) on
+    [0, x_max / scale]."""
+    u = np.linspace(0.0, x_max / scale, n).astype(np.float32)
+    ref = phi(scale * u.astype(np.float64))
+    return float(np.max(np.abs(horner_f32(c, u).astype(np.float64) - ref) / ref))
 
 
 if __name__ == "__main__":
-    c = fit_phi()
-    print("coefficients:", ", ".join(f"{float(v):.9g}f" for v in c))
-    print("max relative error of the FP32 evaluation on [0, %g]: %.3g" % (PHI_X_MAX, phi_error(c)))
+    c = fit_phi(scale=LN2)
+    print("coefficients (in u = x / ln 2):", ", ".join(f"{float(v):.9g}f" for v in c))
+    print("max relative error of the FP32 evaluation on [0, %g / ln 2): %.3g"
+          % (PHI_X_MAX, phi_error(c, scale=LN2)))

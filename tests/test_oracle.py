@@ -194,8 +194,9 @@ def test_reference_fast_math_spread(oracle):
 
 def test_phi_polynomial_matches_fit_and_bound():
     """The coefficients of the FP32 rate kernel's photon-conserving factor
-    (photoion.cuh kPhiC) are the ones argot_b200/fits.py makes, and their
-    FP32 Horner evaluation stays within 1e-7 of (1 - e^-x)/x on [0, 1]."""
+    (photoion.cuh kPhiC, a polynomial in u = x / ln 2) are the ones
+    argot_b200/fits.py makes, and their FP32 Horner evaluation stays within
+    1.5e-7 of (1 - e^-x)/x for x in [0, 1]."""
     import os
     import re
     from argot_b200 import fits
@@ -203,6 +204,8 @@ def test_phi_polynomial_matches_fit_and_bound():
     src = open(os.path.join(ROOT, "argot_b200", "csrc", "photoion.cuh")).read()
     body = re.search(r"kPhiC\[7\]\s*=\s*\{([^}]*)\}", src).group(1)
     c = np.array([float(v.strip().rstrip("f")) for v in body.split(",")], np.float32)
-    assert np.array_equal(c, fits.fit_phi())
+    assert np.array_equal(c, fits.fit_phi(scale=fits.LN2))
     assert float(re.search(r"kPhiXMax\s*=\s*([0-9.]+)f", src).group(1)) == fits.PHI_X_MAX
-    assert fits.phi_error(c) < 1e-7
+    umax = float(re.search(r"kPhiUMax\s*=\s*([0-9.]+)f", src).group(1))
+    assert np.float32(umax) == np.float32(fits.PHI_X_MAX / fits.LN2)
+    assert fits.phi_error(c, scale=fits.LN2) < 1.5e-7
