@@ -60,6 +60,9 @@ SIGNATURES = {
     "argot_b200_error_string": (C.c_char_p, [i32]),
     "argot_b200_version": (C.c_char_p, []),
     "argot_b200_flagset": (C.c_char_p, []),
+    "argot_b200_dev_tree_build": (i32, [vp, i32, vp, vp, f32, vp, vp]),
+    "argot_b200_dev_tree_info": (i32, [vp, vp, vp, vp]),
+    "argot_b200_dev_tree_copy": (i32, [vp, vp, vp, vp, vp, vp]),
     "argot_b200_struct_sizes": (None, [vp]),
     "argot_b200_abi_check": (i32, [vp, i32]),
     "calc_optical_depth_cuda": (None, [vp, vp, vp, vp]),

@@ -211,6 +211,26 @@ typedef struct argot_b200_dev_tree argot_b200_dev_tree;
 ARGOT_B200_API int argot_b200_dev_tree_upload(const argot_b200_tree *t, argot_b200_dev_tree **out,
                                void *stream);
 ARGOT_B200_API void argot_b200_dev_tree_free(argot_b200_dev_tree *d);
+/* The same device tree built on the device from the sources' positions
+ * (nsrc x 3 floats) and spectra (nsrc x 256 doubles) in device memory:
+ * Morton keys, a stable radix sort, node enumeration in depth-first
+ * preorder, node sums level by level from the leaves up.  Bit-identical
+ * to argot_b200_tree_build + argot_b200_dev_tree_upload (the reference's
+ * construct_tree, setup_light_ray_tree.c:465-571); the surrogate's
+ * per-emitter inputs (argot_b200_dev_tree_set_blackbody) still need the
+ * host tree.  Allocates scratch and the tree; synchronises `stream`. */
+ARGOT_B200_API int argot_b200_dev_tree_build(const argot_b200_grid *g, int nsrc, const float *src_pos_dev,
+                                             const double *spectra_dev, float theta, argot_b200_dev_tree **out,
+                                             void *stream);
+/* node and emitter counts and the emitters' bounding box (lo xyz, hi xyz) */
+ARGOT_B200_API int argot_b200_dev_tree_info(const argot_b200_dev_tree *d, int *n_nodes, int *n_emit,
+                                            float *bounds6);
+/* host copies of a device tree's arrays (any pointer may be NULL): emitter
+ * positions (n_emit x 4 floats), FP64 spectra (n_emit x 256), the nodes
+ * (n_nodes x 8 words: centre x y z, side as floats; sources, skip link,
+ * has-children flag, first source as ints) and the sorted source list. */
+ARGOT_B200_API int argot_b200_dev_tree_copy(const argot_b200_dev_tree *d, float *pos4, double *spec64,
+                                            int *nodes8, int *src_list, void *stream);
 
 /* ---- light rays --------------------------------------------------------- */
 
