@@ -91,8 +91,9 @@ __global__ void __launch_bounds__(32 * kRateWarps)
 // kernel has no FP64 arithmetic.
 // Launch shape: ARGOT_RATE_WARPS warps per CTA, at least ARGOT_RATE_MIN_CTAS
 // CTAs resident per SM (which caps the registers per thread).  Measured on
-// B200 (256^3, 4096 sources, 3.2e9 rays): 8 warps x 3 CTAs (80 registers,
-// no spills) 1.07 s, x 4 CTAs (64 registers) 1.08 s, x 5 CTAs 1.34 s.
+// B200 (256^3, 4096 sources, 3.2e9 rays) with the per-cell sums in shared
+// memory: 8 warps x 3 CTAs (80 registers, no spills) 1.02 s, x 4 CTAs (64
+// registers) 1.08 s, x 5 CTAs (48 registers, spilling) 1.14 s.
 #ifndef ARGOT_RATE_WARPS
 #define ARGOT_RATE_WARPS 8
 #endif
