@@ -124,7 +124,7 @@ __device__ void ray_rates_f64(const GridDev &g, const DropinTab *__restrict__ T,
 #pragma unroll
   for (int q = 0; q < kNCol; q++) od[q] = __dmul_rn((double)col[q], cd);
   const RayGeom geo = ray_geometry(g, r.ix_target, r.iy_target, r.iz_target, r.src.xpos, r.src.ypos, r.src.zpos);
-  float dist2 = geo.dist2;
+  [[maybe_unused]] float dist2 = geo.dist2;
 #ifdef __PHOTON_CONSERVING__
   // per-species densities, the cell's own columns and 1/(n V_shell + TINY)
   double n[kNCol], dd[kNCol], rN[kNCol];
@@ -180,7 +180,7 @@ __device__ void ray_rates_f64(const GridDev &g, const DropinTab *__restrict__ T,
 #pragma unroll
     for (int c = 0; c < kNChan; c++) cs[c] = __ldg(&T->cs[c][k]);
     // channel order: HI, [HeI, HeII], [HM, H2I_I, H2II_I, H2II_II]
-    constexpr int cHM = kHe ? 3 : 1;
+    [[maybe_unused]] constexpr int cHM = kHe ? 3 : 1;
     double tau = __dmul_rn(od[0], cs[0]);
 #ifdef __HELIUM__
     tau = __dadd_rn(tau, __dmul_rn(od[kColHeI], cs[1]));
@@ -575,7 +575,6 @@ int do_rates(cuda_mem_space *cm, light_ray *ray, light_ray_IO *ray_io, cuda_para
   const uint64_t nray = run->nray;
   GridDev g;
   if (!grid_from_run(run, &g) || !cm[0].mesh_dev) return ARGOT_B200_EINVAL;
-  const uint64_t ncell = (uint64_t)g.nx * g.ny * g.nz;
   DeviceScope dscope;
   if (!dscope.ok) return ARGOT_B200_ECUDA;
   std::lock_guard<std::mutex> lock(g_mu);

@@ -37,6 +37,9 @@ static int ensure_rate_tables(int device) {
       t.hw[s][i] = (float)((double)c * w);
     }
   }
+  // nu_(k + 16 i) = nu_k 10^(16 i dlog_nu): the bins of the frequency grid
+  // are equally spaced in log nu (source.c:38-53)
+  for (int i = 0; i < 16; i++) t.rpow[i] = (float)(nu[16 * i] / nu[0]);
   for (int s = 0; s < 3; s++) {
     float m = 0.f;
     for (int k = kNu - 1; k >= 0; k--) {
@@ -196,21 +199,25 @@ __device__ __forceinline__ void ray_rates6(const float (&P)[3], float a0, float 
 // and multiply of sm_100.  An 8-lane group integrates one ray; lane j owns
 // the bin pairs (j + 16 i, j + 16 i + 8), i = 0..15 (the bins j + 8 m), and
 // keeps one partial sum per output and pair member.
-// The pair table holds sigma_s log2(e) of the three species and nu of the
-// two bins, 32 bytes, two 16-byte shared loads per pair.  The sums run on
-// these entries: sum sigma_s w = ln2 sum (sigma_s log2 e) w, and, because
+// The pair table holds sigma_s log2(e) of the three species of the two
+// bins, 24 bytes, three 8-byte shared loads per pair; nu of the pair's bins
+// is the lane's first pair times the grid ratio 10^(16 i dlog_nu) (the
+// frequency grid is equally spaced in log nu), one packed multiply, within
+// 2 ulp of the (float) nu the reference compares.  The sums run on these
+// entries: sum sigma_s w = ln2 sum (sigma_s log2 e) w, and, because
 // sigma_s vanishes below the species' threshold nu_s (the fits of
 // prim_chem/cross_section.c are 0 there), the heating sum
 // sum sigma_s (nu - nu_s)^+ w = ln2 (sum (sigma_s log2 e) nu w - nu_s
-// sum (sigma_s log2 e) w).  A 128-bit shared load is served in four
-// wavefronts whatever the broadcast, and the four groups of a warp read the
-// same entries, so the table's size sets the kernel's shared-memory
-// traffic: the earlier 80-byte entry (sigma log2 e, sigma and
-// sigma (nu - nu_s)^+ per species) kept the shared-memory pipe at 79% of
-// its peak (ncu, 256^3 / 16 sources).
-struct alignas(16) BinPair {
+// sum (sigma_s log2 e) w).  A shared load delivers 128 bytes per wavefront
+// whatever the broadcast (the four groups of a warp read the same
+// entries), so the table's bytes per lane set the kernel's shared-memory
+// traffic, which shares the L1 data path with the spectrum loads: the
+// earlier 80-byte entry (sigma log2 e, sigma and sigma (nu - nu_s)^+ per
+// species) kept the shared-memory pipe at 79% of its peak (ncu, 256^3 / 16
+// sources); dropping nu from the 32-byte entry took the 256^3 / 4096-source
+// rates from 1.02 s to 0.93 s.
+struct alignas(8) BinPair {
   float2 l2e[3];  // sigma_s log2(e) of the two bins
-  float2 nu;      // (float) nu of the two bins
 };
 constexpr int kBinPairs = kNu / 2;
 
@@ -223,7 +230,6 @@ __device__ __forceinline__ void load_bin_pairs(BinPair *tab) {
     BinPair b;
 #pragma unroll
     for (int s = 0; s < 3; s++) b.l2e[s] = make_float2(c_tab.cs_l2e[s][k0], c_tab.cs_l2e[s][k1]);
-    b.nu = make_float2(c_tab.nu_f[k0], c_tab.nu_f[k1]);
     tab[p] = b;
   }
 }
@@ -277,8 +283,8 @@ __device__ __forceinline__ int sfu_iters(float D0, float D1, float D2) {
 
 // One iteration of ray_bins_packed: the bin pair p of the lane.
 template <bool kSfu>
-__device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, float2 n0, float2 n1, float2 n2, float2 d0,
-                                         float2 d1, float2 d2, float2 (&acc)[6]) {
+__device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, float2 nu, float2 n0, float2 n1, float2 n2,
+                                         float2 d0, float2 d1, float2 d2, float2 (&acc)[6]) {
   const float2 l0 = b.l2e[0], l1 = b.l2e[1], l2 = b.l2e[2];
   // n0..n2 hold the negated columns: ntl = -tau log2(e)
   const float2 ntl = __ffma2_rn(n0, l0, __ffma2_rn(n1, l1, __fmul2_rn(n2, l2)));
@@ -286,7 +292,7 @@ __device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, float2 n0, 
   const float2 e = make_float2(ex2_approx(ntl.x), ex2_approx(ntl.y));
   const float2 ph = phi_pc2<kSfu>(dl);
   const float2 w = __fmul2_rn(__fmul2_rn(s, e), ph);
-  const float2 vw = __fmul2_rn(b.nu, w);
+  const float2 vw = __fmul2_rn(nu, w);
   acc[0] = __ffma2_rn(l0, w, acc[0]);
   acc[1] = __ffma2_rn(l1, w, acc[1]);
   acc[2] = __ffma2_rn(l2, w, acc[2]);
@@ -313,11 +319,21 @@ __device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab,
   float2 acc[6];
 #pragma unroll
   for (int q = 0; q < 6; q++) acc[q] = make_float2(0.f, 0.f);
+  // nu of the pair's bins from the lane's first pair and the grid ratio
+  const float2 nu0 = make_float2(c_tab.nu_f[j], c_tab.nu_f[j + 8]);
   int i = 0;
 #pragma unroll 2
-  for (; i < nsfu; i++) bin_pair<true>(tab[j + 8 * i], __ldg(sp2 + 8 * i), n0, n1, n2, d0, d1, d2, acc);
+  for (; i < nsfu; i++) {
+    const float r = c_tab.rpow[i];
+    bin_pair<true>(tab[j + 8 * i], __ldg(sp2 + 8 * i), __fmul2_rn(nu0, make_float2(r, r)), n0, n1, n2, d0, d1, d2,
+                   acc);
+  }
 #pragma unroll 4
-  for (; i < kBinPairs / 8; i++) bin_pair<false>(tab[j + 8 * i], __ldg(sp2 + 8 * i), n0, n1, n2, d0, d1, d2, acc);
+  for (; i < kBinPairs / 8; i++) {
+    const float r = c_tab.rpow[i];
+    bin_pair<false>(tab[j + 8 * i], __ldg(sp2 + 8 * i), __fmul2_rn(nu0, make_float2(r, r)), n0, n1, n2, d0, d1, d2,
+                    acc);
+  }
 #pragma unroll
   for (int q = 0; q < 6; q++) out[q] = acc[q].x + acc[q].y;
 }
