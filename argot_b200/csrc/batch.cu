@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(32 * kWarps, ARGOT_BATCH_MIN_WARPS / kWarps)
           float xs, ys, zs;
           ray_start(g, ep.x, ep.y, ep.z, xe, ye, ze, &xs, &ys, &zs);
           int steps = 0;
-          const Tau3 tt = march_kahan(g, cells, xs, ys, zs, xe, ye, ze, &steps, &bad);
+          const Tau3 tt = march_kahan<0, true>(g, cells, xs, ys, zs, xe, ye, ze, &steps, &bad);
           steps_total += (unsigned long long)steps;
           // the rate parameters (as argot_b200_photoion_rays)
           const float4 rw = __ldg(raw + cell_index(g, lx, ly, lz));
@@ -188,7 +188,10 @@ __global__ void __launch_bounds__(32 * kWarps, ARGOT_BATCH_MIN_WARPS / kWarps)
 #define ARGOT_SPLIT_MARCH_MIN_CTAS 6
 #endif
 #ifndef ARGOT_SPLIT_RATE_MIN_CTAS
-#define ARGOT_SPLIT_RATE_MIN_CTAS 4
+#define ARGOT_SPLIT_RATE_MIN_CTAS 2
+#endif
+#ifndef ARGOT_SPLIT_RATE_RAYS_PER_LANE
+#define ARGOT_SPLIT_RATE_RAYS_PER_LANE 2
 #endif
 constexpr int kSplitRateWarps = 8;
 
@@ -221,7 +224,7 @@ __global__ void __launch_bounds__(256, ARGOT_SPLIT_MARCH_MIN_CTAS)
         float xs, ys, zs;
         ray_start(g, ep.x, ep.y, ep.z, xe, ye, ze, &xs, &ys, &zs);
         int steps = 0;
-        const Tau3 t = march_kahan(g, P.cells, xs, ys, zs, xe, ye, ze, &steps, &bad);
+        const Tau3 t = march_kahan<0, true>(g, P.cells, xs, ys, zs, xe, ye, ze, &steps, &bad);
         P.tau[r] = t.hi;
         P.tau[P.nray + r] = t.hei;
         P.tau[2 * P.nray + r] = t.heii;
@@ -253,8 +256,9 @@ __global__ void __launch_bounds__(32 * kSplitRateWarps, ARGOT_SPLIT_RATE_MIN_CTA
     const BatchProb &P = probs[wi.prob];
     const GridDev g = P.g;
     for (uint64_t b = wi.b0; b < wi.b1; b++)
-      rate_block_f32(g, P.raw, P.emit_pos, P.specn, P.total, s_pairs, b, P.blk_off[b], P.blk_off[b + 1], P.rays,
-                     P.nray, P.tau, P.rates6, s_w[wib], lane);
+      rate_block_f32<false, ARGOT_SPLIT_RATE_RAYS_PER_LANE>(g, P.raw, P.emit_pos, P.specn, P.total, s_pairs, b,
+                                                            P.blk_off[b], P.blk_off[b + 1], P.rays, P.nray, P.tau,
+                                                            P.rates6, s_w[wib], lane);
   }
 }
 

@@ -149,6 +149,9 @@ __global__ void __launch_bounds__(256) k_walk(GridDev g, const DevNode *__restri
 #ifndef ARGOT_MARCH_MIN_CTAS
 #define ARGOT_MARCH_MIN_CTAS 8
 #endif
+#ifndef ARGOT_MARCH_CENTRE_END
+#define ARGOT_MARCH_CENTRE_END true
+#endif
 constexpr int kMarchThreads = 256;
 template <int kPrec, bool kInside>
 __global__ void __launch_bounds__(kMarchThreads, ARGOT_MARCH_MIN_CTAS) k_march_rays(GridDev g, const float4 *__restrict__ cells,
@@ -203,8 +206,8 @@ __global__ void __launch_bounds__(kMarchThreads, ARGOT_MARCH_MIN_CTAS) k_march_r
       int steps = 0;
       const Tau3 t = (kPrec == ARGOT_B200_PRECISION_REFERENCE)
                          ? march_reference(g, cells, xs, ys, zs, xe, ye, ze, &steps, &bad)
-                         : march_kahan<kMarchThreads>(g, cells, xs, ys, zs, xe, ye, ze, &steps, &bad,
-                                                      kslot + threadIdx.x);
+                         : march_kahan<kMarchThreads, ARGOT_MARCH_CENTRE_END>(g, cells, xs, ys, zs, xe, ye, ze,
+                                                                              &steps, &bad, kslot + threadIdx.x);
       const uint64_t ro = (((uint64_t)ws[4] << 32) | ws[3]) + j;
       tau[ro] = t.hi;
       tau[nray + ro] = t.hei;

@@ -90,15 +90,20 @@ __global__ void __launch_bounds__(32 * kRateWarps)
 // rays that end in its cell, in ray order (add_chunk_in_order).  The
 // kernel has no FP64 arithmetic.
 // Launch shape: ARGOT_RATE_WARPS warps per CTA, at least ARGOT_RATE_MIN_CTAS
-// CTAs resident per SM (which caps the registers per thread).  Measured on
+// CTAs resident per SM (which caps the registers per thread), and
+// ARGOT_RATE_RAYS_PER_LANE rays per 8-lane group in phase B.  Measured on
 // B200 (256^3, 4096 sources, 3.2e9 rays) with the per-cell sums in shared
-// memory: 8 warps x 3 CTAs (80 registers, no spills) 1.02 s, x 4 CTAs (64
-// registers) 1.08 s, x 5 CTAs (48 registers, spilling) 1.14 s.
+// memory: one ray per group, 8 warps x 3 CTAs (80 registers, no spills)
+// 0.93 s; two rays per group, 8 warps x 2 CTAs (112 registers) 0.85 s,
+// x 3 CTAs (80 registers, spilling) 0.94 s.
 #ifndef ARGOT_RATE_WARPS
 #define ARGOT_RATE_WARPS 8
 #endif
 #ifndef ARGOT_RATE_MIN_CTAS
-#define ARGOT_RATE_MIN_CTAS 3
+#define ARGOT_RATE_MIN_CTAS 2
+#endif
+#ifndef ARGOT_RATE_RAYS_PER_LANE
+#define ARGOT_RATE_RAYS_PER_LANE 2
 #endif
 constexpr int kF32Warps = ARGOT_RATE_WARPS;
 
@@ -122,8 +127,8 @@ __global__ void __launch_bounds__(32 * kF32Warps, ARGOT_RATE_MIN_CTAS)
       if (lane == 0) atomicExch(err, 1);
       continue;
     }
-    rate_block_f32<kServed>(g, raw, emit_pos, specn, total, s_pairs, b, r0, r1, rays, nray, tau, rates6, s_w[wib],
-                            lane, pred);
+    rate_block_f32<kServed, ARGOT_RATE_RAYS_PER_LANE>(g, raw, emit_pos, specn, total, s_pairs, b, r0, r1, rays,
+                                                      nray, tau, rates6, s_w[wib], lane, pred);
   }
 }
 

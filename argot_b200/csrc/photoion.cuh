@@ -290,8 +290,7 @@ __device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, float2 nu, 
   const float2 ntl = __ffma2_rn(n0, l0, __ffma2_rn(n1, l1, __fmul2_rn(n2, l2)));
   const float2 dl = __ffma2_rn(d0, l0, __ffma2_rn(d1, l1, __fmul2_rn(d2, l2)));
   const float2 e = make_float2(ex2_approx(ntl.x), ex2_approx(ntl.y));
-  const float2 ph = phi_pc2<kSfu>(dl);
-  const float2 w = __fmul2_rn(__fmul2_rn(s, e), ph);
+  const float2 w = __fmul2_rn(__fmul2_rn(s, e), phi_pc2<kSfu>(dl));
   const float2 vw = __fmul2_rn(nu, w);
   acc[0] = __ffma2_rn(l0, w, acc[0]);
   acc[1] = __ffma2_rn(l1, w, acc[1]);
@@ -312,7 +311,8 @@ __device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, float2 nu, 
 __device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab, const float *__restrict__ sp,
                                                 int j, int nsfu, float N0, float N1, float N2, float D0, float D1,
                                                 float D2, float (&out)[6]) {
-  const float2 n0 = make_float2(-N0, -N0), n1 = make_float2(-N1, -N1), n2 = make_float2(-N2, -N2);
+  const float m0 = -N0, m1 = -N1, m2 = -N2;
+  const float2 n0 = make_float2(m0, m0), n1 = make_float2(m1, m1), n2 = make_float2(m2, m2);
   const float2 d0 = make_float2(D0, D0), d1 = make_float2(D1, D1), d2 = make_float2(D2, D2);
   // the pair's two spectrum bins in one 8-byte load (pair order)
   const float2 *__restrict__ sp2 = reinterpret_cast<const float2 *>(sp) + j;
@@ -336,6 +336,49 @@ __device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab,
   }
 #pragma unroll
   for (int q = 0; q < 6; q++) out[q] = acc[q].x + acc[q].y;
+}
+
+// ray_bins_packed for two rays at once (columns nd = N0, N1, N2, D0, D1,
+// D2 of each): one load of each bin pair of the table serves both rays,
+// which halves the shared-memory traffic per ray; nsfu covers both.
+__device__ __forceinline__ void ray_bins_packed2(const BinPair *__restrict__ tab, const float *__restrict__ spa,
+                                                 const float *__restrict__ spb, int j, int nsfu,
+                                                 const float *nda, const float *ndb, float (&outa)[6],
+                                                 float (&outb)[6]) {
+  const float ma0 = -nda[0], ma1 = -nda[1], ma2 = -nda[2];
+  const float mb0 = -ndb[0], mb1 = -ndb[1], mb2 = -ndb[2];
+  const float2 a0 = make_float2(ma0, ma0), a1 = make_float2(ma1, ma1), a2 = make_float2(ma2, ma2);
+  const float2 da0 = make_float2(nda[3], nda[3]), da1 = make_float2(nda[4], nda[4]), da2 = make_float2(nda[5], nda[5]);
+  const float2 b0 = make_float2(mb0, mb0), b1 = make_float2(mb1, mb1), b2 = make_float2(mb2, mb2);
+  const float2 db0 = make_float2(ndb[3], ndb[3]), db1 = make_float2(ndb[4], ndb[4]), db2 = make_float2(ndb[5], ndb[5]);
+  const float2 *__restrict__ sa = reinterpret_cast<const float2 *>(spa) + j;
+  const float2 *__restrict__ sb = reinterpret_cast<const float2 *>(spb) + j;
+  float2 acca[6], accb[6];
+#pragma unroll
+  for (int q = 0; q < 6; q++) acca[q] = accb[q] = make_float2(0.f, 0.f);
+  const float2 nu0 = make_float2(c_tab.nu_f[j], c_tab.nu_f[j + 8]);
+  int i = 0;
+#pragma unroll 1
+  for (; i < nsfu; i++) {
+    const float r = c_tab.rpow[i];
+    const float2 nu = __fmul2_rn(nu0, make_float2(r, r));
+    const BinPair b = tab[j + 8 * i];
+    bin_pair<true>(b, __ldg(sa + 8 * i), nu, a0, a1, a2, da0, da1, da2, acca);
+    bin_pair<true>(b, __ldg(sb + 8 * i), nu, b0, b1, b2, db0, db1, db2, accb);
+  }
+#pragma unroll 2
+  for (; i < kBinPairs / 8; i++) {
+    const float r = c_tab.rpow[i];
+    const float2 nu = __fmul2_rn(nu0, make_float2(r, r));
+    const BinPair b = tab[j + 8 * i];
+    bin_pair<false>(b, __ldg(sa + 8 * i), nu, a0, a1, a2, da0, da1, da2, acca);
+    bin_pair<false>(b, __ldg(sb + 8 * i), nu, b0, b1, b2, db0, db1, db2, accb);
+  }
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    outa[q] = acca[q].x + acca[q].y;
+    outb[q] = accb[q].x + accb[q].y;
+  }
 }
 
 // Per-warp scratch of rate_block_f32.
@@ -415,13 +458,14 @@ __device__ __forceinline__ void add_chunk_in_order(Acc &acc, int lane, int t, co
 // (columns in three planes of nray), written to its cells in rates6; one
 // warp.  Phase A: per-ray parameters (ray_params_f32), one lane per ray, 32
 // rays at a time.  Phase B: four 8-lane groups, one ray each, over the bin
-// pairs (ray_bins_packed), three butterfly steps.  Phase C: lane j adds the
+// pairs (ray_bins_packed; with kRaysPerLane 2, two rays per group,
+// ray_bins_packed2), three butterfly steps.  Phase C: lane j adds the
 // rays of cell j of the block in ray order (add_chunk_in_order).
 // kServed: `pred` holds 7 planes of nray floats, six per-ray contributions
 // and a flag; a ray whose flag is non-zero contributes those six values
 // and skips the quadrature, which runs over the remaining rays of the
 // chunk only (the surrogate's fallback).
-template <bool kServed = false>
+template <bool kServed = false, int kRaysPerLane = 1>
 __device__ __forceinline__ void rate_block_f32(const GridDev &g, const float4 *__restrict__ raw,
                                                const float4 *__restrict__ emit_pos, const float *__restrict__ specn,
                                                const double *__restrict__ total, const BinPair *__restrict__ pairs,
@@ -476,30 +520,67 @@ __device__ __forceinline__ void rate_block_f32(const GridDev &g, const float4 *_
       nq = __popc(m);
     }
     __syncwarp();
-    // rounds of four rays, one per group; the groups of a round run the
-    // same bin loop (the largest SFU count of the four), so that the warp
-    // stays converged; a group without a ray in the last round repeats the
-    // round's first ray and discards it
-    for (int i0 = 0; i0 < nq; i0 += 4) {
-      const int i = i0 + grp < nq ? i0 + grp : i0;
-      const int q = kServed ? S.q[i] : i;
-      int nsfu = 0;
+    // rounds of four (eight) rays, one (two) per group; the groups of a
+    // round run the same bin loop (the largest SFU count of the round), so
+    // that the warp stays converged; a group without a ray in the last
+    // round repeats the round's first ray and discards it
+    static_assert(kRaysPerLane == 1 || kRaysPerLane == 2, "one or two rays per lane");
+    if constexpr (kRaysPerLane == 2) {
+      for (int i0 = 0; i0 < nq; i0 += 8) {
+        const int ia = i0 + grp < nq ? i0 + grp : i0, ib = i0 + 4 + grp < nq ? i0 + 4 + grp : i0;
+        const int qa = kServed ? S.q[ia] : ia, qb = kServed ? S.q[ib] : ib;
+        int nsfu = 0;
 #pragma unroll
-      for (int k = 0; k < 4; k++) nsfu = max(nsfu, i0 + k < nq ? S.nsfu[kServed ? S.q[i0 + k] : i0 + k] : 0);
-      float part[6];
-      ray_bins_packed(pairs, specn + (size_t)S.e[q] * kNu, j, nsfu, S.nd[q][0], S.nd[q][1], S.nd[q][2], S.nd[q][3],
-                      S.nd[q][4], S.nd[q][5], part);
+        for (int k = 0; k < 8; k++) nsfu = max(nsfu, i0 + k < nq ? S.nsfu[kServed ? S.q[i0 + k] : i0 + k] : 0);
+        float pa[6], pb[6];
+        ray_bins_packed2(pairs, specn + (size_t)S.e[qa] * kNu, specn + (size_t)S.e[qb] * kNu, j, nsfu, S.nd[qa],
+                         S.nd[qb], pa, pb);
 #pragma unroll
-      for (int o = 1; o < 8; o <<= 1) {
+        for (int o = 1; o < 8; o <<= 1) {
 #pragma unroll
-        for (int s = 0; s < 6; s++) part[s] += __shfl_xor_sync(gmask, part[s], o);
+          for (int s = 0; s < 6; s++) {
+            pa[s] += __shfl_xor_sync(gmask, pa[s], o);
+            pb[s] += __shfl_xor_sync(gmask, pb[s], o);
+          }
+        }
+        if (j == 0) {
+          float out[6];
+          if (i0 + grp < nq) {
+            const float P[3] = {S.p[qa][0], S.p[qa][1], S.p[qa][2]};
+            ray_rates6(P, pa[0], pa[1], pa[2], pa[3], pa[4], pa[5], out);
+#pragma unroll
+            for (int s = 0; s < 6; s++) S.out[qa][s] = out[s];
+          }
+          if (i0 + 4 + grp < nq) {
+            const float P[3] = {S.p[qb][0], S.p[qb][1], S.p[qb][2]};
+            ray_rates6(P, pb[0], pb[1], pb[2], pb[3], pb[4], pb[5], out);
+#pragma unroll
+            for (int s = 0; s < 6; s++) S.out[qb][s] = out[s];
+          }
+        }
       }
-      if (j == 0 && i0 + grp < nq) {
-        const float P[3] = {S.p[q][0], S.p[q][1], S.p[q][2]};
-        float out[6];
-        ray_rates6(P, part[0], part[1], part[2], part[3], part[4], part[5], out);
+    } else {
+      for (int i0 = 0; i0 < nq; i0 += 4) {
+        const int i = i0 + grp < nq ? i0 + grp : i0;
+        const int q = kServed ? S.q[i] : i;
+        int nsfu = 0;
 #pragma unroll
-        for (int s = 0; s < 6; s++) S.out[q][s] = out[s];
+        for (int k = 0; k < 4; k++) nsfu = max(nsfu, i0 + k < nq ? S.nsfu[kServed ? S.q[i0 + k] : i0 + k] : 0);
+        float part[6];
+        ray_bins_packed(pairs, specn + (size_t)S.e[q] * kNu, j, nsfu, S.nd[q][0], S.nd[q][1], S.nd[q][2], S.nd[q][3],
+                        S.nd[q][4], S.nd[q][5], part);
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+#pragma unroll
+          for (int s = 0; s < 6; s++) part[s] += __shfl_xor_sync(gmask, part[s], o);
+        }
+        if (j == 0 && i0 + grp < nq) {
+          const float P[3] = {S.p[q][0], S.p[q][1], S.p[q][2]};
+          float out[6];
+          ray_rates6(P, part[0], part[1], part[2], part[3], part[4], part[5], out);
+#pragma unroll
+          for (int s = 0; s < 6; s++) S.out[q][s] = out[s];
+        }
       }
     }
     __syncwarp();

@@ -133,6 +133,23 @@ def test_march_rays_kahan_vs_fp64(cuda_ok, oracle):
     assert column_error(t32, t64) > cerr
 
 
+@pytest.mark.parametrize("seed", [8, 21])
+def test_march_rays_end_test_equals_face_counts(cuda_ok, seed):
+    """The device path's march ends a ray when its next face lies past the
+    end point (the target cell's centre); the explicit-segment march counts
+    the faces of each axis instead.  Both take the same faces in the same
+    order, so the columns are equal bit for bit."""
+    from argot_b200 import workload as W
+    from argot_b200 import _lib as L
+    from gpu_util import march_segments, run_problem, ray_segments
+    wl = W.tiny(32, 20, seed=seed, sigma_ln=1.2)
+    pb, emit, tgt, tau, _ = run_problem(wl, L.PRECISION_KAHAN, L.RATE_EXACT_F32)
+    segs = ray_segments(pb, emit, tgt)
+    tau_seg = march_segments(32, wl.fields(), segs, L.PRECISION_KAHAN, wl.lunit, wl.denstonh)
+    assert len(segs) > 10000
+    assert np.array_equal(tau, tau_seg)
+
+
 def test_grouped_rays_equal_single_pass(cuda_ok):
     """Memory-bounded groups of target blocks give the same columns."""
     from argot_b200 import workload as W
