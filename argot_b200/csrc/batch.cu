@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(32 * kWarps, ARGOT_BATCH_MIN_WARPS / kWarps)
           const float D0 = s_nd[wib][q][3], D1 = s_nd[wib][q][4], D2 = s_nd[wib][q][5];
           const float *sp = specn + (size_t)s_e[wib][q] * kNu;
           float part[6];
-          ray_bins_packed(s_pairs, sp, j, nsfu, N0, N1, N2, D0, D1, D2, part);
+          ray_bins_packed(s_pairs, sp, j, nsfu, s_nsfu[wib][q], N0, N1, N2, D0, D1, D2, part);
 #pragma unroll
           for (int o = 1; o < 8; o <<= 1) {
 #pragma unroll

@@ -234,37 +234,34 @@ __device__ __forceinline__ void load_bin_pairs(BinPair *tab) {
   }
 }
 
-// The photon-conserving cell factor phi(x) = (1 - e^-x)/x of the two bins
-// of a pair from u = x / ln 2 (the log2-scaled cell optical depth the loop
-// forms).  Below x = 1 the difference 1 - e^-x cancels, so phi comes from a
-// degree-6 polynomial in u, a near-minimax fit of relative error made by
-// argot_b200/fits.py (1.1e-7 relative on [0, 1 / ln 2) evaluated in FP32
-// with Horner's rule, checked by the CPU tests).  Above, e^-x on the SFU:
-// (1 - e^-x) / x to ~2e-7.  kSfu = false: the polynomial alone, for the
-// iterations whose bins are known to lie below x = 1 (sfu_iters): the SFU
-// path is predicated, not branched, so where it is compiled in every pair
-// pays its two exponentials, two reciprocals and their range handling
-// (ncu, 256^3 / 16 sources: three MUFU operations per bin instead of one,
-// 60 warp instructions per iteration instead of ~40).
+// The photon-conserving cell factor phi(x) = (1 - e^-x)/x (x the cell's
+// optical depth in the bin) enters every bin as e^-tau phi(x), tau the
+// optical depth to the cell.  Below x = kPhiXMax the difference 1 - e^-x
+// cancels, so the loop forms e^-tau phi(x) = e^-(tau + x/2) sinh(y)/y,
+// y = x / 2, with sinh(y)/y a polynomial (sinhc_half2); above, it takes
+// e^-tau (1 - e^-x) / x from the SFU (~2e-7).  Only the leading iterations
+// of a ray can hold a bin above kPhiXMax (sfu_iters); the SFU form is
+// predicated, not branched, so where it is compiled in every pair pays its
+// exponentials and reciprocal (ncu, 256^3 / 16 sources: three MUFU
+// operations per bin instead of one, 60 warp instructions per iteration
+// instead of ~40), and it is compiled only into those iterations.
 constexpr float kPhiXMax = 1.0f;
 constexpr float kPhiUMax = 1.44269504088896341f;  // kPhiXMax / ln 2
-template <bool kSfu = true>
-__device__ __forceinline__ float2 phi_pc2(float2 u) {
-  constexpr float kPhiC[7] = {1.f, -0.346573442f, 0.0800737888f, -0.0138690043f, 0.00190972083f, -0.000207789693f,
-                              1.42381168e-05f};
-  float2 p = make_float2(kPhiC[6], kPhiC[6]);
-#pragma unroll
-  for (int k = 5; k >= 0; k--) p = __ffma2_rn(u, p, make_float2(kPhiC[k], kPhiC[k]));
-  if (!kSfu) return p;
-  const bool t0 = u.x < kPhiUMax, t1 = u.y < kPhiUMax;
-  if (!(t0 && t1)) {
-    const float kLn2 = 0.69314718055994531f;
-    const float q0 = __fdividef(1.0f - ex2_approx(-u.x), u.x * kLn2);
-    const float q1 = __fdividef(1.0f - ex2_approx(-u.y), u.y * kLn2);
-    p.x = t0 ? p.x : q0;
-    p.y = t1 ? p.y : q1;
-  }
-  return p;
+
+// sinh(y) / y, y = x / 2 = dl ln2 / 2, of the two bins of a pair from
+// v = dl^2: a near-minimax fit of degree 3 in v made by argot_b200/fits.py
+// (fit_sinhc; times the FP32 mid-cell attenuation 2^(-dl/2) it is within
+// 1.5e-7 of phi(x) on [0, 1], checked by the CPU tests).  With it
+// e^-tau phi(x) = e^-(tau + x/2) sinh(y) / y: the attenuation to the middle
+// of the cell, whose exponent folds into the ray's columns, times an even
+// polynomial, one packed multiply and three packed FMAs where the
+// polynomial of phi(x) in x took six FMAs.
+__device__ __forceinline__ float2 sinhc_half2(float2 dl) {
+  constexpr float kShc[4] = {1.f, 0.0200188775f, 0.000120223514f, 3.4621803e-07f};
+  const float2 v = __fmul2_rn(dl, dl);
+  float2 p = __ffma2_rn(v, make_float2(kShc[3], kShc[3]), make_float2(kShc[2], kShc[2]));
+  p = __ffma2_rn(v, p, make_float2(kShc[1], kShc[1]));
+  return __ffma2_rn(v, p, make_float2(kShc[0], kShc[0]));
 }
 
 // Iterations of ray_bins_packed that may hold a bin with x = sum_s D_s
@@ -281,16 +278,32 @@ __device__ __forceinline__ int sfu_iters(float D0, float D1, float D2) {
   return n;
 }
 
-// One iteration of ray_bins_packed: the bin pair p of the lane.
+// One iteration of ray_bins_packed: the bin pair p of the lane.  n0..n2
+// hold the negated mid-cell columns -(N_s + D_s / 2), so that
+// ntm = -(tau + x / 2) log2(e) and w = s 2^ntm sinh(x/2)/(x/2).  With kSfu
+// and `sfu` (an iteration below the ray's own sfu_iters count) a bin with
+// x >= kPhiXMax takes w = s 2^(ntm + dl/2) (1 - 2^-dl) / x instead.  A
+// bin's value depends on its own ray alone, whichever other rays share the
+// loop's round.
 template <bool kSfu>
 __device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, float2 nu, float2 n0, float2 n1, float2 n2,
-                                         float2 d0, float2 d1, float2 d2, float2 (&acc)[6]) {
+                                         float2 d0, float2 d1, float2 d2, float2 (&acc)[6], bool sfu = false) {
   const float2 l0 = b.l2e[0], l1 = b.l2e[1], l2 = b.l2e[2];
-  // n0..n2 hold the negated columns: ntl = -tau log2(e)
-  const float2 ntl = __ffma2_rn(n0, l0, __ffma2_rn(n1, l1, __fmul2_rn(n2, l2)));
+  const float2 ntm = __ffma2_rn(n0, l0, __ffma2_rn(n1, l1, __fmul2_rn(n2, l2)));
   const float2 dl = __ffma2_rn(d0, l0, __ffma2_rn(d1, l1, __fmul2_rn(d2, l2)));
-  const float2 e = make_float2(ex2_approx(ntl.x), ex2_approx(ntl.y));
-  const float2 w = __fmul2_rn(__fmul2_rn(s, e), phi_pc2<kSfu>(dl));
+  const float2 e = make_float2(ex2_approx(ntm.x), ex2_approx(ntm.y));
+  float2 w = __fmul2_rn(__fmul2_rn(s, e), sinhc_half2(dl));
+  if (kSfu) {
+    const bool t0 = !sfu || dl.x < kPhiUMax, t1 = !sfu || dl.y < kPhiUMax;
+    if (!(t0 && t1)) {
+      const float kLn2 = 0.69314718055994531f;
+      const float2 ntl = __ffma2_rn(dl, make_float2(0.5f, 0.5f), ntm);
+      const float q0 = s.x * ex2_approx(ntl.x) * __fdividef(1.0f - ex2_approx(-dl.x), dl.x * kLn2);
+      const float q1 = s.y * ex2_approx(ntl.y) * __fdividef(1.0f - ex2_approx(-dl.y), dl.y * kLn2);
+      w.x = t0 ? w.x : q0;
+      w.y = t1 ? w.y : q1;
+    }
+  }
   const float2 vw = __fmul2_rn(nu, w);
   acc[0] = __ffma2_rn(l0, w, acc[0]);
   acc[1] = __ffma2_rn(l1, w, acc[1]);
@@ -302,16 +315,17 @@ __device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, float2 nu, 
 
 // The lane's six partial sums of one ray with columns N (to the cell) and
 // D (of the cell) in cm^-2; sp: the emitter's normalised spectrum; j: the
-// lane in the ray's 8-lane group; the first nsfu iterations may need the
-// SFU path of phi (sfu_iters; the caller passes the same count to the four
-// groups of the warp, so that their loops stay converged):
+// lane in the ray's 8-lane group; the first nsfu iterations are compiled
+// with the SFU form (the caller passes the same count, the round's largest
+// sfu_iters, to the four groups of the warp, so that their loops stay
+// converged), which the ray takes in its own first `own` (its sfu_iters):
 // out[s] = sum (sigma_s log2 e) w, out[3 + s] = sum (sigma_s log2 e) nu w
 // over the lane's bins, w = s_nu e^-tau phi(dtau).  The caller adds the
 // eight lanes and forms the rates (ray_rates6).
 __device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab, const float *__restrict__ sp,
-                                                int j, int nsfu, float N0, float N1, float N2, float D0, float D1,
-                                                float D2, float (&out)[6]) {
-  const float m0 = -N0, m1 = -N1, m2 = -N2;
+                                                int j, int nsfu, int own, float N0, float N1, float N2, float D0,
+                                                float D1, float D2, float (&out)[6]) {
+  const float m0 = -fmaf(0.5f, D0, N0), m1 = -fmaf(0.5f, D1, N1), m2 = -fmaf(0.5f, D2, N2);
   const float2 n0 = make_float2(m0, m0), n1 = make_float2(m1, m1), n2 = make_float2(m2, m2);
   const float2 d0 = make_float2(D0, D0), d1 = make_float2(D1, D1), d2 = make_float2(D2, D2);
   // the pair's two spectrum bins in one 8-byte load (pair order)
@@ -326,7 +340,7 @@ __device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab,
   for (; i < nsfu; i++) {
     const float r = c_tab.rpow[i];
     bin_pair<true>(tab[j + 8 * i], __ldg(sp2 + 8 * i), __fmul2_rn(nu0, make_float2(r, r)), n0, n1, n2, d0, d1, d2,
-                   acc);
+                   acc, i < own);
   }
 #pragma unroll 4
   for (; i < kBinPairs / 8; i++) {
@@ -339,14 +353,17 @@ __device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab,
 }
 
 // ray_bins_packed for two rays at once (columns nd = N0, N1, N2, D0, D1,
-// D2 of each): one load of each bin pair of the table serves both rays,
-// which halves the shared-memory traffic per ray; nsfu covers both.
+// D2 of each, own SFU counts owna, ownb): one load of each bin pair of the
+// table serves both rays, which halves the shared-memory traffic per ray;
+// nsfu covers both.
 __device__ __forceinline__ void ray_bins_packed2(const BinPair *__restrict__ tab, const float *__restrict__ spa,
-                                                 const float *__restrict__ spb, int j, int nsfu,
-                                                 const float *nda, const float *ndb, float (&outa)[6],
+                                                 const float *__restrict__ spb, int j, int nsfu, int owna,
+                                                 int ownb, const float *nda, const float *ndb, float (&outa)[6],
                                                  float (&outb)[6]) {
-  const float ma0 = -nda[0], ma1 = -nda[1], ma2 = -nda[2];
-  const float mb0 = -ndb[0], mb1 = -ndb[1], mb2 = -ndb[2];
+  const float ma0 = -fmaf(0.5f, nda[3], nda[0]), ma1 = -fmaf(0.5f, nda[4], nda[1]),
+              ma2 = -fmaf(0.5f, nda[5], nda[2]);
+  const float mb0 = -fmaf(0.5f, ndb[3], ndb[0]), mb1 = -fmaf(0.5f, ndb[4], ndb[1]),
+              mb2 = -fmaf(0.5f, ndb[5], ndb[2]);
   const float2 a0 = make_float2(ma0, ma0), a1 = make_float2(ma1, ma1), a2 = make_float2(ma2, ma2);
   const float2 da0 = make_float2(nda[3], nda[3]), da1 = make_float2(nda[4], nda[4]), da2 = make_float2(nda[5], nda[5]);
   const float2 b0 = make_float2(mb0, mb0), b1 = make_float2(mb1, mb1), b2 = make_float2(mb2, mb2);
@@ -363,8 +380,8 @@ __device__ __forceinline__ void ray_bins_packed2(const BinPair *__restrict__ tab
     const float r = c_tab.rpow[i];
     const float2 nu = __fmul2_rn(nu0, make_float2(r, r));
     const BinPair b = tab[j + 8 * i];
-    bin_pair<true>(b, __ldg(sa + 8 * i), nu, a0, a1, a2, da0, da1, da2, acca);
-    bin_pair<true>(b, __ldg(sb + 8 * i), nu, b0, b1, b2, db0, db1, db2, accb);
+    bin_pair<true>(b, __ldg(sa + 8 * i), nu, a0, a1, a2, da0, da1, da2, acca, i < owna);
+    bin_pair<true>(b, __ldg(sb + 8 * i), nu, b0, b1, b2, db0, db1, db2, accb, i < ownb);
   }
 #pragma unroll 2
   for (; i < kBinPairs / 8; i++) {
@@ -533,8 +550,8 @@ __device__ __forceinline__ void rate_block_f32(const GridDev &g, const float4 *_
 #pragma unroll
         for (int k = 0; k < 8; k++) nsfu = max(nsfu, i0 + k < nq ? S.nsfu[kServed ? S.q[i0 + k] : i0 + k] : 0);
         float pa[6], pb[6];
-        ray_bins_packed2(pairs, specn + (size_t)S.e[qa] * kNu, specn + (size_t)S.e[qb] * kNu, j, nsfu, S.nd[qa],
-                         S.nd[qb], pa, pb);
+        ray_bins_packed2(pairs, specn + (size_t)S.e[qa] * kNu, specn + (size_t)S.e[qb] * kNu, j, nsfu, S.nsfu[qa],
+                         S.nsfu[qb], S.nd[qa], S.nd[qb], pa, pb);
 #pragma unroll
         for (int o = 1; o < 8; o <<= 1) {
 #pragma unroll
@@ -567,8 +584,8 @@ __device__ __forceinline__ void rate_block_f32(const GridDev &g, const float4 *_
 #pragma unroll
         for (int k = 0; k < 4; k++) nsfu = max(nsfu, i0 + k < nq ? S.nsfu[kServed ? S.q[i0 + k] : i0 + k] : 0);
         float part[6];
-        ray_bins_packed(pairs, specn + (size_t)S.e[q] * kNu, j, nsfu, S.nd[q][0], S.nd[q][1], S.nd[q][2], S.nd[q][3],
-                        S.nd[q][4], S.nd[q][5], part);
+        ray_bins_packed(pairs, specn + (size_t)S.e[q] * kNu, j, nsfu, S.nsfu[q], S.nd[q][0], S.nd[q][1], S.nd[q][2],
+                        S.nd[q][3], S.nd[q][4], S.nd[q][5], part);
 #pragma unroll
         for (int o = 1; o < 8; o <<= 1) {
 #pragma unroll

@@ -192,20 +192,36 @@ def test_reference_fast_math_spread(oracle):
     assert np.max(rel) < 1e-3
 
 
-def test_phi_polynomial_matches_fit_and_bound():
-    """The coefficients of the FP32 rate kernel's photon-conserving factor
-    (photoion.cuh kPhiC, a polynomial in u = x / ln 2) are the ones
-    argot_b200/fits.py makes, and their FP32 Horner evaluation stays within
-    1.5e-7 of (1 - e^-x)/x for x in [0, 1]."""
+def test_phi_threshold_of_the_sfu_form():
+    """The FP32 rate kernel takes the SFU form of the photon-conserving
+    factor at x >= kPhiXMax, tested in u = x / ln 2 against kPhiUMax."""
     import os
     import re
     from argot_b200 import fits
     from conftest import ROOT
     src = open(os.path.join(ROOT, "argot_b200", "csrc", "photoion.cuh")).read()
-    body = re.search(r"kPhiC\[7\]\s*=\s*\{([^}]*)\}", src).group(1)
-    c = np.array([float(v.strip().rstrip("f")) for v in body.split(",")], np.float32)
-    assert np.array_equal(c, fits.fit_phi(scale=fits.LN2))
     assert float(re.search(r"kPhiXMax\s*=\s*([0-9.]+)f", src).group(1)) == fits.PHI_X_MAX
     umax = float(re.search(r"kPhiUMax\s*=\s*([0-9.]+)f", src).group(1))
     assert np.float32(umax) == np.float32(fits.PHI_X_MAX / fits.LN2)
-    assert fits.phi_error(c, scale=fits.LN2) < 1.5e-7
+
+
+def test_mid_cell_polynomial_matches_fit_and_bound():
+    """The kernel's sinh(y)/y polynomial in v = u^2 (photoion.cuh kShc, the
+    bins below x = 1) is the one argot_b200/fits.py makes, and the mid-cell
+    attenuation 2^(-u/2) times its FP32 Horner evaluation stays within
+    1.6e-7 of (1 - e^-x)/x for x in [0, 1]; the identity behind it,
+    e^-tau phi(x) = e^-(tau + x/2) sinh(x/2)/(x/2), holds in float64."""
+    import os
+    import re
+    from argot_b200 import fits
+    from conftest import ROOT
+    src = open(os.path.join(ROOT, "argot_b200", "csrc", "photoion.cuh")).read()
+    body = re.search(r"kShc\[4\]\s*=\s*\{([^}]*)\}", src).group(1)
+    c = np.array([float(v.strip().rstrip("f")) for v in body.split(",")], np.float32)
+    assert np.array_equal(c, fits.fit_sinhc())
+    assert fits.mid_cell_error(c) < 1.6e-7
+    x = np.linspace(1e-6, 1.0, 1001)
+    tau = 3.0
+    lhs = np.exp(-tau) * fits.phi(x)
+    rhs = np.exp(-(tau + x / 2)) * fits.sinhc_half(x / fits.LN2)
+    assert np.max(np.abs(lhs - rhs) / lhs) < 1e-14
