@@ -57,7 +57,6 @@ struct RateTables {
   float cs_l2e[3][kNu];   // sigma_s(nu) * log2(e)
   float hw[3][kNu];       // sigma_s(nu) * max((float)nu - nu_s, 0)
   float smax16[3][16];    // max of sigma_s(nu) over the bins k >= 16 i
-  float rpow[16];         // (float) 10^(16 i dlog_nu): nu of bin k + 16 i over nu of bin k
 };
 // Uploads the tables to the constant bank of the translation unit that owns
 // the rate kernels (photoion.cu), once per device.

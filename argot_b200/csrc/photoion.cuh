@@ -39,7 +39,6 @@ static int ensure_rate_tables(int device) {
   }
   // nu_(k + 16 i) = nu_k 10^(16 i dlog_nu): the bins of the frequency grid
   // are equally spaced in log nu (source.c:38-53)
-  for (int i = 0; i < 16; i++) t.rpow[i] = (float)(nu[16 * i] / nu[0]);
   for (int s = 0; s < 3; s++) {
     float m = 0.f;
     for (int k = kNu - 1; k >= 0; k--) {
@@ -196,28 +195,31 @@ __device__ __forceinline__ void ray_rates6(const float (&P)[3], float a0, float 
 }
 
 // ---- packed FP32 bin loop: two bins per instruction with the f32x2 FMA
-// and multiply of sm_100.  An 8-lane group integrates one ray; lane j owns
-// the bin pairs (j + 16 i, j + 16 i + 8), i = 0..15 (the bins j + 8 m), and
-// keeps one partial sum per output and pair member.
-// The pair table holds sigma_s log2(e) of the three species of the two
-// bins, 24 bytes, three 8-byte shared loads per pair; nu of the pair's bins
-// is the lane's first pair times the grid ratio 10^(16 i dlog_nu) (the
-// frequency grid is equally spaced in log nu), one packed multiply, within
-// 2 ulp of the (float) nu the reference compares.  The sums run on these
-// entries: sum sigma_s w = ln2 sum (sigma_s log2 e) w, and, because
+// and multiply of sm_100.  An 8-lane group integrates one ray (or two,
+// ray_bins_packed2); lane j owns the bin pairs (j + 16 i, j + 16 i + 8),
+// i = 0..15 (the bins j + 8 m), and keeps one partial sum per output, pair
+// member and ray.
+// The pair table holds, for the three species and the two bins,
+// sigma_s log2(e) and sigma_s log2(e) nu, 48 bytes, three 16-byte shared
+// loads per pair, each serving the two rays of the lane.  The sums run on
+// these entries: sum sigma_s w = ln2 sum (sigma_s log2 e) w, and, because
 // sigma_s vanishes below the species' threshold nu_s (the fits of
 // prim_chem/cross_section.c are 0 there), the heating sum
 // sum sigma_s (nu - nu_s)^+ w = ln2 (sum (sigma_s log2 e) nu w - nu_s
 // sum (sigma_s log2 e) w).  A shared load delivers 128 bytes per wavefront
 // whatever the broadcast (the four groups of a warp read the same
-// entries), so the table's bytes per lane set the kernel's shared-memory
-// traffic, which shares the L1 data path with the spectrum loads: the
-// earlier 80-byte entry (sigma log2 e, sigma and sigma (nu - nu_s)^+ per
-// species) kept the shared-memory pipe at 79% of its peak (ncu, 256^3 / 16
-// sources); dropping nu from the 32-byte entry took the 256^3 / 4096-source
-// rates from 1.02 s to 0.93 s.
-struct alignas(8) BinPair {
-  float2 l2e[3];  // sigma_s log2(e) of the two bins
+// entries), so the table's bytes per ray set the kernel's shared-memory
+// traffic, which shares the L1 data path with the spectrum loads.
+// Measured at 256^3 / 4096 sources: with one ray per lane, an 80-byte
+// entry (sigma log2 e, sigma and sigma (nu - nu_s)^+ per species) kept the
+// shared-memory pipe at 79% of its peak, and a 24-byte entry without the
+// nu products (nu formed from the lane's first pair and the grid ratio,
+// two packed multiplies per pair and ray) ran the rates in 0.93 s against
+// 1.02 s for 32 bytes; with two rays per lane this 48-byte entry, which
+// saves those multiplies, runs them in 0.78 s against 0.81 s for 24 bytes.
+struct alignas(16) BinPair {
+  float2 l2e[3];    // sigma_s log2(e) of the two bins
+  float2 l2enu[3];  // sigma_s log2(e) nu
 };
 constexpr int kBinPairs = kNu / 2;
 
@@ -229,7 +231,10 @@ __device__ __forceinline__ void load_bin_pairs(BinPair *tab) {
     const int k0 = j + 16 * i, k1 = k0 + 8;
     BinPair b;
 #pragma unroll
-    for (int s = 0; s < 3; s++) b.l2e[s] = make_float2(c_tab.cs_l2e[s][k0], c_tab.cs_l2e[s][k1]);
+    for (int s = 0; s < 3; s++) {
+      b.l2e[s] = make_float2(c_tab.cs_l2e[s][k0], c_tab.cs_l2e[s][k1]);
+      b.l2enu[s] = make_float2(c_tab.cs_l2e[s][k0] * c_tab.nu_f[k0], c_tab.cs_l2e[s][k1] * c_tab.nu_f[k1]);
+    }
     tab[p] = b;
   }
 }
@@ -286,7 +291,7 @@ __device__ __forceinline__ int sfu_iters(float D0, float D1, float D2) {
 // bin's value depends on its own ray alone, whichever other rays share the
 // loop's round.
 template <bool kSfu>
-__device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, float2 nu, float2 n0, float2 n1, float2 n2,
+__device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, float2 n0, float2 n1, float2 n2,
                                          float2 d0, float2 d1, float2 d2, float2 (&acc)[6], bool sfu = false) {
   const float2 l0 = b.l2e[0], l1 = b.l2e[1], l2 = b.l2e[2];
   const float2 ntm = __ffma2_rn(n0, l0, __ffma2_rn(n1, l1, __fmul2_rn(n2, l2)));
@@ -304,13 +309,12 @@ __device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, float2 nu, 
       w.y = t1 ? w.y : q1;
     }
   }
-  const float2 vw = __fmul2_rn(nu, w);
   acc[0] = __ffma2_rn(l0, w, acc[0]);
   acc[1] = __ffma2_rn(l1, w, acc[1]);
   acc[2] = __ffma2_rn(l2, w, acc[2]);
-  acc[3] = __ffma2_rn(l0, vw, acc[3]);
-  acc[4] = __ffma2_rn(l1, vw, acc[4]);
-  acc[5] = __ffma2_rn(l2, vw, acc[5]);
+  acc[3] = __ffma2_rn(b.l2enu[0], w, acc[3]);
+  acc[4] = __ffma2_rn(b.l2enu[1], w, acc[4]);
+  acc[5] = __ffma2_rn(b.l2enu[2], w, acc[5]);
 }
 
 // The lane's six partial sums of one ray with columns N (to the cell) and
@@ -333,21 +337,12 @@ __device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab,
   float2 acc[6];
 #pragma unroll
   for (int q = 0; q < 6; q++) acc[q] = make_float2(0.f, 0.f);
-  // nu of the pair's bins from the lane's first pair and the grid ratio
-  const float2 nu0 = make_float2(c_tab.nu_f[j], c_tab.nu_f[j + 8]);
   int i = 0;
 #pragma unroll 2
-  for (; i < nsfu; i++) {
-    const float r = c_tab.rpow[i];
-    bin_pair<true>(tab[j + 8 * i], __ldg(sp2 + 8 * i), __fmul2_rn(nu0, make_float2(r, r)), n0, n1, n2, d0, d1, d2,
-                   acc, i < own);
-  }
+  for (; i < nsfu; i++)
+    bin_pair<true>(tab[j + 8 * i], __ldg(sp2 + 8 * i), n0, n1, n2, d0, d1, d2, acc, i < own);
 #pragma unroll 4
-  for (; i < kBinPairs / 8; i++) {
-    const float r = c_tab.rpow[i];
-    bin_pair<false>(tab[j + 8 * i], __ldg(sp2 + 8 * i), __fmul2_rn(nu0, make_float2(r, r)), n0, n1, n2, d0, d1, d2,
-                    acc);
-  }
+  for (; i < kBinPairs / 8; i++) bin_pair<false>(tab[j + 8 * i], __ldg(sp2 + 8 * i), n0, n1, n2, d0, d1, d2, acc);
 #pragma unroll
   for (int q = 0; q < 6; q++) out[q] = acc[q].x + acc[q].y;
 }
@@ -373,23 +368,18 @@ __device__ __forceinline__ void ray_bins_packed2(const BinPair *__restrict__ tab
   float2 acca[6], accb[6];
 #pragma unroll
   for (int q = 0; q < 6; q++) acca[q] = accb[q] = make_float2(0.f, 0.f);
-  const float2 nu0 = make_float2(c_tab.nu_f[j], c_tab.nu_f[j + 8]);
   int i = 0;
 #pragma unroll 1
   for (; i < nsfu; i++) {
-    const float r = c_tab.rpow[i];
-    const float2 nu = __fmul2_rn(nu0, make_float2(r, r));
     const BinPair b = tab[j + 8 * i];
-    bin_pair<true>(b, __ldg(sa + 8 * i), nu, a0, a1, a2, da0, da1, da2, acca, i < owna);
-    bin_pair<true>(b, __ldg(sb + 8 * i), nu, b0, b1, b2, db0, db1, db2, accb, i < ownb);
+    bin_pair<true>(b, __ldg(sa + 8 * i), a0, a1, a2, da0, da1, da2, acca, i < owna);
+    bin_pair<true>(b, __ldg(sb + 8 * i), b0, b1, b2, db0, db1, db2, accb, i < ownb);
   }
 #pragma unroll 2
   for (; i < kBinPairs / 8; i++) {
-    const float r = c_tab.rpow[i];
-    const float2 nu = __fmul2_rn(nu0, make_float2(r, r));
     const BinPair b = tab[j + 8 * i];
-    bin_pair<false>(b, __ldg(sa + 8 * i), nu, a0, a1, a2, da0, da1, da2, acca);
-    bin_pair<false>(b, __ldg(sb + 8 * i), nu, b0, b1, b2, db0, db1, db2, accb);
+    bin_pair<false>(b, __ldg(sa + 8 * i), a0, a1, a2, da0, da1, da2, acca);
+    bin_pair<false>(b, __ldg(sb + 8 * i), b0, b1, b2, db0, db1, db2, accb);
   }
 #pragma unroll
   for (int q = 0; q < 6; q++) {
