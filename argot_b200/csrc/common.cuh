@@ -57,6 +57,9 @@ struct RateTables {
   float cs_l2e[3][kNu];   // sigma_s(nu) * log2(e)
   float hw[3][kNu];       // sigma_s(nu) * max((float)nu - nu_s, 0)
   float smax16[3][16];    // max of sigma_s(nu) over the bins k >= 16 i
+  // the bin loop's iterations (16 bins each) before iter_he have sigma_HeI =
+  // sigma_HeII = 0 in every bin, those before iter_heii sigma_HeII = 0
+  int iter_he, iter_heii;
 };
 // Uploads the tables to the constant bank of the translation unit that owns
 // the rate kernels (photoion.cu), once per device.

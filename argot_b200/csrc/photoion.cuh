@@ -1,6 +1,7 @@
 // photoion.cuh -- per-ray photo-ionisation / heating rates
 // (calc_photoion_rate, photon-conserving branch, H + He, not cosmological).
 #pragma once
+#include <algorithm>
 #include <mutex>
 
 #include "march.cuh"
@@ -37,15 +38,21 @@ static int ensure_rate_tables(int device) {
       t.hw[s][i] = (float)((double)c * w);
     }
   }
-  // nu_(k + 16 i) = nu_k 10^(16 i dlog_nu): the bins of the frequency grid
-  // are equally spaced in log nu (source.c:38-53)
+  // suffix maxima of the cross sections per 16-bin iteration (sfu_iters)
+  // and the iterations below the helium thresholds (sigma_s is 0 below
+  // nu_s in the fits of prim_chem/cross_section.c)
+  int first[3];
   for (int s = 0; s < 3; s++) {
     float m = 0.f;
+    first[s] = kNu / 16;
     for (int k = kNu - 1; k >= 0; k--) {
       m = fmaxf(m, t.cs[s][k]);
       if (k % 16 == 0) t.smax16[s][k / 16] = m;
+      if (t.cs[s][k] != 0.f) first[s] = k / 16;
     }
   }
+  t.iter_heii = first[2];
+  t.iter_he = std::min(first[1], first[2]);
   ARGOT_CUDA_TRY(cudaMemcpyToSymbol(c_tab, &t, sizeof(t)));
   done[device] = true;
   return 0;
@@ -283,19 +290,42 @@ __device__ __forceinline__ int sfu_iters(float D0, float D1, float D2) {
   return n;
 }
 
-// One iteration of ray_bins_packed: the bin pair p of the lane.  n0..n2
-// hold the negated mid-cell columns -(N_s + D_s / 2), so that
+// A ray's columns as the bin loop uses them, each value in both halves of
+// a float2: n = the negated mid-cell columns -(N_s + D_s / 2), d = the
+// cell's columns D_s [cm^-2].
+struct RayCols2 {
+  float2 n[3], d[3];
+};
+__device__ __forceinline__ RayCols2 ray_cols2(float N0, float N1, float N2, float D0, float D1, float D2) {
+  const float N[3] = {N0, N1, N2}, D[3] = {D0, D1, D2};
+  RayCols2 c;
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    const float m = -fmaf(0.5f, D[q], N[q]);
+    c.n[q] = make_float2(m, m);
+    c.d[q] = make_float2(D[q], D[q]);
+  }
+  return c;
+}
+
+// One iteration of the bin loop: the bin pair of the lane for one ray.
 // ntm = -(tau + x / 2) log2(e) and w = s 2^ntm sinh(x/2)/(x/2).  With kSfu
 // and `sfu` (an iteration below the ray's own sfu_iters count) a bin with
 // x >= kPhiXMax takes w = s 2^(ntm + dl/2) (1 - 2^-dl) / x instead.  A
 // bin's value depends on its own ray alone, whichever other rays share the
-// loop's round.
-template <bool kSfu>
-__device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, float2 n0, float2 n1, float2 n2,
-                                         float2 d0, float2 d1, float2 d2, float2 (&acc)[6], bool sfu = false) {
-  const float2 l0 = b.l2e[0], l1 = b.l2e[1], l2 = b.l2e[2];
-  const float2 ntm = __ffma2_rn(n0, l0, __ffma2_rn(n1, l1, __fmul2_rn(n2, l2)));
-  const float2 dl = __ffma2_rn(d0, l0, __ffma2_rn(d1, l1, __fmul2_rn(d2, l2)));
+// loop's round.  kNS: the species whose cross sections can be non-zero in
+// the iteration (1: HI, 2: HI and HeI, 3: all; the others are 0 there and
+// their terms would add exact zeros, so the sums are the same bit for bit).
+template <bool kSfu, int kNS>
+__device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, const RayCols2 &c, float2 (&acc)[6],
+                                         bool sfu = false) {
+  float2 ntm = __fmul2_rn(c.n[kNS - 1], b.l2e[kNS - 1]);
+  float2 dl = __fmul2_rn(c.d[kNS - 1], b.l2e[kNS - 1]);
+#pragma unroll
+  for (int q = kNS - 2; q >= 0; q--) {
+    ntm = __ffma2_rn(c.n[q], b.l2e[q], ntm);
+    dl = __ffma2_rn(c.d[q], b.l2e[q], dl);
+  }
   const float2 e = make_float2(ex2_approx(ntm.x), ex2_approx(ntm.y));
   float2 w = __fmul2_rn(__fmul2_rn(s, e), sinhc_half2(dl));
   if (kSfu) {
@@ -309,82 +339,102 @@ __device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, float2 n0, 
       w.y = t1 ? w.y : q1;
     }
   }
-  acc[0] = __ffma2_rn(l0, w, acc[0]);
-  acc[1] = __ffma2_rn(l1, w, acc[1]);
-  acc[2] = __ffma2_rn(l2, w, acc[2]);
-  acc[3] = __ffma2_rn(b.l2enu[0], w, acc[3]);
-  acc[4] = __ffma2_rn(b.l2enu[1], w, acc[4]);
-  acc[5] = __ffma2_rn(b.l2enu[2], w, acc[5]);
+#pragma unroll
+  for (int q = 0; q < kNS; q++) {
+    acc[q] = __ffma2_rn(b.l2e[q], w, acc[q]);
+    acc[3 + q] = __ffma2_rn(b.l2enu[q], w, acc[3 + q]);
+  }
 }
 
-// The lane's six partial sums of one ray with columns N (to the cell) and
-// D (of the cell) in cm^-2; sp: the emitter's normalised spectrum; j: the
-// lane in the ray's 8-lane group; the first nsfu iterations are compiled
+// Unroll factor of the polynomial-only iterations (measured at 256^3 / 4096
+// sources with two rays per lane: 4 runs the rates 2% faster than 2, at 128
+// registers without spills).
+#ifndef ARGOT_RATE_UNROLL
+#define ARGOT_RATE_UNROLL 4
+#endif
+constexpr int kRateUnroll = ARGOT_RATE_UNROLL;
+
+// Iterations [i0, i1) of the bin loop for kR rays (1 or 2) of the lane;
+// one load of a table entry serves the kR rays.
+template <int kR, bool kSfu, int kNS>
+__device__ __forceinline__ void bin_iters(const BinPair *__restrict__ tab, const float2 *const (&sp)[kR], int j,
+                                          int i0, int i1, const int (&own)[kR], const RayCols2 (&c)[kR],
+                                          float2 (&acc)[kR][6]) {
+#pragma unroll(kSfu ? 1 : kRateUnroll)
+  for (int i = i0; i < i1; i++) {
+    const BinPair b = tab[j + 8 * i];
+#pragma unroll
+    for (int r = 0; r < kR; r++) bin_pair<kSfu, kNS>(b, __ldg(sp[r] + 8 * i), c[r], acc[r], i < own[r]);
+  }
+}
+
+// The lane's six partial sums of kR rays (1 or 2) from the columns c; sp:
+// the emitters' normalised spectra as bin pairs, offset to the lane; j: the
+// lane in the rays' 8-lane group; the first nsfu iterations are compiled
 // with the SFU form (the caller passes the same count, the round's largest
 // sfu_iters, to the four groups of the warp, so that their loops stay
-// converged), which the ray takes in its own first `own` (its sfu_iters):
-// out[s] = sum (sigma_s log2 e) w, out[3 + s] = sum (sigma_s log2 e) nu w
-// over the lane's bins, w = s_nu e^-tau phi(dtau).  The caller adds the
+// converged), which a ray takes in its own first own[r] (its sfu_iters);
+// the loop runs in three stretches by the species present (iter_he,
+// iter_heii of the tables), in increasing iteration order:
+// out[r][s] = sum (sigma_s log2 e) w, out[r][3 + s] = sum (sigma_s log2 e)
+// nu w over the lane's bins, w = s_nu e^-tau phi(dtau).  The caller adds the
 // eight lanes and forms the rates (ray_rates6).
+template <int kR>
+__device__ __forceinline__ void ray_bins(const BinPair *__restrict__ tab, const float2 *const (&sp)[kR], int j,
+                                         int nsfu, const int (&own)[kR], const RayCols2 (&c)[kR],
+                                         float (&out)[kR][6]) {
+  float2 acc[kR][6];
+#pragma unroll
+  for (int r = 0; r < kR; r++)
+#pragma unroll
+    for (int q = 0; q < 6; q++) acc[r][q] = make_float2(0.f, 0.f);
+  constexpr int kIters = kBinPairs / 8;
+  const int h1 = c_tab.iter_he, h2 = c_tab.iter_heii;
+  const int s1 = min(nsfu, h1), s2 = min(max(nsfu, h1), h2), s3 = max(nsfu, h2);
+  bin_iters<kR, true, 1>(tab, sp, j, 0, s1, own, c, acc);
+  bin_iters<kR, false, 1>(tab, sp, j, s1, h1, own, c, acc);
+  bin_iters<kR, true, 2>(tab, sp, j, h1, s2, own, c, acc);
+  bin_iters<kR, false, 2>(tab, sp, j, s2, h2, own, c, acc);
+  bin_iters<kR, true, 3>(tab, sp, j, h2, min(s3, kIters), own, c, acc);
+  bin_iters<kR, false, 3>(tab, sp, j, s3, kIters, own, c, acc);
+#pragma unroll
+  for (int r = 0; r < kR; r++)
+#pragma unroll
+    for (int q = 0; q < 6; q++) out[r][q] = acc[r][q].x + acc[r][q].y;
+}
+
+// One ray: columns N (to the cell) and D (of the cell) in cm^-2, sp the
+// emitter's normalised spectrum.
 __device__ __forceinline__ void ray_bins_packed(const BinPair *__restrict__ tab, const float *__restrict__ sp,
                                                 int j, int nsfu, int own, float N0, float N1, float N2, float D0,
                                                 float D1, float D2, float (&out)[6]) {
-  const float m0 = -fmaf(0.5f, D0, N0), m1 = -fmaf(0.5f, D1, N1), m2 = -fmaf(0.5f, D2, N2);
-  const float2 n0 = make_float2(m0, m0), n1 = make_float2(m1, m1), n2 = make_float2(m2, m2);
-  const float2 d0 = make_float2(D0, D0), d1 = make_float2(D1, D1), d2 = make_float2(D2, D2);
   // the pair's two spectrum bins in one 8-byte load (pair order)
-  const float2 *__restrict__ sp2 = reinterpret_cast<const float2 *>(sp) + j;
-  float2 acc[6];
+  const float2 *const sp2[1] = {reinterpret_cast<const float2 *>(sp) + j};
+  const int own1[1] = {own};
+  const RayCols2 c[1] = {ray_cols2(N0, N1, N2, D0, D1, D2)};
+  float o[1][6];
+  ray_bins<1>(tab, sp2, j, nsfu, own1, c, o);
 #pragma unroll
-  for (int q = 0; q < 6; q++) acc[q] = make_float2(0.f, 0.f);
-  int i = 0;
-#pragma unroll 2
-  for (; i < nsfu; i++)
-    bin_pair<true>(tab[j + 8 * i], __ldg(sp2 + 8 * i), n0, n1, n2, d0, d1, d2, acc, i < own);
-#pragma unroll 4
-  for (; i < kBinPairs / 8; i++) bin_pair<false>(tab[j + 8 * i], __ldg(sp2 + 8 * i), n0, n1, n2, d0, d1, d2, acc);
-#pragma unroll
-  for (int q = 0; q < 6; q++) out[q] = acc[q].x + acc[q].y;
+  for (int q = 0; q < 6; q++) out[q] = o[0][q];
 }
 
-// ray_bins_packed for two rays at once (columns nd = N0, N1, N2, D0, D1,
-// D2 of each, own SFU counts owna, ownb): one load of each bin pair of the
-// table serves both rays, which halves the shared-memory traffic per ray;
-// nsfu covers both.
+// Two rays (columns nd = N0, N1, N2, D0, D1, D2 of each, own SFU counts
+// owna, ownb): one load of each bin pair of the table serves both rays,
+// which halves the shared-memory traffic per ray; nsfu covers both.
 __device__ __forceinline__ void ray_bins_packed2(const BinPair *__restrict__ tab, const float *__restrict__ spa,
                                                  const float *__restrict__ spb, int j, int nsfu, int owna,
                                                  int ownb, const float *nda, const float *ndb, float (&outa)[6],
                                                  float (&outb)[6]) {
-  const float ma0 = -fmaf(0.5f, nda[3], nda[0]), ma1 = -fmaf(0.5f, nda[4], nda[1]),
-              ma2 = -fmaf(0.5f, nda[5], nda[2]);
-  const float mb0 = -fmaf(0.5f, ndb[3], ndb[0]), mb1 = -fmaf(0.5f, ndb[4], ndb[1]),
-              mb2 = -fmaf(0.5f, ndb[5], ndb[2]);
-  const float2 a0 = make_float2(ma0, ma0), a1 = make_float2(ma1, ma1), a2 = make_float2(ma2, ma2);
-  const float2 da0 = make_float2(nda[3], nda[3]), da1 = make_float2(nda[4], nda[4]), da2 = make_float2(nda[5], nda[5]);
-  const float2 b0 = make_float2(mb0, mb0), b1 = make_float2(mb1, mb1), b2 = make_float2(mb2, mb2);
-  const float2 db0 = make_float2(ndb[3], ndb[3]), db1 = make_float2(ndb[4], ndb[4]), db2 = make_float2(ndb[5], ndb[5]);
-  const float2 *__restrict__ sa = reinterpret_cast<const float2 *>(spa) + j;
-  const float2 *__restrict__ sb = reinterpret_cast<const float2 *>(spb) + j;
-  float2 acca[6], accb[6];
-#pragma unroll
-  for (int q = 0; q < 6; q++) acca[q] = accb[q] = make_float2(0.f, 0.f);
-  int i = 0;
-#pragma unroll 1
-  for (; i < nsfu; i++) {
-    const BinPair b = tab[j + 8 * i];
-    bin_pair<true>(b, __ldg(sa + 8 * i), a0, a1, a2, da0, da1, da2, acca, i < owna);
-    bin_pair<true>(b, __ldg(sb + 8 * i), b0, b1, b2, db0, db1, db2, accb, i < ownb);
-  }
-#pragma unroll 2
-  for (; i < kBinPairs / 8; i++) {
-    const BinPair b = tab[j + 8 * i];
-    bin_pair<false>(b, __ldg(sa + 8 * i), a0, a1, a2, da0, da1, da2, acca);
-    bin_pair<false>(b, __ldg(sb + 8 * i), b0, b1, b2, db0, db1, db2, accb);
-  }
+  const float2 *const sp2[2] = {reinterpret_cast<const float2 *>(spa) + j, reinterpret_cast<const float2 *>(spb) + j};
+  const int own[2] = {owna, ownb};
+  const RayCols2 c[2] = {ray_cols2(nda[0], nda[1], nda[2], nda[3], nda[4], nda[5]),
+                         ray_cols2(ndb[0], ndb[1], ndb[2], ndb[3], ndb[4], ndb[5])};
+  float o[2][6];
+  ray_bins<2>(tab, sp2, j, nsfu, own, c, o);
 #pragma unroll
   for (int q = 0; q < 6; q++) {
-    outa[q] = acca[q].x + acca[q].y;
-    outb[q] = accb[q].x + accb[q].y;
+    outa[q] = o[0][q];
+    outb[q] = o[1][q];
   }
 }
 
