@@ -195,6 +195,17 @@ __device__ __forceinline__ void kahan_slot(float *slot, int q, float v) {
   slot[(q + NC) * kStride] = c;
 }
 
+// The step of one axis in the end-tested walk: when the axis's next face
+// is the nearest (h == m), its face position t moves on by the spacing T
+// and the cell index by ds.  Written as two predicated adds, where the
+// compiler's form (both sums formed, then selected) took twice the
+// instructions (ncu, 256^3 / 4096 sources: march 0.98 s -> 0.93 s).
+__device__ __forceinline__ void advance_if_hit(uint64_t &t, int &idx, uint32_t h, uint32_t m, uint64_t T, int ds) {
+  asm("{\n\t.reg .pred p;\n\tsetp.eq.u32 p, %2, %3;\n\t@p add.u64 %0, %0, %4;\n\t@p add.s32 %1, %1, %5;\n\t}"
+      : "+l"(t), "+r"(idx)
+      : "r"(h), "r"(m), "l"(T), "r"(ds));
+}
+
 __device__ __forceinline__ uint64_t fixed_32_32(double units) {
   return (uint64_t)__double2ull_rz(units * 4294967296.0);
 }
@@ -258,6 +269,18 @@ static __device__ __forceinline__ Cols<NC> march_kahan_n(const GridDev &g, const
       const uint32_t xh = (uint32_t)(tx >> 32), yh = (uint32_t)(ty >> 32), zh = (uint32_t)(tz >> 32);
       const uint32_t m = min(xh, min(yh, zh));
       if (kCentreEnd ? m >= lu : !(cx | cy | cz)) break;
+      if (kCentreEnd) {
+        float n[NC];
+        ld_cols<NC>(cells, (size_t)idx, n);
+        advance_if_hit(tx, idx, xh, m, Tx, dsx);
+        advance_if_hit(ty, idx, yh, m, Ty, dsy);
+        advance_if_hit(tz, idx, zh, m, Tz, dsz);
+        const float rf = __uint2float_rn(m - t);
+        t = m;
+#pragma unroll
+        for (int q = 0; q < NC; q++) p[q] = fmaf(rf, n[q], p[q]);
+        continue;
+      }
       const bool hx = xh == m, hy = yh == m, hz = zh == m;
       float n[NC];
       ld_cols<NC>(cells, (size_t)idx, n);
@@ -266,16 +289,10 @@ static __device__ __forceinline__ Cols<NC> march_kahan_n(const GridDev &g, const
       t = m;
 #pragma unroll
       for (int q = 0; q < NC; q++) p[q] = fmaf(rf, n[q], p[q]);
-      if (kCentreEnd) {
-        if (hx) tx += Tx;
-        if (hy) ty += Ty;
-        if (hz) tz += Tz;
-      } else {
-        cx -= hx; cy -= hy; cz -= hz;
-        if (hx) tx = cx ? tx + Tx : kNone;
-        if (hy) ty = cy ? ty + Ty : kNone;
-        if (hz) tz = cz ? tz + Tz : kNone;
-      }
+      cx -= hx; cy -= hy; cz -= hz;
+      if (hx) tx = cx ? tx + Tx : kNone;
+      if (hy) ty = cy ? ty + Ty : kNone;
+      if (hz) tz = cz ? tz + Tz : kNone;
     }
     it += kk;
     if (kk < 16) break;
