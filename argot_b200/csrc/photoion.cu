@@ -83,10 +83,10 @@ __global__ void __launch_bounds__(32 * kRateWarps)
 // One warp per target block, rays in chunks of 32.  Phase A: lane i forms
 // the FP32 per-ray parameters of ray i of the chunk (ray_params_f32).
 // Phase B: the warp splits into four groups of eight lanes; a group takes
-// one ray at a time and its lanes share the 256 frequency bins (lane j:
-// bins j, j+8, ..., two at a time with the packed f32x2 arithmetic,
-// ray_bins_packed), reading the bin-pair table from shared memory; three
-// butterfly steps sum the eight partial sums.  Phase C: every lane adds the
+// ARGOT_RATE_RAYS_PER_LANE rays at a time and its lanes share the 256
+// frequency bins (lane j: bins j, j+8, ..., two at a time with the packed
+// f32x2 arithmetic, ray_bins_packed2), reading the bin-pair table from
+// shared memory; three butterfly steps sum the eight partial sums.  Phase C: every lane adds the
 // rays that end in its cell, in ray order (add_chunk_in_order).  The
 // kernel has no FP64 arithmetic.
 // Launch shape: ARGOT_RATE_WARPS warps per CTA, at least ARGOT_RATE_MIN_CTAS
@@ -95,12 +95,17 @@ __global__ void __launch_bounds__(32 * kRateWarps)
 // B200 (256^3, 4096 sources, 3.2e9 rays) with the per-cell sums in shared
 // memory: one ray per group, 8 warps x 3 CTAs (80 registers, no spills)
 // 0.93 s; two rays per group, 8 warps x 2 CTAs (112 registers) 0.85 s,
-// x 3 CTAs (80 registers, spilling) 0.94 s.
+// x 3 CTAs (80 registers, spilling) 0.94 s.  With the later bin loop (the
+// mid-cell form, the 48-byte table, the species stretches, 4-fold unroll)
+// two rays per group at 8 warps x 2 CTAs (126 registers) take 0.75 s, at
+// 4 warps x 4 CTAs 0.78 s; but the smaller CTAs share the SMs better with
+// the march in the overlapped step, which runs 1.2% faster with them
+// (1.437 s against 1.454 s).
 #ifndef ARGOT_RATE_WARPS
-#define ARGOT_RATE_WARPS 8
+#define ARGOT_RATE_WARPS 4
 #endif
 #ifndef ARGOT_RATE_MIN_CTAS
-#define ARGOT_RATE_MIN_CTAS 2
+#define ARGOT_RATE_MIN_CTAS 4
 #endif
 #ifndef ARGOT_RATE_RAYS_PER_LANE
 #define ARGOT_RATE_RAYS_PER_LANE 2
