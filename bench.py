@@ -42,12 +42,12 @@ ART_UENETOK = 1.0e4
 METRIC = "ray-cell crossings/s (march+stitch+rates, 1 B200)"
 # DRAM bytes per ray-cell crossing of k_march_rays<Kahan> measured by ncu on
 # the 256^3 / 16-source case (dram__bytes_read.sum + dram__bytes_write.sum =
-# 119.9 + 18.3 GB over a 109.7 ms launch for 6.030e10 crossings); the
+# 104.7 + 17.4 GB over a 104.1 ms launch for 6.030e10 crossings); the
 # workloads here are too large to capture, so `traffic` scales this figure.
-MARCH_DRAM_BYTES_PER_CROSSING = 2.292
-# the same capture's L2 bytes (lts__t_sectors.sum x 32 B, 402.0 GB over the
+MARCH_DRAM_BYTES_PER_CROSSING = 2.024
+# the same capture's L2 bytes (lts__t_sectors.sum x 32 B, 413.0 GB over the
 # launch's 6.030e10 crossings): what the L2 serves per crossing
-MARCH_L2_BYTES_PER_CROSSING = 6.666
+MARCH_L2_BYTES_PER_CROSSING = 6.848
 UNIT = "crossings/s"
 
 
@@ -594,8 +594,8 @@ def run_ours(args):
                                         f"scaled by this launch's crossings"),
                      "dram_gbs": MARCH_DRAM_BYTES_PER_CROSSING * n_cross / t_march / 1e9,
                      "dram_frac": MARCH_DRAM_BYTES_PER_CROSSING * n_cross / t_march / 1e9 / hbm,
-                     "limiter": ("latency of the L1/L2-hit gathers (ncu: long-scoreboard stalls 13.6 per issue, "
-                                 "issue active 61%); DRAM moves 2.3 B and L2 serves 6.7 B of the 16 B per "
+                     "limiter": ("latency of the L1/L2-hit gathers (ncu: long-scoreboard stalls 14.1 per issue, "
+                                 "issue active 60%); DRAM moves 2.0 B and L2 serves 6.8 B of the 16 B per "
                                  "crossing that the bytes model counts"),
                      "algorithmic_bytes": alg_bytes,
                      "bytes_model": "16 B per crossing + 36 B per ray"},
