@@ -100,12 +100,15 @@ __global__ void __launch_bounds__(32 * kRateWarps)
 // two rays per group at 8 warps x 2 CTAs (126 registers) take 0.75 s, at
 // 4 warps x 4 CTAs 0.78 s; but the smaller CTAs share the SMs better with
 // the march in the overlapped step, which runs 1.2% faster with them
-// (1.437 s against 1.454 s).
+// (1.437 s against 1.454 s); 4 warps x 5 CTAs (96 registers, the
+// polynomial iterations unrolled twice, no spills) run the rates alone in
+// the same time and the step 2.3% faster again (1.403 s; unrolled four
+// times at 5 CTAs the loop spills: rates 0.83 s, step 1.435 s).
 #ifndef ARGOT_RATE_WARPS
 #define ARGOT_RATE_WARPS 4
 #endif
 #ifndef ARGOT_RATE_MIN_CTAS
-#define ARGOT_RATE_MIN_CTAS 4
+#define ARGOT_RATE_MIN_CTAS 5
 #endif
 #ifndef ARGOT_RATE_RAYS_PER_LANE
 #define ARGOT_RATE_RAYS_PER_LANE 2

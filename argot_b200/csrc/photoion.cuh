@@ -347,10 +347,11 @@ __device__ __forceinline__ void bin_pair(const BinPair &b, float2 s, const RayCo
 }
 
 // Unroll factor of the polynomial-only iterations (measured at 256^3 / 4096
-// sources with two rays per lane: 4 runs the rates 2% faster than 2, at 128
-// registers without spills).
+// sources with two rays per lane: at 8 warps x 2 CTAs, 4 runs the rates 2%
+// faster than 2, at 128 registers without spills; at the 96 registers of
+// 5 CTAs of 4 warps, 4 spills and 2 does not).
 #ifndef ARGOT_RATE_UNROLL
-#define ARGOT_RATE_UNROLL 4
+#define ARGOT_RATE_UNROLL 2
 #endif
 constexpr int kRateUnroll = ARGOT_RATE_UNROLL;
 
